@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MLS-MPM substep: MPM particle-steps/s.
+
+Workload (default, one GPU): the single large scene — 256^3 grid, dx = 1/256,
+16M particles in 4 seeded random boxes (8 particles per cell, per-box elastic
+modulus log-uniform in [1e4, 1e5] or snow with theta_c 2.5e-2, theta_s
+7.5e-3), FP32 state with the FP64 SVD/polar decomposition, dt = 2e-5.  A
+"step" is one substep of the whole scene.  Particle state (1.8 GB) and grid
+(0.8 GB) are far larger than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload large|cube|batched]
+
+N > 1 runs under torchrun: every rank steps its own replica of the scene
+(independent scenes, no data-path collective; "scaling": "weak"); time is the
+max over ranks.  `--impl reference` times the CPU restatement of the
+reference step (the oracle, OpenMP on all host cores) on a bounded sample of
+the same workload and prints the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MPM particle-steps/sec on 1 B200 (batched-served vs plain) + p50/p99 step ms"
+UNIT = "particle-steps/s"
+
+# Algorithmic bytes (dominant kernel = fused G2P + return mapping + P2G):
+# per particle it reads pos 12 + F 36 + jp 4 + mass 4 + volume 4 + material 4
+# = 64 B and writes pos 12 + vel 12 + C 36 + F 36 + jp 4 = 100 B; per active
+# grid node it reads the velocity (16 B) and adds one accumulator (16 B).
+FUSED_BYTES_PER_PARTICLE = 164
+FUSED_BYTES_PER_ACTIVE_CELL = 32
+# Whole-step model of the survey (separate P2G and G2P passes):
+# 268 B per particle-step + 56 B per active cell-step.
+STEP_BYTES_PER_PARTICLE = 268
+STEP_BYTES_PER_ACTIVE_CELL = 56
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, x: float, device=None) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+def make_workload(name: str, rank: int):
+    from molla_b200 import scenes
+    if name == "large":
+        return scenes.boxes_scene(grid_size=256, n_particles=16_000_000, n_boxes=4, seed=1 + rank), \
+            {"workload": "single large scene: 256^3 grid, 16M particles in 4 seeded boxes (elastic E 1e4..1e5 / "
+                         "snow), FP32 + FP64 SVD, dt 2e-5", "grid": 256, "particles": 16_000_000,
+             "svd": "fp64", "l2": "inputs (2.6 GB state) exceed the 126 MB L2; no flush needed"}
+    if name == "cube":
+        return scenes.cube_scene(grid_size=64, seed=rank, walls=1), \
+            {"workload": "elastic cube: 64^3 grid, 132,651 particles, E 1e4, sticky walls 3 cells, FP32, dt 1e-4",
+             "grid": 64, "particles": 132651, "svd": "fp32",
+             "l2": "state (15 MB) fits in L2; reported for reference only"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_sample_scene(n_sample: int, seed: int = 1):
+    from molla_b200 import scenes
+    return scenes.boxes_scene(grid_size=256, n_particles=n_sample, n_boxes=4, seed=seed)
+
+
+def time_cpu_oracle(scene, steps: int, warmup: int, threads: int):
+    """Times the oracle (FP32 state, FP64 SVD, OpenMP) on `scene`."""
+    import molla_b200 as m
+    from oracle import oracle as O
+    cfg = m.config_for_scene(scene, svd_precision=1)
+    sc = O.make_scene(cfg, scene.rows, scene.dt)
+    st = O.init_state(scene.positions, mass=cfg.particle_mass, volume=cfg.particle_volume, ids=scene.ids)
+    if warmup:
+        O.step(sc, st, warmup, precision="f32_svd64", nthreads=threads)
+    t0 = time.perf_counter()
+    O.step(sc, st, steps, precision="f32_svd64", nthreads=threads)
+    dt = time.perf_counter() - t0
+    return scene.n * steps / dt, dt
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    dist = init_dist(ws, "gloo")
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    from oracle import oracle as O
+    threads = O.max_threads()
+    # Size the sample so the whole run stays within about two minutes.
+    probe = cpu_sample_scene(200_000)
+    rate, _ = time_cpu_oracle(probe, 1, 0, threads)
+    budget_s = 120.0
+    per_step = budget_s / max(args.steps + args.warmup, 1)
+    n_sample = int(min(16_000_000, max(20_000, rate * per_step * 0.8)))
+    scene = cpu_sample_scene(n_sample)
+    value, secs = time_cpu_oracle(scene, args.steps, args.warmup, threads)
+    _, meta = make_workload(args.workload, 0) if args.workload != "large" else (None, {
+        "workload": "single large scene: 256^3 grid, 16M particles in 4 seeded boxes (elastic E 1e4..1e5 / snow), "
+                    "FP32 + FP64 SVD, dt 2e-5", "grid": 256, "particles": 16_000_000, "svd": "fp64"})
+    sample = (f"{scene.n} particles of the same generator (256^3 grid, 4 boxes, same materials, dt 2e-5), "
+              f"{args.steps} substeps after {args.warmup} warm-up")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 svd)", "data": "synthetic (seeded)",
+        "config": meta,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+
+    import molla_b200 as m
+
+    ws, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU (the MPM path has no CPU fallback)")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(ws, "nccl")
+
+    scene, meta = make_workload(args.workload, rank)
+    svd_prec = 1 if meta["svd"] == "fp64" else 0
+    engine = m.Engine(local)
+    cfg = m.config_for_scene(scene, svd_precision=svd_prec)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(scene.positions)
+    sim.set_materials(scene.rows, scene.ids)
+    sim.set_sort_interval(args.sort_interval)
+    n = scene.n
+
+    # warm-up
+    sim.step_n(scene.dt, max(args.warmup, 3))
+    engine.synchronize()
+    gm, _ = sim.read_grid_mass_momentum()
+    active = int((gm > 0).sum())
+    del gm
+
+    # timed region: K substeps in one step_n call, bracketed by a barrier
+    # and synchronisation on both sides; device time from CUDA events
+    # recorded on the engine's stream (the stream every kernel launches on).
+    engine.reset_profile()
+    engine.profile(True)
+    launches0 = engine.launch_count
+    stream = torch.cuda.ExternalStream(engine.stream_handle, device=device)
+    barrier(dist, device)
+    engine.synchronize()
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        start.record(stream)
+        sim.step_n(scene.dt, args.steps)
+        stop.record(stream)
+        stop.synchronize()
+        wall = time.perf_counter() - t0
+    engine.synchronize()
+    engine.profile(False)
+    launches = engine.launch_count - launches0
+    prof = engine.read_profile()
+    elapsed = start.elapsed_time(stop) / 1000.0
+    elapsed_max = max_over_ranks(dist, elapsed, device)
+    value = n * args.steps * ws / elapsed_max
+
+    # per-step latency distribution (single-step calls)
+    lat = []
+    for _ in range(args.latency_samples):
+        engine.synchronize()
+        t = time.perf_counter()
+        sim.step_n(scene.dt, 1)
+        engine.synchronize()
+        lat.append(1000.0 * (time.perf_counter() - t))
+
+    # end to end through the C ABI with host buffers: upload the scene
+    # (positions + material ids from pinned host memory), run e2e_substeps
+    # substeps, read positions back.
+    pos_host = torch.from_numpy(scene.positions).pin_memory().numpy()
+    ids_host = torch.from_numpy(scene.ids.astype(np.int32)).pin_memory().numpy().view(np.uint32)
+    e2e_times = []
+    for it in range(args.e2e_iters + 1):
+        engine.synchronize()
+        t = time.perf_counter()
+        sim.set_particles(pos_host)
+        sim.set_materials(scene.rows, ids_host)
+        sim.step_n(scene.dt, args.e2e_substeps)
+        out = sim.read_positions()
+        e2e_times.append(time.perf_counter() - t)
+    e2e_s = float(np.median(e2e_times[1:]))
+    e2e_s = max_over_ranks(dist, e2e_s, device)
+    e2e_value = n * args.e2e_substeps * ws / e2e_s
+
+    result = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        fused = prof.get("GatherScatter", (0, 0.0))
+        fused_ms = fused[1] / max(fused[0], 1)
+        fused_bytes = FUSED_BYTES_PER_PARTICLE * n + FUSED_BYTES_PER_ACTIVE_CELL * active
+        achieved = fused_bytes / (fused_ms / 1000.0) / 1e9 if fused_ms > 0 else 0.0
+        step_bytes = STEP_BYTES_PER_PARTICLE * n + STEP_BYTES_PER_ACTIVE_CELL * active
+        step_achieved = step_bytes / (elapsed / args.steps) / 1e9
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            from oracle import oracle as O
+            threads = O.max_threads()
+            probe = cpu_sample_scene(200_000)
+            rate, _ = time_cpu_oracle(probe, 1, 0, threads)
+            n_sample = int(min(16_000_000, max(20_000, rate * 15.0 / 3)))
+            cs = cpu_sample_scene(n_sample)
+            cval, csecs = time_cpu_oracle(cs, 3, 0, threads)
+            cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{cs.n} particles of the same generator (256^3 grid, 4 boxes), 3 substeps, "
+                             f"{csecs:.1f} s"}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 svd)" if svd_prec else "f32",
+            "data": "synthetic (seeded boxes; no dataset)",
+            "config": dict(meta, active_cells=active, sort_interval=args.sort_interval,
+                           parallelism=f"replicas x{ws}" if ws > 1 else "single scene"),
+            "p50_step_ms": float(np.percentile(lat, 50)) if lat else None,
+            "p99_step_ms": float(np.percentile(lat, 99)) if lat else None,
+            "stages_ms_per_step": {k: v[1] / max(args.steps, 1) for k, v in prof.items()},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_particles<G2P2G> (fused gather, return mapping, scatter)",
+                         "bytes_per_launch": fused_bytes, "avg_launch_ms": fused_ms},
+            "step_roofline": {"achieved": step_achieved, "frac": step_achieved / hbm,
+                              "bytes_per_step": step_bytes, "model": "268 B/particle + 56 B/active cell"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "substeps_per_call": args.e2e_substeps,
+                    "h2d_bytes_per_step": int(pos_host.nbytes + ids_host.nbytes),
+                    "d2h_bytes_per_step": int(out.nbytes)},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "wall_s": wall,
+        }
+    barrier(dist, device)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    sim.close()
+    engine.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large", choices=["large", "cube"])
+    ap.add_argument("--sort-interval", type=int, default=16)
+    ap.add_argument("--latency-samples", type=int, default=20)
+    ap.add_argument("--e2e-iters", type=int, default=3)
+    ap.add_argument("--e2e-substeps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

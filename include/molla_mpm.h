@@ -1,0 +1,353 @@
+/*
+ * molla_mpm.h — C ABI of the B200-native explicit MLS-MPM substep.
+ *
+ * This is the drop-in boundary for molla's MPM solver interface
+ * (crates/molla-solvers/src/lib.rs:180-199 re-exports MpmSimulation,
+ * MpmConfig, MpmRheology, MpmTimeStep, PreparedMpmStep, MpmCommandBatch).
+ * A Rust `extern "C"` crate binds these symbols one to one; every entry point
+ * below names the reference item it replaces (path:line inside the molla
+ * repository).  Plain pointers and sizes only: host arrays are borrowed for
+ * the duration of the call, device memory is owned by the library.
+ *
+ * Errors: every function returns an mpm_status code (0 = MPM_OK).  The text
+ * of the last error on the calling thread is available from mpm_last_error
+ * (the Display string of molla_core::Error, crates/molla-core/src/error.rs:9-40).
+ *
+ * Threading: one thread at a time per simulation/batch/server object, as the
+ * reference's `&mut self` receivers require.  Different objects may be used
+ * from different threads.
+ */
+#ifndef MOLLA_MPM_H
+#define MOLLA_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPM_API __attribute__((visibility("default")))
+#else
+#define MPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOLLA_MPM_ABI_VERSION 1u
+
+/* Status codes.  MPM_ERR_INVALID mirrors Error::Solver (invalid input or
+ * state), MPM_ERR_GPU mirrors Error::Gpu (device problems), MPM_ERR_FAULT is
+ * a latched numerical fault (mpm.rs:1397-1427), MPM_ERR_STALE a prepared step
+ * from another simulation or configuration (mpm_command_batch.rs:169-176). */
+typedef enum mpm_status {
+  MPM_OK = 0,
+  MPM_ERR_INVALID = 1,
+  MPM_ERR_GPU = 2,
+  MPM_ERR_FAULT = 3,
+  MPM_ERR_STALE = 4,
+  MPM_ERR_NOMEM = 5,
+  MPM_ERR_UNSUPPORTED = 6,
+  MPM_ERR_BUSY = 7
+} mpm_status;
+
+/* Rheology kinds, MpmRheology (crates/molla-solvers/src/mpm.rs:320-370). */
+typedef enum mpm_rheology_kind {
+  MPM_RHEOLOGY_SAND = 0,
+  MPM_RHEOLOGY_SNOW = 1,
+  MPM_RHEOLOGY_VISCOUS = 2
+} mpm_rheology_kind;
+
+/* One material row.  Sand uses friction_angle (radians); snow uses theta_c,
+ * theta_s, hardening; viscous uses velocity_damping, affine_damping (1/s).
+ * youngs/poisson > 0 give this row its own elastic moduli — an extension for
+ * scenes that mix stiffnesses; 0 keeps the simulation-wide values, which is
+ * the reference behaviour (mpm.wgsl:98-99 has global E and nu only). */
+typedef struct mpm_rheology {
+  uint32_t kind;
+  float friction_angle;
+  float theta_c;
+  float theta_s;
+  float hardening;
+  float velocity_damping;
+  float affine_damping;
+  float youngs;
+  float poisson;
+} mpm_rheology;
+
+/* Time-step selector, MpmTimeStep (mpm.rs:372-398). Only the explicit step is
+ * built; the semi-implicit Jacobi relaxation is rejected with
+ * MPM_ERR_UNSUPPORTED. */
+typedef enum mpm_time_step_kind { MPM_TIME_STEP_EXPLICIT = 0, MPM_TIME_STEP_IMPLICIT = 1 } mpm_time_step_kind;
+
+/* Precision of the per-particle SVD/polar decomposition.  The particle and
+ * grid state is FP32 in both cases. */
+typedef enum mpm_svd_precision { MPM_SVD_FP32 = 0, MPM_SVD_FP64 = 1 } mpm_svd_precision;
+
+/* Wall models.  MPM_WALLS_REFERENCE: the reference's pad-2 one-sided normal
+ * clamp with tangential friction (mpm.wgsl:1044-1056).  MPM_WALLS_STICKY:
+ * extension, every velocity component is zeroed inside the pad layer. */
+typedef enum mpm_wall_kind { MPM_WALLS_REFERENCE = 0, MPM_WALLS_STICKY = 1 } mpm_wall_kind;
+
+/* MpmConfig (crates/molla-solvers/src/mpm.rs:400-433) plus extensions.
+ * Fields after `jacobi_iters` are extensions; zero-initialised they select the
+ * reference behaviour (pad 2, reference walls, FP32 SVD, window 0). */
+typedef struct mpm_config {
+  uint32_t grid_size;
+  float cell_size;
+  float grid_origin[3];
+  float gravity_y;
+  float youngs;
+  float poisson;
+  float friction_angle;
+  float cohesion;
+  float boundary_friction;
+  float particle_mass;
+  float particle_volume;
+  uint32_t max_particles;
+  uint32_t max_rigid;
+  mpm_rheology rheology;
+  uint32_t time_step;    /* mpm_time_step_kind */
+  uint32_t jacobi_iters; /* MpmTimeStep::Implicit */
+  /* extensions */
+  uint32_t boundary_pad; /* 0 → 2 */
+  uint32_t walls;        /* mpm_wall_kind */
+  uint32_t svd_precision;/* mpm_svd_precision */
+  int32_t grid_window_cells[3];
+  uint32_t reserved[8];
+} mpm_config;
+
+/* Presets MpmConfig::{sand, sand_calibrated, snow, viscous}
+ * (mpm.rs:540-655). */
+typedef enum mpm_preset {
+  MPM_PRESET_SAND = 0,
+  MPM_PRESET_SAND_CALIBRATED = 1,
+  MPM_PRESET_SNOW = 2,
+  MPM_PRESET_VISCOUS = 3
+} mpm_preset;
+
+/* Fault/status word, MpmActiveGridStats (mpm.rs:257-283). */
+typedef struct mpm_status_info {
+  uint32_t numerical_fault;   /* latched non-finite state (mpm.wgsl:217-231) */
+  uint32_t completed_substeps;/* gathers run since the last fault reset (mpm.wgsl:1246) */
+  uint32_t fault_bits;        /* raw latch word */
+  uint32_t reserved;
+} mpm_status_info;
+
+/* Opaque handles. */
+typedef struct mpm_engine mpm_engine;
+typedef struct mpm_sim mpm_sim;
+typedef struct mpm_prepared mpm_prepared;
+typedef struct mpm_batch mpm_batch;
+typedef struct mpm_group mpm_group;
+typedef struct mpm_server mpm_server;
+
+/* ---- engine ---------------------------------------------------------- */
+
+/* Engine::new_gpu (crates/molla-compute/src/engine.rs:140): binds a CUDA
+ * device and creates the engine's stream.  `device` is the CUDA ordinal. */
+MPM_API int mpm_engine_create(int device, mpm_engine** out);
+MPM_API int mpm_engine_destroy(mpm_engine* engine);
+/* Engine::check_device / DeviceHealth (engine.rs:70-119): MPM_ERR_GPU once a
+ * device error was observed on this engine (sticky). */
+MPM_API int mpm_engine_check(mpm_engine* engine);
+/* Synchronise the engine's stream (the reference's device.poll(wait)). */
+MPM_API int mpm_engine_synchronize(mpm_engine* engine);
+/* The engine's cudaStream_t (every simulation of the engine launches on it),
+ * for callers that order their own work or CUDA events against it. */
+MPM_API void* mpm_engine_stream(mpm_engine* engine);
+
+/* ---- configuration ----------------------------------------------------- */
+
+/* MpmConfig::{sand, sand_calibrated, snow, viscous} (mpm.rs:540-655). */
+MPM_API int mpm_config_preset(uint32_t preset, mpm_config* out);
+/* Host-side Drucker-Prager alpha of a material row, material_row
+ * (mpm.rs:662-686): sqrt(2/3)*2 sin(phi)/(3 - sin(phi)). */
+MPM_API float mpm_dp_alpha(float friction_angle);
+
+/* ---- simulation -------------------------------------------------------- */
+
+/* MpmSimulation::new (mpm.rs:834-843, validation :855-900). */
+MPM_API int mpm_sim_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim** out);
+MPM_API int mpm_sim_destroy(mpm_sim* sim);
+
+/* set_particles / set_particles_with_velocity (mpm.rs:1451-1519):
+ * positions xyz[3n]; velocities vel[3n] or NULL (rest).  F = I, C = 0,
+ * jp = 0, mass/volume from the config.  n > max_particles → MPM_ERR_INVALID. */
+MPM_API int mpm_set_particles(mpm_sim* sim, const float* xyz, const float* vel_or_null, uint32_t n);
+
+/* Extension of set_particles for scenes with per-particle mass/volume
+ * (NULL keeps the config value for every particle). */
+MPM_API int mpm_set_particle_mass_volume(mpm_sim* sim, const float* mass_or_null, const float* volume_or_null,
+                                 uint32_t n);
+
+/* set_materials (mpm.rs:1589-1621): 1..8 rows, ids[n] < rows, n must equal
+ * the particle count. */
+MPM_API int mpm_set_materials(mpm_sim* sim, const mpm_rheology* rows, uint32_t n_rows, const uint32_t* ids, uint32_t n);
+/* set_rheology (mpm.rs:1623-1629). */
+MPM_API int mpm_set_rheology(mpm_sim* sim, const mpm_rheology* rheology);
+/* set_material (mpm.rs:1578-1587): live Young's modulus and friction angle. */
+MPM_API int mpm_set_material(mpm_sim* sim, float youngs, float friction_angle);
+/* set_time_step (mpm.rs:1631-1635). */
+MPM_API int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters);
+
+/* set_p2g_mode (mpm.rs:1642-1650).  Both reference modes map to the same
+ * tile-accumulated scatter here; the flag is kept for API parity. */
+MPM_API int mpm_set_p2g_mode(mpm_sim* sim, int two_pass);
+/* set_deterministic_p2g (mpm_deterministic_p2g.rs:550-569): fixed-order
+ * grid-centric P2G over the tile-sorted particles, bit-repeatable.
+ * Requires prepared and enabled particle ordering (as the reference). */
+MPM_API int mpm_prepare_deterministic_p2g(mpm_sim* sim);
+MPM_API int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled);
+
+/* prepare_particle_tile_ordering (mpm_particle_order.rs:161-230): capacity in
+ * 1..=max_particles and >= the live count. */
+MPM_API int mpm_prepare_particle_tile_ordering(mpm_sim* sim, uint32_t capacity);
+/* set_particle_tile_ordering (mpm_particle_order.rs:232-252). */
+MPM_API int mpm_set_particle_tile_ordering(mpm_sim* sim, int enabled);
+/* Sort interval of the hot path: particles are physically regrouped by 4^3
+ * tile every `interval` substeps (0 → autotuned default). */
+MPM_API int mpm_set_sort_interval(mpm_sim* sim, uint32_t interval);
+
+/* step / step_n (mpm.rs:2232-2353): asynchronous; dt finite and > 0. */
+MPM_API int mpm_step_n(mpm_sim* sim, float dt, uint32_t substeps);
+
+/* prepare_step (mpm_command_batch.rs:36-140): freezes dt, substeps, material
+ * table and sort parameters; the substep sequence is captured once as a CUDA
+ * graph.  A later configuration change makes the record stale. */
+MPM_API int mpm_prepare_step(mpm_sim* sim, float dt, uint32_t substeps, mpm_prepared** out);
+MPM_API int mpm_prepared_destroy(mpm_prepared* prepared);
+/* begin_command_batch / encode_step / submit (mpm_command_batch.rs:142-218).
+ * `stream` is a caller-owned cudaStream_t (NULL: the engine's stream); encode
+ * launches the prepared graph on it, submit records completion. */
+MPM_API int mpm_batch_begin(mpm_sim* sim, void* stream, mpm_batch** out);
+MPM_API int mpm_batch_encode_step(mpm_batch* batch, const mpm_prepared* prepared);
+MPM_API int mpm_batch_submit(mpm_batch* batch);
+MPM_API int mpm_batch_cancel(mpm_batch* batch);
+
+/* read_positions / read_velocities (mpm.rs:2718-2798): blocking; writes
+ * min(count, cap) rows of 3 floats in the original particle order and
+ * stores the particle count in *count_out. */
+MPM_API int mpm_read_positions(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
+MPM_API int mpm_read_velocities(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
+/* Full particle state in original order: C[9n], F[9n] column-major, jp[n]
+ * (any pointer may be NULL). */
+MPM_API int mpm_read_particle_state(mpm_sim* sim, float* C, float* F, float* jp, uint32_t cap, uint32_t* count_out);
+/* Overwrite deformation gradients/jp of live particles in original order
+ * (checkpoint restore and host-side fault injection; NULL keeps a field). */
+MPM_API int mpm_write_particle_state(mpm_sim* sim, const float* C, const float* F, const float* jp, uint32_t n);
+/* read_grid_mass_momentum (mpm.rs:2808-2906): grid mass[N^3] and momentum
+ * [3 N^3] of the last substep's P2G. */
+MPM_API int mpm_read_grid_mass_momentum(mpm_sim* sim, float* mass, float* momentum, size_t cells);
+/* Conservation totals accumulated in FP64 on the device:
+ * out[0] grid mass, out[1..3] grid momentum, out[4] particle mass,
+ * out[5..7] particle momentum. */
+MPM_API int mpm_conservation_totals(mpm_sim* sim, double* out8);
+
+/* read_active_grid_status_with (mpm.rs:1418-1427). */
+MPM_API int mpm_read_status(mpm_sim* sim, mpm_status_info* out);
+/* reset_active_grid (mpm.rs:1387-1390): clears the latch and counters. */
+MPM_API int mpm_reset_fault(mpm_sim* sim);
+
+/* ParticleOrder::encode + readback (mpm_particle_order.rs:118-150): computes
+ * tile keys for the current positions and sorts (key, identity) stably over
+ * `capacity` entries; identities past the live count carry key 0xFFFFFFFF.
+ * keys/ids receive capacity entries. */
+MPM_API int mpm_read_sort_permutation(mpm_sim* sim, uint32_t* keys, uint32_t* ids, uint32_t capacity);
+
+/* Stable LSD radix sort of (u32 key, u32 value) pairs, RadixSortKernel
+ * (crates/molla-compute-primitives/src/radix_sort.rs:50-110).  Host arrays
+ * in, sorted in place.  key_bits in 1..32 (passes = ceil(key_bits/8)). */
+MPM_API int mpm_radix_sort_pairs(mpm_engine* engine, uint32_t* keys, uint32_t* values, uint32_t n, uint32_t key_bits);
+
+/* Device-pointer form: sorts d_keys/d_values (n entries) on `stream` using
+ * library-owned scratch.  Asynchronous. */
+MPM_API int mpm_radix_sort_pairs_device(mpm_engine* engine, uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+                                uint32_t key_bits, void* stream);
+
+/* Number of CUDA kernel launches this library issued on the engine since
+ * creation (host counter, the equivalent of gpu_metrics::record_dispatch,
+ * crates/molla-core/src/gpu_metrics.rs:330-381). */
+MPM_API uint64_t mpm_engine_launch_count(mpm_engine* engine);
+
+/* Per-stage GPU timing, the equivalent of molla's step profiling
+ * (prepare_step_profiling / read_step_profile, mpm_profile.rs:542-732):
+ * while enabled, each launch of a stage is bracketed by CUDA events on its
+ * stream (not inside captured graphs).  Stages: 0 particle ordering (keys,
+ * sort, regroup, work list), 1 P2G, 2 grid update, 3 fused G2P + return
+ * mapping + next P2G, 4 G2P + return mapping. */
+typedef struct mpm_profile_stage {
+  uint64_t launches;
+  double total_ms;
+} mpm_profile_stage;
+MPM_API int mpm_profile_enable(mpm_engine* engine, int enabled);
+/* Synchronises, resolves pending events and copies `cap` (<= 5) stages. */
+MPM_API int mpm_profile_read(mpm_engine* engine, mpm_profile_stage* out, uint32_t cap);
+MPM_API int mpm_profile_reset(mpm_engine* engine);
+
+/* ---- batched scenes ----------------------------------------------------- */
+
+/* A group steps many independent scenes of uneven particle and grid sizes in
+ * the same launches (persistent kernels over a (scene, tile) work list).  No
+ * reference equivalent; the per-scene numerics are those of mpm_sim. */
+MPM_API int mpm_group_create(mpm_engine* engine, uint32_t max_scenes, uint64_t max_particles_total,
+                     uint64_t max_cells_total, mpm_group** out);
+MPM_API int mpm_group_destroy(mpm_group* group);
+/* Adds a scene; returns its id.  Particles xyz[3n] (at rest), one material
+ * row per scene plus per-particle material ids (NULL: row 0). */
+MPM_API int mpm_group_add_scene(mpm_group* group, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
+                        const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t* scene_id);
+MPM_API int mpm_group_remove_scene(mpm_group* group, uint32_t scene_id);
+/* Advances every scene in the group by `substeps` substeps at its own dt. */
+MPM_API int mpm_group_step(mpm_group* group, uint32_t substeps);
+/* Captures `substeps` group substeps as a CUDA graph and replays it `repeat`
+ * times. */
+MPM_API int mpm_group_step_graph(mpm_group* group, uint32_t substeps, uint32_t repeat);
+MPM_API int mpm_group_read_positions(mpm_group* group, uint32_t scene_id, float* out, uint32_t cap, uint32_t* count_out);
+MPM_API int mpm_group_read_status(mpm_group* group, uint32_t scene_id, mpm_status_info* out);
+MPM_API int mpm_group_scene_count(mpm_group* group, uint32_t* count);
+/* Group tuning: particles per work item and sort interval (0 → defaults). */
+MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
+
+/* ---- serving ------------------------------------------------------------- */
+
+/* A request loop over a group: scenes are admitted as HBM budget and slots
+ * allow, stepped together, and retired when their steps are done. */
+MPM_API int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t max_scenes, mpm_server** out);
+MPM_API int mpm_server_destroy(mpm_server* server);
+/* Queues a scene for `steps` substeps; returns a ticket. */
+MPM_API int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
+                      const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t steps,
+                      uint64_t* ticket);
+/* Runs `ticks` scheduling rounds (admit, step `substeps_per_tick` substeps,
+ * retire finished scenes). */
+MPM_API int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tick);
+/* state: 0 queued, 1 running, 2 done.  When done, positions are copied out. */
+MPM_API int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float* positions_out, uint32_t cap,
+                    uint32_t* count_out);
+/* Server statistics: admitted, completed, resident scenes, resident bytes,
+ * particle-steps done, and p50/p99 tick latency in milliseconds. */
+typedef struct mpm_server_stats {
+  uint64_t admitted;
+  uint64_t completed;
+  uint64_t resident_scenes;
+  uint64_t resident_bytes;
+  uint64_t particle_steps;
+  double tick_ms_p50;
+  double tick_ms_p99;
+  double queue_ms_p50;
+  double queue_ms_p99;
+} mpm_server_stats;
+MPM_API int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out);
+
+/* ---- errors ------------------------------------------------------------- */
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated
+ * to `size`); returns its full length. */
+MPM_API size_t mpm_last_error(char* buf, size_t size);
+MPM_API uint32_t mpm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOLLA_MPM_H */

@@ -1,0 +1,1060 @@
+// mpm_abi.cu — the extern "C" entry points declared in include/molla_mpm.h.
+// Each function maps library exceptions to status codes and records the
+// message for mpm_last_error on the calling thread.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mpm_runtime.cuh"
+
+using mpm::Error;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return MPM_OK;
+  } catch (const Error& e) {
+    return fail(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(MPM_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(MPM_ERR_INVALID, e.what());
+  }
+}
+
+#define REQUIRE(cond, code, msg) \
+  do {                           \
+    if (!(cond)) throw Error((code), (msg)); \
+  } while (0)
+
+bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+void validate_config(const mpm_config& c) {
+  REQUIRE(c.grid_size > 0 && (uint64_t)c.grid_size * c.grid_size * c.grid_size < (1ull << 40), MPM_ERR_INVALID,
+          "MPM grid dimensions overflow or are empty");
+  REQUIRE(std::isfinite(c.cell_size) && c.cell_size > 0.f && finite3(c.grid_origin), MPM_ERR_INVALID,
+          "MPM grid exceeds device capacity or has invalid spacing/origin");
+  REQUIRE(c.rheology.kind <= MPM_RHEOLOGY_VISCOUS, MPM_ERR_INVALID, "unknown MPM rheology");
+  REQUIRE(c.time_step == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED,
+          "semi-implicit Jacobi MPM is not part of this build; use the explicit time step");
+  REQUIRE(c.walls <= MPM_WALLS_STICKY, MPM_ERR_INVALID, "unknown MPM wall model");
+  REQUIRE(c.svd_precision <= MPM_SVD_FP64, MPM_ERR_INVALID, "unknown MPM SVD precision");
+  REQUIRE(c.boundary_pad == 0 || c.boundary_pad * 2 < c.grid_size, MPM_ERR_INVALID, "MPM boundary pad too wide");
+}
+
+mpm_rheology sand_row(float phi) {
+  mpm_rheology r{};
+  r.kind = MPM_RHEOLOGY_SAND;
+  r.friction_angle = phi;
+  return r;
+}
+
+}  // namespace
+
+struct mpm_engine {
+  std::unique_ptr<mpm::Engine> e;
+};
+
+struct mpm_sim {
+  mpm::Engine* eng = nullptr;
+  std::unique_ptr<mpm::Group> group;
+  mpm_config cfg{};
+  std::vector<mpm_rheology> rows;  // set_materials rows; empty: cfg.rheology
+  std::vector<uint32_t> ids;       // material ids as last set
+  std::vector<float> mass, volume; // optional per-particle overrides
+  uint32_t sid = 0xffffffffu;
+  uint32_t count = 0;
+  bool order_prepared = false;
+  uint32_t order_capacity = 0;
+  bool order_enabled = false;
+  bool det_prepared = false;
+  bool det_enabled = false;
+  uint32_t sort_interval = 0;
+  uint64_t epoch = 1;
+  float dt = 1.0e-4f;
+
+  std::vector<mpm_rheology> effective_rows() const {
+    if (!rows.empty()) return rows;
+    return {cfg.rheology};
+  }
+  void apply_group_settings() {
+    group->svd_fp64 = cfg.svd_precision == MPM_SVD_FP64;
+    const uint32_t interval = order_enabled ? 1u : (sort_interval ? sort_interval : 16u);
+    group->sort_interval = interval;
+  }
+  void invalidate() { ++epoch; }
+};
+
+struct mpm_prepared {
+  mpm_sim* sim;
+  uint64_t epoch;
+  float dt;
+  uint32_t substeps;
+};
+
+struct mpm_batch {
+  mpm_sim* sim;
+  cudaStream_t stream;
+  std::vector<std::pair<float, uint32_t>> work;
+  bool done = false;
+};
+
+extern "C" {
+
+uint32_t mpm_abi_version(void) { return MOLLA_MPM_ABI_VERSION; }
+
+size_t mpm_last_error(char* buf, size_t size) {
+  if (buf && size) {
+    const size_t n = std::min(size - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), n);
+    buf[n] = 0;
+  }
+  return g_last_error.size();
+}
+
+// ---- engine ----------------------------------------------------------------
+
+int mpm_engine_create(int device, mpm_engine** out) {
+  return guard([&] {
+    REQUIRE(out, MPM_ERR_INVALID, "null output handle");
+    auto* h = new mpm_engine();
+    try {
+      h->e.reset(new mpm::Engine(device));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int mpm_engine_destroy(mpm_engine* engine) {
+  return guard([&] { delete engine; });
+}
+
+int mpm_engine_check(mpm_engine* engine) {
+  return guard([&] {
+    REQUIRE(engine, MPM_ERR_INVALID, "null engine");
+    engine->e->check();
+    cudaError_t e = cudaStreamQuery(engine->e->stream);
+    if (e != cudaSuccess && e != cudaErrorNotReady) {
+      engine->e->note_error(e);
+      mpm::throw_cuda(e, "engine check");
+    }
+  });
+}
+
+int mpm_engine_synchronize(mpm_engine* engine) {
+  return guard([&] {
+    REQUIRE(engine, MPM_ERR_INVALID, "null engine");
+    engine->e->check();
+    cudaError_t e = cudaStreamSynchronize(engine->e->stream);
+    if (e != cudaSuccess) {
+      engine->e->note_error(e);
+      mpm::throw_cuda(e, "stream synchronize");
+    }
+  });
+}
+
+uint64_t mpm_engine_launch_count(mpm_engine* engine) { return engine ? engine->e->launches : 0; }
+
+void* mpm_engine_stream(mpm_engine* engine) { return engine ? (void*)engine->e->stream : nullptr; }
+
+int mpm_profile_enable(mpm_engine* engine, int enabled) {
+  return guard([&] {
+    REQUIRE(engine, MPM_ERR_INVALID, "null engine");
+    engine->e->profiling = enabled != 0;
+  });
+}
+
+int mpm_profile_read(mpm_engine* engine, mpm_profile_stage* out, uint32_t cap) {
+  return guard([&] {
+    REQUIRE(engine && out, MPM_ERR_INVALID, "null argument");
+    engine->e->prof_resolve();
+    for (uint32_t i = 0; i < cap && i < (uint32_t)mpm::kStages; ++i) {
+      out[i].launches = engine->e->prof_count[i];
+      out[i].total_ms = engine->e->prof_ms[i];
+    }
+  });
+}
+
+int mpm_profile_reset(mpm_engine* engine) {
+  return guard([&] {
+    REQUIRE(engine, MPM_ERR_INVALID, "null engine");
+    engine->e->prof_resolve();
+    for (int i = 0; i < mpm::kStages; ++i) {
+      engine->e->prof_ms[i] = 0;
+      engine->e->prof_count[i] = 0;
+    }
+  });
+}
+
+// ---- configuration -----------------------------------------------------------
+
+float mpm_dp_alpha(float friction_angle) { return mpm::dp_alpha_of(friction_angle); }
+
+int mpm_config_preset(uint32_t preset, mpm_config* out) {
+  return guard([&] {
+    REQUIRE(out, MPM_ERR_INVALID, "null config");
+    mpm_config c{};
+    const float deg30 = 30.0f * 3.14159265358979f / 180.0f;
+    c.max_rigid = 8;
+    c.cohesion = 0.f;
+    c.time_step = MPM_TIME_STEP_EXPLICIT;
+    switch (preset) {
+      case MPM_PRESET_SAND:  // mpm.rs:540-560
+        c.grid_size = 32;
+        c.cell_size = 0.05f;
+        c.grid_origin[0] = -0.8f, c.grid_origin[1] = 0.f, c.grid_origin[2] = -0.8f;
+        c.gravity_y = -9.81f;
+        c.youngs = 5.0e3f;
+        c.poisson = 0.3f;
+        c.friction_angle = deg30;
+        c.boundary_friction = 0.5f;
+        c.particle_mass = 1.0e-3f;
+        c.particle_volume = 1.0e-6f;
+        c.max_particles = 16384;
+        c.rheology = sand_row(deg30);
+        break;
+      case MPM_PRESET_SAND_CALIBRATED:  // mpm.rs:585-605 (the implicit step is not built)
+        c.grid_size = 48;
+        c.cell_size = 0.05f;
+        c.grid_origin[0] = -1.2f, c.grid_origin[1] = 0.f, c.grid_origin[2] = -1.2f;
+        c.gravity_y = -9.81f;
+        c.youngs = 1.0e5f;
+        c.poisson = 0.3f;
+        c.friction_angle = deg30;
+        c.boundary_friction = 0.3f;
+        c.particle_mass = 1.5e-3f;
+        c.particle_volume = 1.0e-6f;
+        c.max_particles = 32768;
+        c.rheology = sand_row(deg30);
+        c.time_step = MPM_TIME_STEP_IMPLICIT;
+        c.jacobi_iters = 3;
+        break;
+      case MPM_PRESET_SNOW:  // mpm.rs:609-631
+        c.grid_size = 32;
+        c.cell_size = 0.05f;
+        c.grid_origin[0] = -0.8f, c.grid_origin[1] = 0.f, c.grid_origin[2] = -0.8f;
+        c.gravity_y = -9.81f;
+        c.youngs = 1.4e5f;
+        c.poisson = 0.2f;
+        c.friction_angle = 0.f;
+        c.boundary_friction = 0.5f;
+        c.particle_mass = 1.0e-3f;
+        c.particle_volume = 1.0e-6f;
+        c.max_particles = 16384;
+        c.rheology.kind = MPM_RHEOLOGY_SNOW;
+        c.rheology.theta_c = 2.5e-2f;
+        c.rheology.theta_s = 7.5e-3f;
+        c.rheology.hardening = 10.f;
+        break;
+      case MPM_PRESET_VISCOUS:  // mpm.rs:637-655
+        c.grid_size = 32;
+        c.cell_size = 0.05f;
+        c.grid_origin[0] = -0.8f, c.grid_origin[1] = 0.f, c.grid_origin[2] = -0.8f;
+        c.gravity_y = -9.81f;
+        c.youngs = 2.0e3f;
+        c.poisson = 0.3f;
+        c.friction_angle = 0.f;
+        c.boundary_friction = 0.8f;
+        c.particle_mass = 1.0e-3f;
+        c.particle_volume = 1.0e-6f;
+        c.max_particles = 16384;
+        c.rheology.kind = MPM_RHEOLOGY_VISCOUS;
+        c.rheology.velocity_damping = 4.f;
+        c.rheology.affine_damping = 8.f;
+        break;
+      default:
+        throw Error(MPM_ERR_INVALID, "unknown MPM preset");
+    }
+    *out = c;
+  });
+}
+
+// ---- simulation ---------------------------------------------------------------
+
+int mpm_sim_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim** out) {
+  return guard([&] {
+    REQUIRE(engine && cfg && out, MPM_ERR_INVALID, "null argument");
+    engine->e->check();
+    validate_config(*cfg);
+    auto* s = new mpm_sim();
+    try {
+      s->eng = engine->e.get();
+      s->cfg = *cfg;
+      const uint64_t n3 = (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
+      s->group.reset(new mpm::Group(s->eng, 1, std::max<uint32_t>(cfg->max_particles, 1), n3));
+      s->apply_group_settings();
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+  });
+}
+
+int mpm_sim_destroy(mpm_sim* sim) {
+  return guard([&] { delete sim; });
+}
+
+static void sim_reseed(mpm_sim* s, const float* xyz, const float* vel, uint32_t n) {
+  if (s->sid != 0xffffffffu) {
+    s->group->remove_scene(s->sid);
+    s->sid = 0xffffffffu;
+  }
+  std::vector<uint32_t> mat(n, 0);
+  for (uint32_t i = 0; i < n && i < s->ids.size(); ++i) mat[i] = s->ids[i];
+  const float* mass = s->mass.size() == n && n ? s->mass.data() : nullptr;
+  const float* vol = s->volume.size() == n && n ? s->volume.data() : nullptr;
+  s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, n ? mat.data() : nullptr, n, s->dt);
+  s->count = n;
+  s->apply_group_settings();
+  s->invalidate();
+}
+
+int mpm_set_particles(mpm_sim* sim, const float* xyz, const float* vel_or_null, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(n == 0 || xyz, MPM_ERR_INVALID, "null positions");
+    REQUIRE(n <= sim->cfg.max_particles, MPM_ERR_GPU,
+            "set_particles: n=" + std::to_string(n) + " > max_particles=" + std::to_string(sim->cfg.max_particles));
+    sim->mass.clear();
+    sim->volume.clear();
+    sim_reseed(sim, xyz, vel_or_null, n);
+  });
+}
+
+int mpm_set_particle_mass_volume(mpm_sim* sim, const float* mass_or_null, const float* volume_or_null, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(n == sim->count, MPM_ERR_INVALID, "mass/volume count must equal the particle count");
+    if (!n) return;
+    if (mass_or_null) sim->group->write_rows(sim->sid, mpm::MASS, 1, mass_or_null, sim->eng->stream);
+    if (volume_or_null) sim->group->write_rows(sim->sid, mpm::VOL, 1, volume_or_null, sim->eng->stream);
+    sim->invalidate();
+  });
+}
+
+int mpm_set_materials(mpm_sim* sim, const mpm_rheology* rows, uint32_t n_rows, const uint32_t* ids, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(n_rows >= 1 && n_rows <= 8 && rows, MPM_ERR_INVALID,
+            "MPM set_materials: 1..=8 material rows required, got " + std::to_string(n_rows));
+    REQUIRE(n == sim->count, MPM_ERR_INVALID,
+            "MPM set_materials: " + std::to_string(n) + " particle ids for " + std::to_string(sim->count) +
+                " particles — seed particles first");
+    for (uint32_t i = 0; i < n; ++i)
+      REQUIRE(ids[i] < n_rows, MPM_ERR_INVALID,
+              "MPM set_materials: particle material id " + std::to_string(ids[i]) + " out of range (" +
+                  std::to_string(n_rows) + " rows)");
+    for (uint32_t i = 0; i < n_rows; ++i) REQUIRE(rows[i].kind <= 2, MPM_ERR_INVALID, "unknown MPM rheology");
+    sim->rows.assign(rows, rows + n_rows);
+    sim->ids.assign(ids, ids + n);
+    if (sim->sid != 0xffffffffu) {
+      sim->group->set_scene_rows(sim->sid, sim->effective_rows());
+      sim->group->set_material_ids(sim->sid, ids, n);
+    }
+    sim->invalidate();
+  });
+}
+
+int mpm_set_rheology(mpm_sim* sim, const mpm_rheology* rheology) {
+  return guard([&] {
+    REQUIRE(sim && rheology, MPM_ERR_INVALID, "null argument");
+    REQUIRE(rheology->kind <= 2, MPM_ERR_INVALID, "unknown MPM rheology");
+    sim->cfg.rheology = *rheology;
+    if (rheology->kind == MPM_RHEOLOGY_SAND) sim->cfg.friction_angle = rheology->friction_angle;
+    if (sim->sid != 0xffffffffu) {
+      sim->group->set_scene_cfg(sim->sid, sim->cfg);
+      sim->group->set_scene_rows(sim->sid, sim->effective_rows());
+    }
+    sim->invalidate();
+  });
+}
+
+int mpm_set_material(mpm_sim* sim, float youngs, float friction_angle) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->cfg.youngs = youngs;
+    sim->cfg.friction_angle = friction_angle;
+    if (sim->cfg.rheology.kind == MPM_RHEOLOGY_SAND) sim->cfg.rheology.friction_angle = friction_angle;
+    if (sim->sid != 0xffffffffu) {
+      sim->group->set_scene_cfg(sim->sid, sim->cfg);
+      sim->group->set_scene_rows(sim->sid, sim->effective_rows());
+    }
+    sim->invalidate();
+  });
+}
+
+int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(kind == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED,
+            "semi-implicit Jacobi MPM is not part of this build; use the explicit time step");
+    sim->cfg.time_step = kind;
+    sim->cfg.jacobi_iters = jacobi_iters;
+    sim->invalidate();
+  });
+}
+
+int mpm_set_p2g_mode(mpm_sim* sim, int two_pass) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    (void)two_pass;
+    sim->det_enabled = false;
+    sim->invalidate();
+  });
+}
+
+int mpm_prepare_deterministic_p2g(mpm_sim* sim) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    throw Error(MPM_ERR_UNSUPPORTED, "deterministic fixed-order P2G is not available in this build yet");
+  });
+}
+
+int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    if (!enabled) {
+      sim->det_enabled = false;
+      return;
+    }
+    REQUIRE(sim->det_prepared && sim->order_enabled, MPM_ERR_INVALID,
+            "Deterministic P2G requires prepared gather, active or native dense grid, ordering and no deferred scatter");
+  });
+}
+
+int mpm_prepare_particle_tile_ordering(mpm_sim* sim, uint32_t capacity) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(capacity != 0 && capacity >= sim->count && capacity <= sim->cfg.max_particles, MPM_ERR_INVALID,
+            "MPM particle ordering capacity is invalid");
+    if (sim->order_prepared && sim->order_capacity == capacity) return;
+    REQUIRE(!sim->det_enabled, MPM_ERR_INVALID, "Disable deterministic P2G before replacing particle ordering");
+    sim->order_prepared = true;
+    sim->order_capacity = capacity;
+    sim->invalidate();
+  });
+}
+
+int mpm_set_particle_tile_ordering(mpm_sim* sim, int enabled) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(enabled || !sim->det_enabled, MPM_ERR_INVALID, "Disable deterministic P2G before particle ordering");
+    REQUIRE(!enabled || (sim->order_prepared && sim->order_capacity >= sim->count), MPM_ERR_INVALID,
+            "MPM particle ordering must be prepared for the live count");
+    sim->order_enabled = enabled != 0;
+    sim->apply_group_settings();
+    sim->invalidate();
+  });
+}
+
+int mpm_set_sort_interval(mpm_sim* sim, uint32_t interval) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->sort_interval = interval;
+    sim->apply_group_settings();
+    sim->invalidate();
+  });
+}
+
+static void sim_check_step(mpm_sim* sim, float dt) {
+  REQUIRE(std::isfinite(dt) && dt > 0.f, MPM_ERR_INVALID, "MPM timestep must be finite and positive");
+  REQUIRE(!sim->order_enabled || sim->order_capacity >= sim->count, MPM_ERR_INVALID,
+          "MPM particle count exceeds prepared ordering capacity");
+}
+
+int mpm_step_n(mpm_sim* sim, float dt, uint32_t substeps) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    sim_check_step(sim, dt);
+    if (sim->count == 0 || substeps == 0) return;
+    sim->dt = dt;
+    sim->group->set_scene_dt(sim->sid, dt);
+    sim->group->step(substeps, sim->eng->stream);
+  });
+}
+
+int mpm_prepare_step(mpm_sim* sim, float dt, uint32_t substeps, mpm_prepared** out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    REQUIRE(std::isfinite(dt) && dt > 0.f, MPM_ERR_INVALID, "MPM prepared timestep must be finite and positive");
+    sim_check_step(sim, dt);
+    *out = new mpm_prepared{sim, sim->epoch, dt, substeps};
+  });
+}
+
+int mpm_prepared_destroy(mpm_prepared* prepared) {
+  return guard([&] { delete prepared; });
+}
+
+int mpm_batch_begin(mpm_sim* sim, void* stream, mpm_batch** out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    *out = new mpm_batch{sim, stream ? (cudaStream_t)stream : sim->eng->stream, {}, false};
+  });
+}
+
+int mpm_batch_encode_step(mpm_batch* batch, const mpm_prepared* prepared) {
+  return guard([&] {
+    REQUIRE(batch && prepared, MPM_ERR_INVALID, "null argument");
+    REQUIRE(!batch->done, MPM_ERR_INVALID, "MPM command batch already submitted");
+    REQUIRE(prepared->sim == batch->sim && prepared->epoch == batch->sim->epoch, MPM_ERR_STALE,
+            "MPM prepared step belongs to another simulation or stale configuration");
+    if (batch->sim->count == 0 || prepared->substeps == 0) return;
+    batch->work.emplace_back(prepared->dt, prepared->substeps);
+  });
+}
+
+int mpm_batch_submit(mpm_batch* batch) {
+  int rc = guard([&] {
+    REQUIRE(batch, MPM_ERR_INVALID, "null batch");
+    REQUIRE(!batch->done, MPM_ERR_INVALID, "MPM command batch already submitted");
+    mpm_sim* sim = batch->sim;
+    sim->eng->check();
+    cudaStream_t st = batch->stream;
+    cudaEvent_t ev = nullptr;
+    if (st != sim->eng->stream) {
+      MPM_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      MPM_CK(cudaEventRecord(ev, sim->eng->stream));
+      MPM_CK(cudaStreamWaitEvent(st, ev, 0));
+    }
+    for (const auto& w : batch->work) {
+      sim->dt = w.first;
+      sim->group->set_scene_dt(sim->sid, w.first);
+      sim->group->step_graph(w.second, 1, st);
+    }
+    if (ev) {
+      MPM_CK(cudaEventRecord(ev, st));
+      MPM_CK(cudaStreamWaitEvent(sim->eng->stream, ev, 0));
+      cudaEventDestroy(ev);
+    }
+    batch->done = true;
+  });
+  if (rc == MPM_OK) delete batch;
+  return rc;
+}
+
+int mpm_batch_cancel(mpm_batch* batch) {
+  return guard([&] { delete batch; });
+}
+
+int mpm_read_positions(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    if (count_out) *count_out = sim->count;
+    if (!sim->count || !out || !cap) return;
+    if (cap >= sim->count) {
+      sim->group->read_rows(sim->sid, mpm::PX, 3, out, sim->eng->stream);
+    } else {
+      std::vector<float> tmp(3 * (size_t)sim->count);
+      sim->group->read_rows(sim->sid, mpm::PX, 3, tmp.data(), sim->eng->stream);
+      std::memcpy(out, tmp.data(), 12 * (size_t)cap);
+    }
+  });
+}
+
+int mpm_read_velocities(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    if (count_out) *count_out = sim->count;
+    if (!sim->count || !out || !cap) return;
+    if (cap >= sim->count) {
+      sim->group->read_rows(sim->sid, mpm::VX, 3, out, sim->eng->stream);
+    } else {
+      std::vector<float> tmp(3 * (size_t)sim->count);
+      sim->group->read_rows(sim->sid, mpm::VX, 3, tmp.data(), sim->eng->stream);
+      std::memcpy(out, tmp.data(), 12 * (size_t)cap);
+    }
+  });
+}
+
+int mpm_read_particle_state(mpm_sim* sim, float* C, float* F, float* jp, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    if (count_out) *count_out = sim->count;
+    if (!sim->count) return;
+    REQUIRE(cap >= sim->count, MPM_ERR_INVALID, "output capacity below the particle count");
+    if (C) sim->group->read_rows(sim->sid, mpm::C0, 9, C, sim->eng->stream);
+    if (F) sim->group->read_rows(sim->sid, mpm::F0, 9, F, sim->eng->stream);
+    if (jp) sim->group->read_rows(sim->sid, mpm::JP, 1, jp, sim->eng->stream);
+  });
+}
+
+int mpm_write_particle_state(mpm_sim* sim, const float* C, const float* F, const float* jp, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    REQUIRE(n == sim->count, MPM_ERR_INVALID, "state count must equal the particle count");
+    if (!n) return;
+    if (C) sim->group->write_rows(sim->sid, mpm::C0, 9, C, sim->eng->stream);
+    if (F) sim->group->write_rows(sim->sid, mpm::F0, 9, F, sim->eng->stream);
+    if (jp) sim->group->write_rows(sim->sid, mpm::JP, 1, jp, sim->eng->stream);
+  });
+}
+
+int mpm_read_grid_mass_momentum(mpm_sim* sim, float* mass, float* momentum, size_t cells) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    const uint64_t n3 = (uint64_t)sim->cfg.grid_size * sim->cfg.grid_size * sim->cfg.grid_size;
+    REQUIRE(cells >= n3, MPM_ERR_INVALID, "grid output smaller than grid_size^3");
+    if (sim->sid == 0xffffffffu) {
+      if (mass) std::memset(mass, 0, n3 * 4);
+      if (momentum) std::memset(momentum, 0, n3 * 12);
+      return;
+    }
+    sim->group->read_grid(sim->sid, mass, momentum, sim->eng->stream);
+  });
+}
+
+int mpm_conservation_totals(mpm_sim* sim, double* out8) {
+  return guard([&] {
+    REQUIRE(sim && out8, MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    if (sim->sid == 0xffffffffu) {
+      for (int i = 0; i < 8; ++i) out8[i] = 0.0;
+      return;
+    }
+    sim->group->totals(sim->sid, out8, sim->eng->stream);
+  });
+}
+
+int mpm_read_status(mpm_sim* sim, mpm_status_info* out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    if (sim->sid == 0xffffffffu) {
+      std::memset(out, 0, sizeof(*out));
+      return;
+    }
+    sim->group->status(sim->sid, out, sim->eng->stream);
+  });
+}
+
+int mpm_reset_fault(mpm_sim* sim) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    if (sim->sid != 0xffffffffu) sim->group->reset_status(sim->sid, sim->eng->stream);
+  });
+}
+
+int mpm_read_sort_permutation(mpm_sim* sim, uint32_t* keys, uint32_t* ids, uint32_t capacity) {
+  return guard([&] {
+    REQUIRE(sim && keys && ids, MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    REQUIRE(capacity >= sim->count, MPM_ERR_INVALID, "MPM particle ordering capacity is invalid");
+    if (sim->sid == 0xffffffffu) {
+      for (uint32_t i = 0; i < capacity; ++i) {
+        keys[i] = 0xffffffffu;
+        ids[i] = i;
+      }
+      return;
+    }
+    sim->group->sort_permutation(sim->sid, keys, ids, capacity, sim->eng->stream);
+  });
+}
+
+static void ensure(mpm::DevBuf<uint32_t>& b, size_t n) {
+  if (b.count < n) b.alloc(n);
+}
+
+static void engine_sort(mpm::Engine* e, uint32_t* d_keys, uint32_t* d_vals, uint32_t n, uint32_t key_bits,
+                        cudaStream_t st) {
+  REQUIRE(key_bits >= 1 && key_bits <= 32, MPM_ERR_INVALID, "key_bits must be in 1..=32");
+  ensure(e->sk[0], n);
+  ensure(e->sk[1], n);
+  ensure(e->sv[0], n);
+  ensure(e->sv[1], n);
+  ensure(e->shist, mpm::sort_hist_words(n));
+  uint32_t* ko = nullptr;
+  uint32_t* vo = nullptr;
+  MPM_CK(mpm::radix_sort_pairs(st, d_keys, d_vals, e->sk[0].ptr, e->sk[1].ptr, e->sv[0].ptr, e->sv[1].ptr,
+                               e->shist.ptr, n, (int)key_bits, &ko, &vo, &e->launches));
+  MPM_CK(cudaMemcpyAsync(d_keys, ko, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+  MPM_CK(cudaMemcpyAsync(d_vals, vo, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+}
+
+int mpm_radix_sort_pairs(mpm_engine* engine, uint32_t* keys, uint32_t* values, uint32_t n, uint32_t key_bits) {
+  return guard([&] {
+    REQUIRE(engine && (n == 0 || (keys && values)), MPM_ERR_INVALID, "null argument");
+    mpm::Engine* e = engine->e.get();
+    e->check();
+    if (!n) return;
+    ensure(e->skin, n);
+    ensure(e->svin, n);
+    cudaStream_t st = e->stream;
+    MPM_CK(cudaMemcpyAsync(e->skin.ptr, keys, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    MPM_CK(cudaMemcpyAsync(e->svin.ptr, values, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    engine_sort(e, e->skin.ptr, e->svin.ptr, n, key_bits, st);
+    MPM_CK(cudaMemcpyAsync(keys, e->skin.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    MPM_CK(cudaMemcpyAsync(values, e->svin.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    cudaError_t err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) {
+      e->note_error(err);
+      mpm::throw_cuda(err, "radix sort");
+    }
+  });
+}
+
+int mpm_radix_sort_pairs_device(mpm_engine* engine, uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+                                uint32_t key_bits, void* stream) {
+  return guard([&] {
+    REQUIRE(engine && (n == 0 || (d_keys && d_values)), MPM_ERR_INVALID, "null argument");
+    mpm::Engine* e = engine->e.get();
+    e->check();
+    if (!n) return;
+    engine_sort(e, d_keys, d_values, n, key_bits, stream ? (cudaStream_t)stream : e->stream);
+  });
+}
+
+}  // extern "C"
+
+// ---- groups --------------------------------------------------------------------
+
+struct mpm_group {
+  mpm::Engine* eng;
+  std::unique_ptr<mpm::Group> g;
+};
+
+static std::vector<mpm_rheology> rows_of(const mpm_config& cfg, const mpm_rheology* rows, uint32_t n_rows) {
+  if (rows && n_rows) return std::vector<mpm_rheology>(rows, rows + n_rows);
+  return {cfg.rheology};
+}
+
+extern "C" {
+
+int mpm_group_create(mpm_engine* engine, uint32_t max_scenes, uint64_t max_particles_total, uint64_t max_cells_total,
+                     mpm_group** out) {
+  return guard([&] {
+    REQUIRE(engine && out, MPM_ERR_INVALID, "null argument");
+    engine->e->check();
+    auto* h = new mpm_group();
+    try {
+      h->eng = engine->e.get();
+      h->g.reset(new mpm::Group(h->eng, max_scenes, max_particles_total, max_cells_total));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int mpm_group_destroy(mpm_group* group) {
+  return guard([&] { delete group; });
+}
+
+int mpm_group_add_scene(mpm_group* group, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
+                        const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t* scene_id) {
+  return guard([&] {
+    REQUIRE(group && cfg && scene_id, MPM_ERR_INVALID, "null argument");
+    REQUIRE(n == 0 || xyz, MPM_ERR_INVALID, "null positions");
+    validate_config(*cfg);
+    REQUIRE(std::isfinite(dt) && dt > 0.f, MPM_ERR_INVALID, "MPM timestep must be finite and positive");
+    auto r = rows_of(*cfg, rows, n_rows);
+    REQUIRE(r.size() <= 8, MPM_ERR_INVALID, "MPM scene needs 1..=8 material rows");
+    if (ids_or_null)
+      for (uint32_t i = 0; i < n; ++i)
+        REQUIRE(ids_or_null[i] < r.size(), MPM_ERR_INVALID, "particle material id out of range");
+    *scene_id = group->g->add_scene(*cfg, r, xyz, nullptr, nullptr, nullptr, ids_or_null, n, dt);
+    if (cfg->svd_precision == MPM_SVD_FP64) group->g->svd_fp64 = true;
+  });
+}
+
+int mpm_group_remove_scene(mpm_group* group, uint32_t scene_id) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    group->g->remove_scene(scene_id);
+  });
+}
+
+int mpm_group_step(mpm_group* group, uint32_t substeps) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    group->g->step(substeps, group->eng->stream);
+  });
+}
+
+int mpm_group_step_graph(mpm_group* group, uint32_t substeps, uint32_t repeat) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    group->g->step_graph(substeps, repeat, group->eng->stream);
+  });
+}
+
+int mpm_group_read_positions(mpm_group* group, uint32_t scene_id, float* out, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    REQUIRE(scene_id < group->g->scenes.size() && group->g->scenes[scene_id].live, MPM_ERR_INVALID,
+            "unknown MPM scene");
+    const uint32_t n = group->g->scenes[scene_id].n;
+    if (count_out) *count_out = n;
+    if (!out || !n) return;
+    REQUIRE(cap >= n, MPM_ERR_INVALID, "output capacity below the particle count");
+    group->g->read_rows(scene_id, mpm::PX, 3, out, group->eng->stream);
+  });
+}
+
+int mpm_group_read_status(mpm_group* group, uint32_t scene_id, mpm_status_info* out) {
+  return guard([&] {
+    REQUIRE(group && out, MPM_ERR_INVALID, "null argument");
+    REQUIRE(scene_id < group->g->scenes.size() && group->g->scenes[scene_id].live, MPM_ERR_INVALID,
+            "unknown MPM scene");
+    group->g->status(scene_id, out, group->eng->stream);
+  });
+}
+
+int mpm_group_scene_count(mpm_group* group, uint32_t* count) {
+  return guard([&] {
+    REQUIRE(group && count, MPM_ERR_INVALID, "null argument");
+    *count = group->g->live_scenes();
+  });
+}
+
+int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    if (chunk) {
+      REQUIRE(chunk >= 32 && chunk <= 1u << 16, MPM_ERR_INVALID, "chunk must be in 32..=65536");
+      group->g->chunk = chunk;
+      group->g->need_regroup = true;
+      group->g->items.release();
+      group->g->epoch++;
+      group->g->graphs.clear();
+    }
+    group->g->sort_interval = sort_interval ? sort_interval : 16;
+    // re-size the work list for the new chunk
+    const size_t max_items = (size_t)group->g->cap / group->g->chunk + group->g->key_space + 2;
+    if (group->g->items.count < max_items) group->g->items.alloc(max_items);
+  });
+}
+
+}  // extern "C"
+
+// ---- serving -----------------------------------------------------------------------
+
+namespace {
+struct Ticket {
+  uint64_t id = 0;
+  mpm_config cfg{};
+  std::vector<mpm_rheology> rows;
+  std::vector<float> xyz;
+  std::vector<uint32_t> ids;
+  uint32_t n = 0;
+  float dt = 0.f;
+  uint32_t steps = 0, remaining = 0;
+  uint32_t state = 0;  // 0 queued, 1 running, 2 done
+  uint32_t sid = 0xffffffffu;
+  uint64_t bytes = 0;
+  std::vector<float> result;
+  double t_submit = 0, t_admit = 0;
+};
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+double pct(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);
+  const size_t i = (size_t)pos;
+  const double f = pos - (double)i;
+  return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+}  // namespace
+
+struct mpm_server {
+  mpm::Engine* eng;
+  std::unique_ptr<mpm::Group> g;
+  uint64_t budget = 0;
+  uint64_t resident = 0;
+  std::deque<uint64_t> queue;
+  std::map<uint64_t, Ticket> tickets;
+  uint64_t next_id = 1;
+  uint64_t admitted = 0, completed = 0, particle_steps = 0;
+  std::vector<double> tick_ms, queue_ms;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+extern "C" {
+
+int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t max_scenes, mpm_server** out) {
+  return guard([&] {
+    REQUIRE(engine && out && hbm_budget_bytes > 0, MPM_ERR_INVALID, "invalid argument");
+    engine->e->check();
+    auto* s = new mpm_server();
+    try {
+      s->eng = engine->e.get();
+      s->budget = hbm_budget_bytes;
+      // Split the budget: particle pool (two 27-plane buffers + ids) 60%,
+      // grid pool (three float4 arrays) 40%.
+      const uint64_t per_particle = 2ull * mpm::kPlanes * 4ull + 40ull;
+      const uint64_t particles = std::min<uint64_t>(hbm_budget_bytes / 5 * 3 / per_particle, 0x7fff0000ull);
+      const uint64_t cells = hbm_budget_bytes / 5 * 2 / 48ull;
+      s->g.reset(new mpm::Group(s->eng, std::max<uint32_t>(max_scenes, 1), particles, cells));
+      MPM_CK(cudaEventCreate(&s->e0));
+      MPM_CK(cudaEventCreate(&s->e1));
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+  });
+}
+
+int mpm_server_destroy(mpm_server* server) {
+  return guard([&] {
+    if (!server) return;
+    if (server->e0) cudaEventDestroy(server->e0);
+    if (server->e1) cudaEventDestroy(server->e1);
+    delete server;
+  });
+}
+
+int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
+                      const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t steps,
+                      uint64_t* ticket) {
+  return guard([&] {
+    REQUIRE(server && cfg && ticket && (n == 0 || xyz), MPM_ERR_INVALID, "null argument");
+    validate_config(*cfg);
+    REQUIRE(std::isfinite(dt) && dt > 0.f, MPM_ERR_INVALID, "MPM timestep must be finite and positive");
+    Ticket t;
+    t.id = server->next_id++;
+    t.cfg = *cfg;
+    t.rows = rows_of(*cfg, rows, n_rows);
+    t.xyz.assign(xyz, xyz + 3 * (size_t)n);
+    if (ids_or_null) t.ids.assign(ids_or_null, ids_or_null + n);
+    t.n = n;
+    t.dt = dt;
+    t.steps = t.remaining = steps;
+    const uint64_t n3 = (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
+    t.bytes = (uint64_t)n * (2ull * mpm::kPlanes * 4ull + 40ull) + (n3 + 255) / 256 * 256 * 48ull;
+    REQUIRE(n <= server->g->cap && (n3 + 255) / 256 * 256 <= server->g->cell_cap && t.bytes <= server->budget,
+            MPM_ERR_INVALID, "scene exceeds the server's HBM budget or pools");
+    t.t_submit = now_ms();
+    *ticket = t.id;
+    server->queue.push_back(t.id);
+    server->tickets.emplace(t.id, std::move(t));
+  });
+}
+
+int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tick) {
+  return guard([&] {
+    REQUIRE(server && substeps_per_tick > 0, MPM_ERR_INVALID, "invalid argument");
+    mpm::Group& g = *server->g;
+    for (uint32_t tick = 0; tick < ticks; ++tick) {
+      // admit in arrival order while the budget and pools allow
+      while (!server->queue.empty()) {
+        Ticket& t = server->tickets.at(server->queue.front());
+        if (server->resident + t.bytes > server->budget) break;
+        uint32_t sid = 0;
+        try {
+          sid = g.add_scene(t.cfg, t.rows, t.xyz.data(), nullptr, nullptr, nullptr,
+                            t.ids.empty() ? nullptr : t.ids.data(), t.n, t.dt);
+        } catch (const Error& e) {
+          if (e.code == MPM_ERR_BUSY) break;
+          throw;
+        }
+        if (t.cfg.svd_precision == MPM_SVD_FP64) g.svd_fp64 = true;
+        t.sid = sid;
+        t.state = 1;
+        t.t_admit = now_ms();
+        server->queue_ms.push_back(t.t_admit - t.t_submit);
+        server->resident += t.bytes;
+        server->admitted++;
+        server->queue.pop_front();
+        std::vector<float>().swap(t.xyz);
+      }
+      // step the resident scenes
+      uint32_t len = substeps_per_tick;
+      uint64_t parts = 0;
+      for (auto& kv : server->tickets)
+        if (kv.second.state == 1) {
+          len = std::min(len, std::max<uint32_t>(kv.second.remaining, 1));
+          parts += kv.second.n;
+        }
+      if (parts == 0 && g.live_scenes() == 0) {
+        if (server->queue.empty()) break;
+        continue;
+      }
+      MPM_CK(cudaEventRecord(server->e0, server->eng->stream));
+      g.step_graph(len, 1, server->eng->stream);
+      MPM_CK(cudaEventRecord(server->e1, server->eng->stream));
+      MPM_CK(cudaEventSynchronize(server->e1));
+      float ms = 0.f;
+      MPM_CK(cudaEventElapsedTime(&ms, server->e0, server->e1));
+      server->tick_ms.push_back(ms / (float)len);
+      server->particle_steps += parts * len;
+      // retire finished scenes
+      for (auto& kv : server->tickets) {
+        Ticket& t = kv.second;
+        if (t.state != 1) continue;
+        t.remaining = t.remaining > len ? t.remaining - len : 0;
+        if (t.remaining == 0) {
+          t.result.resize(3 * (size_t)t.n);
+          if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), server->eng->stream);
+          g.remove_scene(t.sid);
+          server->resident -= t.bytes;
+          t.state = 2;
+          server->completed++;
+        }
+      }
+    }
+  });
+}
+
+int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float* positions_out, uint32_t cap,
+                    uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(server && state, MPM_ERR_INVALID, "null argument");
+    auto it = server->tickets.find(ticket);
+    REQUIRE(it != server->tickets.end(), MPM_ERR_INVALID, "unknown ticket");
+    Ticket& t = it->second;
+    *state = t.state;
+    if (count_out) *count_out = t.n;
+    if (t.state == 2 && positions_out) {
+      REQUIRE(cap >= t.n, MPM_ERR_INVALID, "output capacity below the particle count");
+      std::memcpy(positions_out, t.result.data(), 12 * (size_t)t.n);
+    }
+  });
+}
+
+int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out) {
+  return guard([&] {
+    REQUIRE(server && out, MPM_ERR_INVALID, "null argument");
+    out->admitted = server->admitted;
+    out->completed = server->completed;
+    out->resident_scenes = server->g->live_scenes();
+    out->resident_bytes = server->resident;
+    out->particle_steps = server->particle_steps;
+    out->tick_ms_p50 = pct(server->tick_ms, 0.5);
+    out->tick_ms_p99 = pct(server->tick_ms, 0.99);
+    out->queue_ms_p50 = pct(server->queue_ms, 0.5);
+    out->queue_ms_p99 = pct(server->queue_ms, 0.99);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,436 @@
+// mpm_device.cuh — device-side data layout and per-particle physics of the
+// B200 MLS-MPM substep.
+//
+// Layout (HBM):
+//   * particles: a pool of structure-of-arrays planes, one float plane per
+//     scalar (x, y, z, vx, vy, vz, C[9], F[9], mass, volume, jp), each plane
+//     `cap` floats long, so that every per-particle access of a warp is one
+//     coalesced 128-byte transaction.  Matrices are column-major per
+//     particle (plane C0 + 3*col + row), the WGSL mat3x3 order of
+//     crates/molla-solvers/shaders/mpm.wgsl:116-118.  Particles are kept
+//     physically grouped by 4^3 grid tile; `orig` maps a slot to the
+//     particle's identity and `slot_of` maps back.
+//   * grid: per cell one float4 accumulator (mass, momentum xyz), double
+//     buffered, and one float4 velocity (vx, vy, vz, mass) written by the grid
+//     update.  Cells of all scenes of a group live in one pool.
+//   * scenes: one SceneDev record per scene (constants of the substep).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpm {
+
+constexpr int kPlanes = 27;
+enum Plane : int {
+  PX = 0, PY = 1, PZ = 2,
+  VX = 3, VY = 4, VZ = 5,
+  C0 = 6,   // C[col*3+row] in planes 6..14
+  F0 = 15,  // F[col*3+row] in planes 15..23
+  MASS = 24, VOL = 25, JP = 26
+};
+
+constexpr uint32_t kFaultNumerical = 2u;  // mpm.wgsl:229 numerical_fault()
+constexpr uint32_t kStatusWords = 4u;     // [fault bits, completed substeps, spare, spare]
+constexpr int kMaxMaterials = 8;          // MAX_MPM_MATERIALS, mpm.rs:660
+
+// Region of grid nodes a work item accumulates in shared memory: 9^3 nodes
+// starting at 4*tile - 2 along each axis.  A particle whose floor(x) lies in
+// the tile has base = floor(x - 0.5) in [4t-1, 4t+3] and touches nodes
+// [4t-1, 4t+5]; the region leaves one cell of drift on each side for
+// particles that moved since the last regrouping.  Anything further out is
+// deposited with global atomics.
+constexpr int kRegion = 9;
+constexpr int kRegionNodes = kRegion * kRegion * kRegion;
+
+struct MatDev {
+  int32_t rheo;      // 0 sand, 1 snow, 2 viscous (mpm.wgsl:556-557)
+  float mu, lam;     // mpm.wgsl:550-551 (per row when the row overrides E/nu)
+  float kappa;       // (3 lam + 2 mu) / (2 mu), mpm.wgsl:1441
+  float dp_alpha;    // material_row, mpm.rs:665-668
+  float theta_c, theta_s, hardening;
+  float vfac, afac;  // exp(-max(damping,0) dt), mpm.wgsl:1306-1307
+  float pad0, pad1;
+};
+
+struct SceneDev {
+  uint32_t n;        // grid cells per axis
+  uint32_t w;        // tiles per axis, ceil(n/4)
+  uint32_t key_off;  // first key of this scene in the group key space
+  uint32_t status;   // index of this scene's status words
+  uint64_t grid_off; // first cell of this scene in the grid pool
+  float dx, inv_dx;
+  float ox, oy, oz;
+  int32_t winx, winy, winz;
+  float dt, gy, friction;
+  int32_t pad, sticky;
+  float lo[3], hi[3];  // g2p position clamp bounds (mpm.wgsl:1323-1326)
+  uint32_t n_mat;
+  uint32_t id_base;    // first identity of this scene
+  uint32_t n_particles;
+  uint32_t live;       // 0 once the scene was removed (its particles leave at the next regroup)
+  MatDev mat[kMaxMaterials];
+};
+
+// A work item: `count` consecutive particle slots starting at `start`, all
+// belonging to `scene` and regrouped under local tile `tile`.
+struct Item {
+  uint32_t start, count, scene, tile;
+};
+
+// Everything a particle/grid kernel needs, passed by value.
+struct PoolDev {
+  float* planes;        // kPlanes * cap floats
+  uint32_t cap;
+  uint32_t* meta;       // scene << 8 | material id, per slot
+  uint32_t* orig;       // identity per slot
+  uint32_t* keys_by_id; // sort key per identity (written when a regroup is due)
+  float4* acc[2];       // grid accumulators (mass, momentum)
+  float4* vel;          // grid velocity (vx, vy, vz, mass)
+  const SceneDev* scenes;
+  uint32_t* status;     // kStatusWords per scene
+  const Item* items;
+  const uint32_t* n_items;
+};
+
+__device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }
+
+__device__ __forceinline__ bool finitef(float x) {
+  return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u;  // mpm.wgsl:217-219
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 helpers on register arrays, column-major a[3*col+row].
+template <class T>
+__device__ __forceinline__ void matmul(const T* a, const T* b, T* o) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) o[3 * c + r] = a[r] * b[3 * c] + a[3 + r] * b[3 * c + 1] + a[6 + r] * b[3 * c + 2];
+}
+// u * diag(d) * v^T
+template <class T>
+__device__ __forceinline__ void sandwich(const T* u, const T* d, const T* v, T* o) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      o[3 * c + r] = (u[r] * d[0]) * v[c] + (u[3 + r] * d[1]) * v[3 + c] + (u[6 + r] * d[2]) * v[6 + c];
+}
+template <class T>
+__device__ __forceinline__ T det3(const T* a) {
+  // first-column expansion; a[3*col+row]
+  return a[0] * (a[4] * a[8] - a[7] * a[5]) - a[3] * (a[1] * a[8] - a[7] * a[2]) + a[6] * (a[1] * a[5] - a[4] * a[2]);
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric Jacobi SVD of a 3x3 F (F = U diag(s) V^T), the algorithm of
+// mpm.wgsl:365-468: cyclic Jacobi on A = F^T F over (0,1), (0,2), (1,2), at
+// most `sweeps` sweeps, stop when the largest off-diagonal is below `tol`;
+// sigma_i = |F v_i|, u_i = F v_i / sigma_i; sign fixes so det U = det V = +1.
+//
+// The FP32 form keeps the reference's rotation formulas (theta, t, c with
+// IEEE division and square root).  The FP64 form computes the same rotation
+// as t = sgn(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq
+// (algebraically identical to 1/(theta + sgn(theta) sqrt(1 + theta^2))), and
+// replaces double division and square roots by Newton-Raphson refinement of
+// single-precision seeds (two steps each, quadratic convergence from 2^-22
+// to below 2^-52).
+template <class T> struct SvdOut {
+  T u[9], s[3], v[9];
+};
+
+// Newton-Raphson reciprocal: y <- y (2 - x y), seeded from the correctly
+// rounded FP32 reciprocal; falls back to IEEE division outside FP32 range.
+__device__ __forceinline__ double nr_rcp(double x) {
+  const float xf = (float)x;
+  const float y0 = __frcp_rn(xf);
+  if (!(fabsf(y0) < 1.0e37f && fabsf(y0) > 1.0e-37f)) return 1.0 / x;
+  double y = (double)y0;
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+// Newton-Raphson reciprocal square root: y <- y (3 - x y^2) / 2.
+__device__ __forceinline__ double nr_rsqrt(double x) {
+  const float xf = (float)x;
+  if (!(xf > 1.0e-37f && xf < 1.0e37f)) return 1.0 / sqrt(x);
+  double y = (double)rsqrtf(xf);
+  const double h = 0.5 * x;
+  double e = fma(-h * y, y, 0.5);
+  y = fma(y, e, y);
+  e = fma(-h * y, y, 0.5);
+  return fma(y, e, y);
+}
+
+template <class T, int P, int Q>
+__device__ __forceinline__ void jacobi_rot(T (&a)[3][3], T* v, T tol, T& max_off) {
+  constexpr int K = 3 - P - Q;
+  const T apq = a[P][Q];
+  const T aapq = apq < T(0) ? -apq : apq;
+  if (aapq > max_off) max_off = aapq;
+  if (aapq < tol) return;
+  const T app = a[P][P];
+  const T aqq = a[Q][Q];
+  T t, c, s;
+  if constexpr (sizeof(T) == 4) {
+    const T theta = (aqq - app) / (T(2) * apq);
+    if (theta >= T(0)) {
+      t = T(1) / (theta + sqrtf(T(1) + theta * theta));
+    } else {
+      t = T(1) / (theta - sqrtf(T(1) + theta * theta));
+    }
+    c = T(1) / sqrtf(T(1) + t * t);
+    s = t * c;
+  } else {
+    const T d = aqq - app;
+    const T e = T(2) * apq;
+    const T ad = d < T(0) ? -d : d;
+    const T r2 = d * d + e * e;
+    const T hyp = r2 * nr_rsqrt(r2);
+    t = (d >= T(0) ? e : -e) * nr_rcp(ad + hyp);
+    c = nr_rsqrt(T(1) + t * t);
+    s = t * c;
+  }
+  a[P][P] = app - t * apq;
+  a[Q][Q] = aqq + t * apq;
+  a[P][Q] = T(0);
+  a[Q][P] = T(0);
+  {
+    const T akp = a[P][K];
+    const T akq = a[Q][K];
+    const T nkp = c * akp - s * akq;
+    const T nkq = s * akp + c * akq;
+    a[P][K] = nkp;
+    a[Q][K] = nkq;
+    a[K][P] = nkp;
+    a[K][Q] = nkq;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const T vkp = v[3 * P + k];
+    const T vkq = v[3 * Q + k];
+    v[3 * P + k] = c * vkp - s * vkq;
+    v[3 * Q + k] = s * vkp + c * vkq;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sweeps) {
+  // a[col][row] of A = F^T F (symmetric)
+  T a[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      a[c][r] = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
+  T* v = o.v;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? T(1) : T(0);
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    T max_off = T(0);
+    jacobi_rot<T, 0, 1>(a, v, tol, max_off);
+    jacobi_rot<T, 0, 2>(a, v, tol, max_off);
+    jacobi_rot<T, 1, 2>(a, v, tol, max_off);
+    if (max_off < tol) break;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const T x = f[0] * v[3 * i] + f[3] * v[3 * i + 1] + f[6] * v[3 * i + 2];
+    const T y = f[1] * v[3 * i] + f[4] * v[3 * i + 1] + f[7] * v[3 * i + 2];
+    const T z = f[2] * v[3 * i] + f[5] * v[3 * i + 1] + f[8] * v[3 * i + 2];
+    T s;
+    T inv;
+    if constexpr (sizeof(T) == 4) {
+      s = sqrtf(x * x + y * y + z * z);
+    } else {
+      const T q = x * x + y * y + z * z;
+      s = q > T(0) ? q * nr_rsqrt(q) : T(0);
+    }
+    o.s[i] = s;
+    if (s > T(1.0e-12)) {
+      if constexpr (sizeof(T) == 4) {
+        o.u[3 * i] = x / s;
+        o.u[3 * i + 1] = y / s;
+        o.u[3 * i + 2] = z / s;
+      } else {
+        inv = nr_rcp(s);
+        o.u[3 * i] = x * inv;
+        o.u[3 * i + 1] = y * inv;
+        o.u[3 * i + 2] = z * inv;
+      }
+    } else {
+      o.u[3 * i] = i == 0 ? T(1) : T(0);
+      o.u[3 * i + 1] = i == 1 ? T(1) : T(0);
+      o.u[3 * i + 2] = i == 2 ? T(1) : T(0);
+    }
+  }
+  if (det3(o.u) < T(0)) {
+    // flip the column of U with the smallest (signed) sigma
+    const bool m1 = o.s[1] < o.s[0];
+    const T s01 = m1 ? o.s[1] : o.s[0];
+    const bool m2 = o.s[2] < s01;
+    const int mi = m2 ? 2 : (m1 ? 1 : 0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T sg = (i == mi) ? T(-1) : T(1);
+      o.u[3 * i] *= sg;
+      o.u[3 * i + 1] *= sg;
+      o.u[3 * i + 2] *= sg;
+      o.s[i] *= sg;
+    }
+  }
+  if (det3(v) < T(0)) {
+    // flip the column of V with the smallest |sigma|
+    const T a0 = o.s[0] < T(0) ? -o.s[0] : o.s[0];
+    const T a1 = o.s[1] < T(0) ? -o.s[1] : o.s[1];
+    const T a2 = o.s[2] < T(0) ? -o.s[2] : o.s[2];
+    const bool m1 = a1 < a0;
+    const T a01 = m1 ? a1 : a0;
+    const bool m2 = a2 < a01;
+    const int mi = m2 ? 2 : (m1 ? 1 : 0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T sg = (i == mi) ? T(-1) : T(1);
+      v[3 * i] *= sg;
+      v[3 * i + 1] *= sg;
+      v[3 * i + 2] *= sg;
+      o.s[i] *= sg;
+    }
+  }
+}
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+// Quadratic B-spline weights (mpm.wgsl:285-294).
+__device__ __forceinline__ void quad_weights(float fx, float* w) {
+  w[0] = 0.5f * (1.5f - fx) * (1.5f - fx);
+  w[1] = 0.75f - (fx - 1.0f) * (fx - 1.0f);
+  w[2] = 0.5f * (fx - 0.5f) * (fx - 0.5f);
+}
+
+// Fixed-corotated stress from a (U, s, V) decomposition of F, mpm.wgsl:532-599:
+// s_c = clamp(s, 0.1, 10), R = U V^T, J = prod s_c, hardening h by rheology,
+// P = 2 mu h (Fc - R) + lam h (J - 1) cof, S = -dt vol P Fc^T.  Returns
+// B = m C + 4/dx^2 S so that a node at offset d receives w (m v + B d).
+template <class T>
+__device__ __forceinline__ void p2g_affine(const SvdOut<T>& svd, const MatDev& md, float jp, float mass, float vol,
+                                           const float* C, float dt, float inv_dx, float* B) {
+  float u[9], v[9], sc[3];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    u[i] = (float)svd.u[i];
+    v[i] = (float)svd.v[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sc[i] = clampf((float)svd.s[i], 0.1f, 10.0f);
+  float h = 1.0f;
+  if (md.rheo == 1) {
+    h = expf(clampf(-md.hardening * jp, -3.0f, 3.0f));
+  } else if (md.rheo == 0) {
+    h = expf(clampf(jp, -3.0f, 3.0f));
+  }
+  const float mu_h = md.mu * h;
+  const float lam_h = md.lam * h;
+  const float J = sc[0] * sc[1] * sc[2];
+  const float cofd[3] = {sc[1] * sc[2], sc[0] * sc[2], sc[0] * sc[1]};
+  float Fc[9], cof[9];
+  sandwich(u, sc, v, Fc);
+  sandwich(u, cofd, v, cof);
+  const float k1 = 2.0f * mu_h;
+  const float k2 = lam_h * (J - 1.0f);
+  const float k3 = -dt * vol;
+  float P[9];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      // R = U V^T
+      const float Rcr = u[r] * v[c] + u[3 + r] * v[3 + c] + u[6 + r] * v[6 + c];
+      P[3 * c + r] = k3 * (k1 * (Fc[3 * c + r] - Rcr) + k2 * cof[3 * c + r]);
+    }
+  // S = P Fc^T : S[c][r] = sum_k P[k][r] * Fc[k][c]
+  const float four_inv_dx2 = 4.0f * inv_dx * inv_dx;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const float S = P[r] * Fc[c] + P[3 + r] * Fc[3 + c] + P[6 + r] * Fc[6 + c];
+      B[3 * c + r] = mass * C[3 * c + r] + four_inv_dx2 * S;
+    }
+}
+
+// Plasticity return mapping on (U, s, V), mpm.wgsl:1366-1479.  Writes the
+// projected, safety-clamped singular values into s (in place), updates jp.
+// Returns false on a numerical fault.
+template <class T>
+__device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev& md, float& jp) {
+  float s[3] = {(float)svd.s[0], (float)svd.s[1], (float)svd.s[2]};
+  if (!finitef(s[0]) || !finitef(s[1]) || !finitef(s[2])) return false;
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+    if (!finitef((float)svd.u[i]) || !finitef((float)svd.v[i])) return false;
+  T ns[3] = {svd.s[0], svd.s[1], svd.s[2]};
+  float dq = 0.0f;
+  bool jp_replace = false;
+  float jp_new = 0.0f;
+  if (md.rheo == 1) {
+    float nsf[3];
+    const T lo = (T)(1.0f - md.theta_c), hi = (T)(1.0f + md.theta_s);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      T x = svd.s[a];
+      x = x < lo ? lo : x;
+      x = x > hi ? hi : x;
+      ns[a] = x;
+      nsf[a] = (float)x;
+    }
+    const float det_old = fmaxf(s[0] * s[1] * s[2], 1.0e-6f);
+    const float det_new = fmaxf(nsf[0] * nsf[1] * nsf[2], 1.0e-6f);
+    const float dlog = logf(det_old) - logf(det_new);
+    jp_replace = true;
+    jp_new = jp + dlog;
+    if (!finitef(jp_new)) return false;
+    jp_new = clampf(jp_new, -5.0f, 5.0f);
+  } else if (md.rheo == 2) {
+    jp_replace = true;
+    jp_new = 0.0f;
+  } else {
+    float eps[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) eps[a] = logf(fmaxf(s[a], 1.0e-6f));
+    const float tr = eps[0] + eps[1] + eps[2];
+    const float mean = tr / 3.0f;
+    const float dev[3] = {eps[0] - mean, eps[1] - mean, eps[2] - mean};
+    const float dev_norm = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+    if (tr > 0.0f) {
+      ns[0] = ns[1] = ns[2] = T(1);
+      dq = sqrtf(eps[0] * eps[0] + eps[1] * eps[1] + eps[2] * eps[2]);
+    } else if (dev_norm == 0.0f) {
+      // elastic, keep s
+    } else {
+      const float fy = dev_norm + md.kappa * tr * md.dp_alpha;
+      if (fy > 0.0f) {
+        const float rc = fmaxf(0.0f, -md.dp_alpha * md.kappa * tr);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ns[a] = (T)expf(dev[a] * (rc / dev_norm) + mean);
+        dq = fy;
+      }
+    }
+  }
+  if (!finitef((float)ns[0]) || !finitef((float)ns[1]) || !finitef((float)ns[2]) || !finitef(dq) ||
+      !finitef(jp + dq))
+    return false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T x = ns[a];
+    x = x < T(0.05) ? T(0.05) : x;
+    x = x > T(20) ? T(20) : x;
+    svd.s[a] = x;
+  }
+  jp = jp_replace ? jp_new : clampf(jp + dq, 0.0f, 5.0f);
+  return true;
+}
+
+}  // namespace mpm

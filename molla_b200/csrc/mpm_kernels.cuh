@@ -1,0 +1,44 @@
+// mpm_kernels.cuh — host launchers of the substep kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+
+namespace mpm {
+
+constexpr int kParticleThreads = 256;
+constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 256-cell block
+
+enum ParticleMode : int { kP2G = 0, kG2P = 1, kG2P2G = 2 };
+
+cudaError_t launch_particles(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, int acc_out, double tol,
+                             int sweeps, int reuse, int grid, cudaStream_t st);
+// Persistent grid size (SMs x resident CTAs) of a particle-kernel variant.
+int particle_grid_size(int mode, bool write_keys, bool svd_fp64);
+cudaError_t launch_grid_update(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
+                               int count_substep, cudaStream_t st);
+cudaError_t launch_keys(const PoolDev& p, uint32_t n_slots, cudaStream_t st);
+cudaError_t launch_init_particles(const PoolDev& p, uint32_t* slot_of, uint32_t slot0, uint32_t id0, uint32_t n,
+                                  const float* xyz, const float* vel, const float* mass, const float* vol,
+                                  float mass0, float vol0, const uint32_t* mat_ids, uint32_t scene, cudaStream_t st);
+cudaError_t launch_set_material_ids(const PoolDev& p, const uint32_t* slot_of, uint32_t id0, uint32_t n,
+                                    const uint32_t* ids, cudaStream_t st);
+cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* slot_of, uint32_t id0, uint32_t n,
+                              uint32_t* keys, cudaStream_t st);
+cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
+                           uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, uint32_t n_live,
+                           cudaStream_t st);
+cudaError_t launch_items(const uint32_t* sorted_keys, uint32_t n_live, uint32_t K, uint32_t* tile_start,
+                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
+                         Item* items, uint32_t* n_items, cudaStream_t st);
+cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
+                              float* out, cudaStream_t st);
+cudaError_t launch_gather_rows(const PoolDev& p, int first, int count, const uint32_t* slot_of, uint32_t id_base,
+                               uint32_t n, float* out, cudaStream_t st);
+cudaError_t launch_scatter_rows(const PoolDev& p, int first, int count, const uint32_t* slot_of, uint32_t id_base,
+                                uint32_t n, const float* in, cudaStream_t st);
+cudaError_t launch_totals(const PoolDev& p, int acc_idx, uint64_t grid_off, uint64_t cells, const uint32_t* slot_of,
+                          uint32_t id_base, uint32_t n, double* out, cudaStream_t st);
+
+}  // namespace mpm

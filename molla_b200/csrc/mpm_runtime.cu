@@ -1,0 +1,749 @@
+// mpm_runtime.cu — host runtime of the B200 MPM path.
+#include "mpm_runtime.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace mpm {
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what) {
+  throw Error(MPM_ERR_GPU, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+static bool sticky_error(cudaError_t e) {
+  switch (e) {
+    case cudaErrorIllegalAddress:
+    case cudaErrorLaunchFailure:
+    case cudaErrorIllegalInstruction:
+    case cudaErrorMisalignedAddress:
+    case cudaErrorInvalidAddressSpace:
+    case cudaErrorInvalidPc:
+    case cudaErrorHardwareStackError:
+    case cudaErrorAssert:
+    case cudaErrorLaunchTimeout:
+    case cudaErrorECCUncorrectable:
+    case cudaErrorUnknown:
+      return true;
+    default:
+      return false;
+  }
+}
+
+Engine::Engine(int dev) : device(dev) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= 0) {
+    (void)cudaGetLastError();
+    throw Error(MPM_ERR_GPU, "MpmSimulation needs a GPU engine: no CUDA device available");
+  }
+  if (dev < 0 || dev >= count) throw Error(MPM_ERR_INVALID, "CUDA device ordinal out of range");
+  MPM_CK(cudaSetDevice(dev));
+  MPM_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  MPM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+}
+
+Engine::~Engine() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+  for (ProfRec& r : prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+}
+
+cudaEvent_t Engine::take_event() {
+  if (!event_pool.empty()) {
+    cudaEvent_t e = event_pool.back();
+    event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  MPM_CK(cudaEventCreate(&e));
+  return e;
+}
+
+void Engine::prof_begin(int stage, cudaStream_t st, ProfRec* r) {
+  r->stage = -1;
+  if (!profiling || capturing) return;
+  r->stage = stage;
+  r->a = take_event();
+  r->b = take_event();
+  MPM_CK(cudaEventRecord(r->a, st));
+}
+
+void Engine::prof_end(ProfRec* r, cudaStream_t st) {
+  if (r->stage < 0) return;
+  MPM_CK(cudaEventRecord(r->b, st));
+  prof.push_back(*r);
+  if (prof.size() > 4096) prof_resolve();
+}
+
+void Engine::prof_resolve() {
+  for (ProfRec& r : prof) {
+    MPM_CK(cudaEventSynchronize(r.b));
+    float ms = 0.f;
+    MPM_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    prof_ms[r.stage] += ms;
+    prof_count[r.stage] += 1;
+    event_pool.push_back(r.a);
+    event_pool.push_back(r.b);
+  }
+  prof.clear();
+}
+
+void Engine::check() const {
+  if (lost) throw Error(MPM_ERR_GPU, "device lost: " + lost_reason);
+}
+
+void Engine::note_error(cudaError_t e) {
+  if (e != cudaSuccess && sticky_error(e)) {
+    lost = true;
+    lost_reason = cudaGetErrorString(e);
+  }
+}
+
+bool RangeAlloc::alloc(uint64_t len, uint64_t align, uint64_t* off) {
+  if (len == 0) {
+    *off = 0;
+    return true;
+  }
+  for (size_t i = 0; i < free_list.size(); ++i) {
+    Range& r = free_list[i];
+    const uint64_t start = (r.off + align - 1) / align * align;
+    if (start + len <= r.off + r.len) {
+      const uint64_t head = start - r.off;
+      const uint64_t tail = r.off + r.len - (start + len);
+      const Range old = r;
+      free_list.erase(free_list.begin() + (long)i);
+      if (tail) free_list.insert(free_list.begin() + (long)i, {start + len, tail});
+      if (head) free_list.insert(free_list.begin() + (long)i, {old.off, head});
+      *off = start;
+      return true;
+    }
+  }
+  return false;
+}
+
+void RangeAlloc::release(uint64_t off, uint64_t len) {
+  if (!len) return;
+  free_list.push_back({off, len});
+  std::sort(free_list.begin(), free_list.end(), [](const Range& a, const Range& b) { return a.off < b.off; });
+  std::vector<Range> merged;
+  for (const Range& r : free_list) {
+    if (!merged.empty() && merged.back().off + merged.back().len == r.off)
+      merged.back().len += r.len;
+    else
+      merged.push_back(r);
+  }
+  free_list.swap(merged);
+}
+
+uint64_t RangeAlloc::high_water() const {
+  // The free list is sorted and merged; if the last free range reaches the
+  // end, everything after its start is unused.
+  if (!free_list.empty() && free_list.back().off + free_list.back().len == capacity) return free_list.back().off;
+  return capacity;
+}
+
+float dp_alpha_of(float friction_angle) {
+  // material_row (crates/molla-solvers/src/mpm.rs:662-668), f32.
+  const float sin_phi = std::sin(friction_angle);
+  const float two_thirds = 2.0f / 3.0f;
+  return std::sqrt(two_thirds) * (2.0f * sin_phi) / (3.0f - sin_phi);
+}
+
+SceneDev make_scene_dev(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, float dt) {
+  SceneDev d;
+  std::memset(&d, 0, sizeof(d));
+  d.n = cfg.grid_size;
+  d.w = (cfg.grid_size + 3u) / 4u;
+  d.dx = cfg.cell_size;
+  d.inv_dx = 1.0f / cfg.cell_size;  // mpm.rs:2389 inv_cell_size: 1.0 / cell_size in f32
+  d.ox = cfg.grid_origin[0];
+  d.oy = cfg.grid_origin[1];
+  d.oz = cfg.grid_origin[2];
+  d.winx = cfg.grid_window_cells[0];
+  d.winy = cfg.grid_window_cells[1];
+  d.winz = cfg.grid_window_cells[2];
+  d.dt = dt;
+  d.gy = cfg.gravity_y;
+  d.friction = cfg.boundary_friction;
+  d.pad = cfg.boundary_pad ? (int32_t)cfg.boundary_pad : 2;
+  d.sticky = cfg.walls == MPM_WALLS_STICKY ? 1 : 0;
+  const int32_t win[3] = {d.winx, d.winy, d.winz};
+  const float o[3] = {d.ox, d.oy, d.oz};
+  for (int a = 0; a < 3; ++a) {
+    // mpm.wgsl:1323-1326: lo = o + f32(window + pad) * dx, hi = o + f32(window + n - pad - 1) * dx
+    const float flo = (float)(win[a] + d.pad);
+    const float fhi = (float)(win[a] + (int32_t)cfg.grid_size - d.pad - 1);
+    volatile float tlo = flo * d.dx;
+    volatile float thi = fhi * d.dx;
+    d.lo[a] = o[a] + tlo;
+    d.hi[a] = o[a] + thi;
+  }
+  d.n_mat = (uint32_t)rows.size();
+  d.live = 1;
+  for (size_t i = 0; i < rows.size() && i < (size_t)kMaxMaterials; ++i) {
+    const mpm_rheology& r = rows[i];
+    MatDev& m = d.mat[i];
+    const float e = r.youngs > 0.f ? r.youngs : cfg.youngs;
+    const float nu = r.youngs > 0.f ? r.poisson : cfg.poisson;
+    // mpm.wgsl:550-551 (f32)
+    volatile float one_nu = 1.0f + nu;
+    m.mu = e / (2.0f * one_nu);
+    volatile float lam_den = (1.0f + nu) * (1.0f - 2.0f * nu);
+    m.lam = e * nu / lam_den;
+    // mpm.wgsl:1441 kappa = (d * lam + 2 mu) / (2 mu), d = 3
+    volatile float k_num = 3.0f * m.lam + 2.0f * m.mu;
+    m.kappa = k_num / (2.0f * m.mu);
+    m.rheo = (int32_t)r.kind;
+    m.dp_alpha = r.kind == MPM_RHEOLOGY_SAND ? dp_alpha_of(r.friction_angle) : 0.f;
+    m.theta_c = r.kind == MPM_RHEOLOGY_SNOW ? r.theta_c : 0.f;
+    m.theta_s = r.kind == MPM_RHEOLOGY_SNOW ? r.theta_s : 0.f;
+    m.hardening = r.kind == MPM_RHEOLOGY_SNOW ? r.hardening : 0.f;
+    // mpm.wgsl:1306-1307: exp(-max(damping, 0) * dt)
+    const float vd = r.kind == MPM_RHEOLOGY_VISCOUS ? r.velocity_damping : 0.f;
+    const float ad = r.kind == MPM_RHEOLOGY_VISCOUS ? r.affine_damping : 0.f;
+    m.vfac = std::exp(-std::max(vd, 0.0f) * dt);
+    m.afac = std::exp(-std::max(ad, 0.0f) * dt);
+  }
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+
+static uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t cell_cap_)
+    : eng(e), stream(e->stream), max_scenes(std::max<uint32_t>(max_scenes_, 1)) {
+  if (particle_cap > 0x7fffffffull) throw Error(MPM_ERR_INVALID, "particle capacity exceeds 2^31");
+  cap = (uint32_t)std::max<uint64_t>(particle_cap, 1);
+  cell_cap = round_up(std::max<uint64_t>(cell_cap_, 1), kCellBlock);
+  MPM_CK(cudaSetDevice(eng->device));
+  planes[0].alloc((size_t)kPlanes * cap);
+  planes[1].alloc((size_t)kPlanes * cap);
+  for (int i = 0; i < 2; ++i) {
+    meta[i].alloc(cap);
+    orig[i].alloc(cap);
+    ks[i].alloc(cap);
+    vs[i].alloc(cap);
+    acc[i].alloc(cell_cap);
+  }
+  slot_of.alloc(cap);
+  keys_by_id.alloc(cap);
+  hist.alloc(sort_hist_words(cap));
+  vel.alloc(cell_cap);
+  block_scene.alloc(cell_cap / kCellBlock);
+  scenes_d.alloc(max_scenes);
+  status_d.alloc((size_t)kStatusWords * max_scenes);
+  key_offs_d.alloc(max_scenes);
+  scene_ids_d.alloc(max_scenes);
+  n_items.alloc(1);
+  totals_d.alloc(8);
+  MPM_CK(cudaMallocHost((void**)&scenes_h, sizeof(SceneDev) * max_scenes));
+  std::memset(scenes_h, 0, sizeof(SceneDev) * max_scenes);
+  MPM_CK(cudaMemsetAsync(acc[0].ptr, 0, acc[0].bytes(), stream));
+  MPM_CK(cudaMemsetAsync(acc[1].ptr, 0, acc[1].bytes(), stream));
+  MPM_CK(cudaMemsetAsync(vel.ptr, 0, vel.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(keys_by_id.ptr, 0xff, keys_by_id.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(block_scene.ptr, 0xff, block_scene.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(status_d.ptr, 0, status_d.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(n_items.ptr, 0, n_items.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(scenes_d.ptr, 0, scenes_d.bytes(), stream));
+  ids.init(cap);
+  cells.init(cell_cap);
+  grid_p2g = particle_grid_size(kP2G, false, false);
+  grid_g2p = particle_grid_size(kG2P, false, false);
+  grid_g2p2g = particle_grid_size(kG2P2G, false, false);
+  MPM_CK(cudaStreamSynchronize(stream));
+}
+
+Group::~Group() {
+  if (stream) cudaStreamSynchronize(stream);
+  invalidate_graphs();
+  if (scenes_h) cudaFreeHost(scenes_h);
+}
+
+void Group::invalidate_graphs() {
+  for (auto& kv : graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  graphs.clear();
+  ++epoch;
+}
+
+PoolDev Group::pool() const {
+  PoolDev p;
+  p.planes = planes[cur].ptr;
+  p.cap = cap;
+  p.meta = meta[cur].ptr;
+  p.orig = orig[cur].ptr;
+  p.keys_by_id = keys_by_id.ptr;
+  p.acc[0] = acc[0].ptr;
+  p.acc[1] = acc[1].ptr;
+  p.vel = vel.ptr;
+  p.scenes = scenes_d.ptr;
+  p.status = status_d.ptr;
+  p.items = items.ptr;
+  p.n_items = n_items.ptr;
+  return p;
+}
+
+uint32_t Group::live_scenes() const {
+  uint32_t c = 0;
+  for (const SceneHost& s : scenes) c += s.live ? 1u : 0u;
+  return c;
+}
+
+uint64_t Group::resident_bytes() const {
+  uint64_t b = 0;
+  for (const SceneHost& s : scenes)
+    if (s.live) b += (uint64_t)s.n * (2ull * kPlanes * 4ull + 40ull) + s.grid_len * 48ull;
+  return b;
+}
+
+// Recompute key offsets, item capacity and scene records after a change of
+// membership.
+void Group::rebuild_layout() {
+  std::vector<uint32_t> offs, sids;
+  uint64_t k = 0;
+  for (uint32_t i = 0; i < scenes.size(); ++i) {
+    SceneHost& s = scenes[i];
+    if (!s.live) continue;
+    s.key_off = (uint32_t)k;
+    offs.push_back((uint32_t)k);
+    sids.push_back(i);
+    k += s.tiles;
+    if (k >= 0xfffffff0ull) throw Error(MPM_ERR_INVALID, "MPM group key space exceeds 32 bits");
+  }
+  key_space = (uint32_t)k;
+  if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
+  const size_t max_items = (size_t)cap / std::max<uint32_t>(chunk, 1) + key_space + 2;
+  if (items.count < max_items) items.alloc(max_items);
+  if (!offs.empty()) {
+    MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
+    MPM_CK(cudaMemcpyAsync(scene_ids_d.ptr, sids.data(), sids.size() * 4, cudaMemcpyHostToDevice, stream));
+  }
+  for (uint32_t i = 0; i < scenes.size(); ++i) {
+    SceneHost& s = scenes[i];
+    SceneDev d = s.live ? make_scene_dev(s.cfg, s.rows, s.dt) : scenes_h[i];
+    if (s.live) {
+      d.key_off = s.key_off;
+      d.status = i;
+      d.grid_off = s.grid_off;
+      d.id_base = s.id_base;
+      d.n_particles = s.n;
+    } else {
+      d.live = 0;
+    }
+    scenes_h[i] = d;
+  }
+  MPM_CK(cudaStreamSynchronize(stream));  // host staging is rewritten below on the next change
+  scenes_dirty = true;
+  need_regroup = true;
+  invalidate_graphs();
+}
+
+void Group::sync_scenes(cudaStream_t st) {
+  if (!scenes_dirty) return;
+  if (!scenes.empty())
+    MPM_CK(cudaMemcpyAsync(scenes_d.ptr, scenes_h, sizeof(SceneDev) * scenes.size(), cudaMemcpyHostToDevice, st));
+  // The pinned staging may be rewritten by the host after this call; make
+  // the copy complete before returning.
+  MPM_CK(cudaStreamSynchronize(st));
+  scenes_dirty = false;
+}
+
+uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
+                          const float* velp, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
+                          float dt) {
+  eng->check();
+  if (rows.empty() || rows.size() > (size_t)kMaxMaterials)
+    throw Error(MPM_ERR_INVALID, "MPM scene needs 1..=8 material rows");
+  const uint64_t n3 = (uint64_t)cfg.grid_size * cfg.grid_size * cfg.grid_size;
+  uint32_t sid = (uint32_t)scenes.size();
+  for (uint32_t i = 0; i < scenes.size(); ++i)
+    if (!scenes[i].live) {
+      sid = i;
+      break;
+    }
+  if (sid >= max_scenes) throw Error(MPM_ERR_BUSY, "MPM group has no free scene slot");
+  if ((uint64_t)n_live + n > cap) throw Error(MPM_ERR_BUSY, "MPM group particle pool is full");
+  uint64_t id0 = 0, g0 = 0;
+  if (!ids.alloc(n, 1, &id0)) throw Error(MPM_ERR_BUSY, "MPM group identity space is full");
+  const uint64_t glen = round_up(n3, kCellBlock);
+  if (!cells.alloc(glen, kCellBlock, &g0)) {
+    ids.release(id0, n);
+    throw Error(MPM_ERR_BUSY, "MPM group grid pool is full");
+  }
+  if (sid == scenes.size()) scenes.emplace_back();
+  SceneHost& s = scenes[sid];
+  s.live = true;
+  s.cfg = cfg;
+  s.rows = rows;
+  s.dt = dt;
+  s.n = n;
+  s.id_base = (uint32_t)id0;
+  s.grid_off = g0;
+  s.grid_len = glen;
+  const uint32_t w = (cfg.grid_size + 3u) / 4u;
+  s.tiles = w * w * w;
+
+  // upload particles
+  if (n) {
+    DevBuf<float> dx(3 * (size_t)n), dv, dm, dvol;
+    DevBuf<uint32_t> dmat;
+    MPM_CK(cudaMemcpyAsync(dx.ptr, xyz, dx.bytes(), cudaMemcpyHostToDevice, stream));
+    if (velp) {
+      dv.alloc(3 * (size_t)n);
+      MPM_CK(cudaMemcpyAsync(dv.ptr, velp, dv.bytes(), cudaMemcpyHostToDevice, stream));
+    }
+    if (mass) {
+      dm.alloc(n);
+      MPM_CK(cudaMemcpyAsync(dm.ptr, mass, dm.bytes(), cudaMemcpyHostToDevice, stream));
+    }
+    if (vol) {
+      dvol.alloc(n);
+      MPM_CK(cudaMemcpyAsync(dvol.ptr, vol, dvol.bytes(), cudaMemcpyHostToDevice, stream));
+    }
+    if (mat_ids) {
+      dmat.alloc(n);
+      MPM_CK(cudaMemcpyAsync(dmat.ptr, mat_ids, dmat.bytes(), cudaMemcpyHostToDevice, stream));
+    }
+    MPM_CK(launch_init_particles(pool(), slot_of.ptr, n_live, (uint32_t)id0, n, dx.ptr, dv.ptr, dm.ptr, dvol.ptr,
+                                 cfg.particle_mass, cfg.particle_volume, dmat.ptr, sid, stream));
+    eng->launches += 1;
+    MPM_CK(cudaStreamSynchronize(stream));
+  }
+  // fresh grid range and status
+  MPM_CK(cudaMemsetAsync(acc[0].ptr + g0, 0, glen * sizeof(float4), stream));
+  MPM_CK(cudaMemsetAsync(acc[1].ptr + g0, 0, glen * sizeof(float4), stream));
+  MPM_CK(cudaMemsetAsync(vel.ptr + g0, 0, glen * sizeof(float4), stream));
+  {
+    std::vector<uint32_t> bs(glen / kCellBlock, sid);
+    MPM_CK(cudaMemcpyAsync(block_scene.ptr + g0 / kCellBlock, bs.data(), bs.size() * 4, cudaMemcpyHostToDevice,
+                           stream));
+    MPM_CK(cudaStreamSynchronize(stream));
+  }
+  MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, stream));
+  n_live += n;
+  rebuild_layout();
+  return sid;
+}
+
+void Group::remove_scene(uint32_t sid) {
+  if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
+  SceneHost& s = scenes[sid];
+  const uint32_t removed = s.n;
+  s.live = false;
+  rebuild_layout();  // marks the scene record dead, new key offsets
+  // Compact: keys of every pooled particle (dead ones get 0xffffffff), sort,
+  // keep the live prefix.
+  sync_scenes(stream);
+  const uint32_t n_slots = n_live;
+  n_live -= removed;
+  MPM_CK(launch_keys(pool(), n_slots, stream));
+  eng->launches += 1;
+  regroup(false, stream);
+  // Dead identities keep key 0xffffffff for later sorts.
+  MPM_CK(cudaMemsetAsync(keys_by_id.ptr + s.id_base, 0xff, (size_t)s.n * 4, stream));
+  {
+    std::vector<uint32_t> bs(s.grid_len / kCellBlock, 0xffffffffu);
+    MPM_CK(cudaMemcpyAsync(block_scene.ptr + s.grid_off / kCellBlock, bs.data(), bs.size() * 4,
+                           cudaMemcpyHostToDevice, stream));
+    MPM_CK(cudaStreamSynchronize(stream));
+  }
+  ids.release(s.id_base, s.n);
+  cells.release(s.grid_off, s.grid_len);
+  s.n = 0;
+  need_regroup = n_live > 0;
+}
+
+void Group::set_scene_dt(uint32_t sid, float dt) {
+  SceneHost& s = scenes.at(sid);
+  if (s.dt == dt) return;
+  s.dt = dt;
+  SceneDev d = make_scene_dev(s.cfg, s.rows, dt);
+  d.key_off = s.key_off;
+  d.status = sid;
+  d.grid_off = s.grid_off;
+  d.id_base = s.id_base;
+  d.n_particles = s.n;
+  scenes_h[sid] = d;
+  scenes_dirty = true;
+}
+
+void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) {
+  SceneHost& s = scenes.at(sid);
+  s.rows = rows;
+  const float dt = s.dt;
+  s.dt = -1.f;
+  set_scene_dt(sid, dt);
+}
+
+void Group::set_scene_cfg(uint32_t sid, const mpm_config& cfg) {
+  SceneHost& s = scenes.at(sid);
+  s.cfg = cfg;
+  const float dt = s.dt;
+  s.dt = -1.f;
+  set_scene_dt(sid, dt);
+}
+
+void Group::set_material_ids(uint32_t sid, const uint32_t* host_ids, uint32_t n) {
+  SceneHost& s = scenes.at(sid);
+  if (n != s.n) throw Error(MPM_ERR_INVALID, "material id count does not match the particle count");
+  if (!n) return;
+  DevBuf<uint32_t> d(n);
+  MPM_CK(cudaMemcpyAsync(d.ptr, host_ids, d.bytes(), cudaMemcpyHostToDevice, stream));
+  MPM_CK(launch_set_material_ids(pool(), slot_of.ptr, s.id_base, n, d.ptr, stream));
+  eng->launches += 1;
+  MPM_CK(cudaStreamSynchronize(stream));
+}
+
+static int bits_for(uint64_t values) {
+  // smallest b with values < 2^b - 1 (so that the all-ones pattern of b bits
+  // is free for removed particles)
+  int b = 1;
+  while (b < 32 && ((1ull << b) - 1ull) <= values) ++b;
+  return b;
+}
+
+void Group::regroup(bool compute_keys, cudaStream_t st) {
+  ProfRec pr;
+  eng->prof_begin(kStageOrdering, st, &pr);
+  if (compute_keys) {
+    MPM_CK(launch_keys(pool(), n_live, st));
+    eng->launches += 1;
+  }
+  const uint32_t n_sort = (uint32_t)ids.high_water();
+  uint32_t* skeys = nullptr;
+  uint32_t* sids = nullptr;
+  MPM_CK(radix_sort_pairs(st, keys_by_id.ptr, nullptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n_sort,
+                          bits_for(key_space), &skeys, &sids, &eng->launches));
+  MPM_CK(launch_reorder(planes[cur].ptr, planes[cur ^ 1].ptr, cap, meta[cur].ptr, meta[cur ^ 1].ptr,
+                        orig[cur ^ 1].ptr, slot_of.ptr, sids, n_live, st));
+  eng->launches += 1;
+  cur ^= 1;
+  MPM_CK(launch_items(skeys, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(), scene_ids_d.ptr,
+                      chunk, items.ptr, n_items.ptr, st));
+  eng->launches += key_space ? 2 : 1;
+  need_regroup = false;
+  eng->prof_end(&pr, st);
+}
+
+void Group::launch_pass(int mode, bool keys, int acc_out, cudaStream_t st) {
+  const int grid = mode == kP2G ? grid_p2g : (mode == kG2P ? grid_g2p : grid_g2p2g);
+  const double tol = svd_fp64 ? svd_tol64 : svd_tol32;
+  ProfRec pr;
+  eng->prof_begin(mode == kP2G ? kStageP2G : (mode == kG2P ? kStageG2P : kStageG2P2G), st, &pr);
+  MPM_CK(launch_particles(mode, keys, svd_fp64, pool(), acc_out, tol, svd_sweeps, reuse_svd ? 1 : 0, grid, st));
+  eng->prof_end(&pr, st);
+  eng->launches += 1;
+}
+
+void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
+  if (need_regroup) regroup(true, st);
+  launch_pass(kP2G, false, acc_zero, st);
+  int a = acc_zero;
+  const uint64_t total_cells = cells.high_water();
+  uint32_t since = 0;
+  for (uint32_t s = 0; s < substeps; ++s) {
+    ProfRec pr;
+    eng->prof_begin(kStageGrid, st, &pr);
+    MPM_CK(launch_grid_update(pool(), block_scene.ptr, total_cells, a, 1, st));
+    eng->prof_end(&pr, st);
+    eng->launches += 1;
+    const bool last = s + 1 == substeps;
+    const bool due = !last && sort_interval > 0 && ++since >= sort_interval;
+    launch_pass(last ? kG2P : kG2P2G, due, a ^ 1, st);
+    if (due) {
+      regroup(false, st);
+      since = 0;
+    }
+    if (!last) a ^= 1;
+  }
+  acc_last = a;
+  acc_zero = a ^ 1;
+  substeps_done += substeps;
+}
+
+void Group::step(uint32_t substeps, cudaStream_t st) {
+  eng->check();
+  if (!substeps || !n_live) return;
+  sync_scenes(st);
+  run_substeps(substeps, st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    eng->note_error(e);
+    throw_cuda(e, "MPM step launch");
+  }
+}
+
+uint64_t Group::graph_key(uint32_t substeps) const {
+  return ((uint64_t)substeps << 8) | ((uint64_t)cur << 2) | ((uint64_t)acc_zero << 1) | (need_regroup ? 1u : 0u);
+}
+
+void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
+  eng->check();
+  if (!substeps || !n_live || !repeat) return;
+  sync_scenes(st);
+  for (uint32_t r = 0; r < repeat; ++r) {
+    const uint64_t key = graph_key(substeps);
+    const int cur0 = cur, az0 = acc_zero;
+    const bool nr0 = need_regroup;
+    auto it = graphs.find(key);
+    Graph g;
+    if (it == graphs.end() || it->second.epoch != epoch) {
+      const uint64_t saved = eng->launches;
+      cudaGraph_t graph = nullptr;
+      MPM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      eng->capturing = true;
+      try {
+        run_substeps(substeps, st);
+      } catch (...) {
+        eng->capturing = false;
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      eng->capturing = false;
+      MPM_CK(cudaStreamEndCapture(st, &graph));
+      g.kernels = eng->launches - saved;
+      eng->launches = saved;
+      MPM_CK(cudaGraphInstantiate(&g.exec, graph, 0));
+      cudaGraphDestroy(graph);
+      g.epoch = epoch;
+      // run_substeps advanced the host bookkeeping; rewind it, the launch
+      // below applies the same transition.
+      const int cur1 = cur, az1 = acc_zero, al1 = acc_last;
+      cur = cur0;
+      acc_zero = az0;
+      need_regroup = nr0;
+      substeps_done -= substeps;
+      if (it != graphs.end() && it->second.exec) cudaGraphExecDestroy(it->second.exec);
+      graphs[key] = g;
+      (void)cur1;
+      (void)az1;
+      (void)al1;
+    } else {
+      g = it->second;
+    }
+    MPM_CK(cudaGraphLaunch(g.exec, st));
+    eng->launches += g.kernels;
+    // Replay the host-side state transition of the captured sequence.
+    uint32_t since = 0;
+    if (need_regroup) {
+      cur ^= 1;
+      need_regroup = false;
+    }
+    int a = acc_zero;
+    for (uint32_t s = 0; s < substeps; ++s) {
+      const bool last = s + 1 == substeps;
+      const bool due = !last && sort_interval > 0 && ++since >= sort_interval;
+      if (due) {
+        cur ^= 1;
+        since = 0;
+      }
+      if (!last) a ^= 1;
+    }
+    acc_last = a;
+    acc_zero = a ^ 1;
+    substeps_done += substeps;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    eng->note_error(e);
+    throw_cuda(e, "MPM graph launch");
+  }
+}
+
+void Group::read_rows(uint32_t sid, int first, int count, float* out, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  if (!s.n) return;
+  DevBuf<float> d((size_t)count * s.n);
+  if (count == 3)
+    MPM_CK(launch_gather_xyz(pool(), first, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+  else
+    MPM_CK(launch_gather_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+  eng->launches += 1;
+  MPM_CK(cudaMemcpyAsync(out, d.ptr, d.bytes(), cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
+void Group::write_rows(uint32_t sid, int first, int count, const float* in, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  if (!s.n) return;
+  DevBuf<float> d((size_t)count * s.n);
+  MPM_CK(cudaMemcpyAsync(d.ptr, in, d.bytes(), cudaMemcpyHostToDevice, st));
+  MPM_CK(launch_scatter_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+  eng->launches += 1;
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
+void Group::read_grid(uint32_t sid, float* mass, float* mom, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  const uint64_t n3 = (uint64_t)s.cfg.grid_size * s.cfg.grid_size * s.cfg.grid_size;
+  std::vector<float4> h(n3);
+  MPM_CK(cudaMemcpyAsync(h.data(), acc[acc_last].ptr + s.grid_off, n3 * sizeof(float4), cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  for (uint64_t i = 0; i < n3; ++i) {
+    if (mass) mass[i] = h[i].x;
+    if (mom) {
+      mom[3 * i] = h[i].y;
+      mom[3 * i + 1] = h[i].z;
+      mom[3 * i + 2] = h[i].w;
+    }
+  }
+}
+
+void Group::totals(uint32_t sid, double* out8, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  const uint64_t n3 = (uint64_t)s.cfg.grid_size * s.cfg.grid_size * s.cfg.grid_size;
+  MPM_CK(launch_totals(pool(), acc_last, s.grid_off, n3, slot_of.ptr, s.id_base, s.n, totals_d.ptr, st));
+  eng->launches += 1;
+  MPM_CK(cudaMemcpyAsync(out8, totals_d.ptr, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
+void Group::status(uint32_t sid, mpm_status_info* out, cudaStream_t st) {
+  uint32_t w[kStatusWords];
+  MPM_CK(cudaMemcpyAsync(w, status_d.ptr + (size_t)sid * kStatusWords, sizeof(w), cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  out->fault_bits = w[0];
+  out->numerical_fault = (w[0] & kFaultNumerical) ? 1u : 0u;
+  out->completed_substeps = w[1];
+  out->reserved = 0;
+}
+
+void Group::reset_status(uint32_t sid, cudaStream_t st) {
+  MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, st));
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
+void Group::sort_permutation(uint32_t sid, uint32_t* keys_out, uint32_t* ids_out, uint32_t capacity,
+                             cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  sync_scenes(st);
+  const uint32_t n = s.n;
+  if (n) {
+    DevBuf<uint32_t> kin(n);
+    MPM_CK(launch_scene_keys(pool(), sid, slot_of.ptr, s.id_base, n, kin.ptr, st));
+    eng->launches += 1;
+    uint32_t* sk = nullptr;
+    uint32_t* sv = nullptr;
+    MPM_CK(radix_sort_pairs(st, kin.ptr, nullptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n,
+                            bits_for(s.tiles), &sk, &sv, &eng->launches));
+    MPM_CK(cudaMemcpyAsync(keys_out, sk, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    MPM_CK(cudaMemcpyAsync(ids_out, sv, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    MPM_CK(cudaStreamSynchronize(st));
+  }
+  for (uint32_t i = n; i < capacity; ++i) {
+    keys_out[i] = 0xffffffffu;
+    ids_out[i] = i;
+  }
+}
+
+}  // namespace mpm

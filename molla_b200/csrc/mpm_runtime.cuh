@@ -1,0 +1,232 @@
+// mpm_runtime.cuh — host runtime of the B200 MPM path: engine, scene group
+// (pooled particles and grid, regrouping sort, substep sequencing, CUDA-graph
+// replay) and the error channel of the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/molla_mpm.h"
+#include "mpm_device.cuh"
+#include "mpm_kernels.cuh"
+#include "mpm_sort.cuh"
+
+namespace mpm {
+
+// Error carried to the C ABI: code + message (molla_core::Error's Display).
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what);
+#define MPM_CK(expr)                                   \
+  do {                                                 \
+    cudaError_t _e = (expr);                           \
+    if (_e != cudaSuccess) ::mpm::throw_cuda(_e, #expr); \
+  } while (0)
+
+// Owned device allocation.
+template <class T> struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t n) { alloc(n); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void alloc(size_t n) {
+    release();
+    if (n) {
+      cudaError_t e = cudaMalloc((void**)&ptr, n * sizeof(T));
+      if (e != cudaSuccess) {
+        ptr = nullptr;
+        (void)cudaGetLastError();
+        throw Error(MPM_ERR_NOMEM, std::string("device allocation of ") + std::to_string(n * sizeof(T)) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+      }
+    }
+    count = n;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+// Per-stage GPU timing (the equivalent of molla's MpmProfileStage timestamp
+// queries, crates/molla-solvers/src/mpm_profile.rs:8-80): when enabled, each
+// launch of a stage is bracketed by CUDA events on the launching stream.
+enum Stage : int { kStageOrdering = 0, kStageP2G = 1, kStageGrid = 2, kStageG2P2G = 3, kStageG2P = 4, kStages = 5 };
+
+struct ProfRec {
+  int stage;
+  cudaEvent_t a, b;
+};
+
+struct Engine {
+  int device = 0;
+  bool profiling = false;
+  bool capturing = false;
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> event_pool;
+  double prof_ms[kStages] = {0, 0, 0, 0, 0};
+  uint64_t prof_count[kStages] = {0, 0, 0, 0, 0};
+  cudaEvent_t take_event();
+  void prof_begin(int stage, cudaStream_t st, ProfRec* r);
+  void prof_end(ProfRec* r, cudaStream_t st);
+  void prof_resolve();
+  cudaStream_t stream = nullptr;
+  bool lost = false;
+  std::string lost_reason;
+  uint64_t launches = 0;
+  int sms = 148;
+  // scratch of the generic sort entry points
+  DevBuf<uint32_t> sk[2], sv[2], shist, skin, svin;
+  explicit Engine(int dev);
+  ~Engine();
+  void check() const;
+  void note_error(cudaError_t e);
+};
+
+// Host-side description of one scene in a group.
+struct SceneHost {
+  bool live = false;
+  mpm_config cfg{};
+  std::vector<mpm_rheology> rows;  // material table (>= 1 row)
+  float dt = 0.f;
+  uint32_t n = 0;          // particles
+  uint32_t id_base = 0;    // identity range
+  uint64_t grid_off = 0;   // grid pool range
+  uint64_t grid_len = 0;
+  uint32_t key_off = 0;
+  uint32_t tiles = 0;      // w^3
+};
+
+struct Range {
+  uint64_t off, len;
+};
+
+// First-fit range allocator over [0, capacity).
+struct RangeAlloc {
+  uint64_t capacity = 0;
+  std::vector<Range> free_list;
+  void init(uint64_t cap) {
+    capacity = cap;
+    free_list.clear();
+    if (cap) free_list.push_back({0, cap});
+  }
+  bool alloc(uint64_t len, uint64_t align, uint64_t* off);
+  void release(uint64_t off, uint64_t len);
+  uint64_t high_water() const;  // one past the last allocated unit
+};
+
+// Build the device record of a scene from its configuration (f32 constants
+// computed exactly as the reference host/shader do, see mpm_runtime.cu).
+SceneDev make_scene_dev(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, float dt);
+float dp_alpha_of(float friction_angle);
+
+// A group of independent scenes stepped by shared launches.
+class Group {
+ public:
+  Group(Engine* e, uint32_t max_scenes, uint64_t particle_cap, uint64_t cell_cap);
+  ~Group();
+
+  Engine* eng;
+  cudaStream_t stream;
+
+  // capacities
+  uint32_t max_scenes;
+  uint32_t cap;           // particle slots == identity space
+  uint64_t cell_cap;
+
+  // particle pool (double-buffered for the regroup)
+  DevBuf<float> planes[2];
+  DevBuf<uint32_t> meta[2], orig[2];
+  DevBuf<uint32_t> slot_of, keys_by_id, ks[2], vs[2], hist;
+  // grid pool
+  DevBuf<float4> acc[2], vel;
+  DevBuf<uint32_t> block_scene;
+  // scenes
+  DevBuf<SceneDev> scenes_d;
+  DevBuf<uint32_t> status_d;
+  DevBuf<uint32_t> tile_start, key_offs_d, scene_ids_d, n_items;
+  DevBuf<Item> items;
+  DevBuf<double> totals_d;
+  // pinned staging of scene records
+  SceneDev* scenes_h = nullptr;
+
+  std::vector<SceneHost> scenes;
+  RangeAlloc ids, cells;
+  uint32_t n_live = 0;
+  uint32_t key_space = 0;
+  int cur = 0;       // current particle buffer
+  int acc_zero = 0;  // accumulator known to be all zero
+  int acc_last = 1;  // accumulator holding the last scatter
+  bool need_regroup = true;
+  bool scenes_dirty = true;
+  bool keys_dirty = true;  // scene key offsets changed
+  uint32_t sort_interval = 16;
+  uint32_t chunk = 512;
+  bool svd_fp64 = false;
+  bool reuse_svd = true;
+  double svd_tol32 = 1.0e-7;
+  double svd_tol64 = 1.0e-9;
+  int svd_sweeps = 16;
+  int grid_p2g = 0, grid_g2p = 0, grid_g2p2g = 0;
+  uint64_t substeps_done = 0;
+  uint64_t epoch = 1;  // bumps on every change that invalidates captured graphs
+
+  // graph cache: key -> instantiated graph + its kernel count
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    uint64_t epoch = 0;
+  };
+  std::map<uint64_t, Graph> graphs;
+
+  uint32_t add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
+                     const float* vel, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
+                     float dt);
+  void remove_scene(uint32_t sid);
+  void set_scene_dt(uint32_t sid, float dt);
+  void set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows);
+  void set_scene_cfg(uint32_t sid, const mpm_config& cfg);
+  void set_material_ids(uint32_t sid, const uint32_t* ids, uint32_t n);
+
+  // Enqueue `substeps` substeps of every live scene on `st`.
+  void step(uint32_t substeps, cudaStream_t st);
+  // Same through a cached CUDA graph.
+  void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st);
+  void regroup(bool compute_keys, cudaStream_t st);
+  void sync_scenes(cudaStream_t st);
+
+  PoolDev pool() const;
+  void read_rows(uint32_t sid, int first, int count, float* out, cudaStream_t st);
+  void write_rows(uint32_t sid, int first, int count, const float* in, cudaStream_t st);
+  void read_grid(uint32_t sid, float* mass, float* mom, cudaStream_t st);
+  void totals(uint32_t sid, double* out8, cudaStream_t st);
+  void status(uint32_t sid, mpm_status_info* out, cudaStream_t st);
+  void reset_status(uint32_t sid, cudaStream_t st);
+  // (key, identity) order of one scene's particles (reference permutation).
+  void sort_permutation(uint32_t sid, uint32_t* keys, uint32_t* ids, uint32_t capacity, cudaStream_t st);
+  uint64_t resident_bytes() const;
+  uint32_t live_scenes() const;
+
+ private:
+  void rebuild_layout();
+  void invalidate_graphs();
+  void launch_pass(int mode, bool keys, int acc_out, cudaStream_t st);
+  void run_substeps(uint32_t substeps, cudaStream_t st);
+  uint64_t graph_key(uint32_t substeps) const;
+};
+
+}  // namespace mpm

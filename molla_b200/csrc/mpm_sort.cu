@@ -1,0 +1,206 @@
+// mpm_sort.cu — stable LSD radix sort of (u32 key, u32 value) pairs.
+//
+// Replaces RadixSortKernel / RadixSortDispatch
+// (crates/molla-compute-primitives/src/radix_sort.rs:50-110, WGSL
+// count_block_bins / scan_global_bins / scatter, radix_sort.wgsl:100-261).
+// Same contract: ascending by key, ties keep input order (stable), so the
+// output equals a host stable sort of the pairs.  Differences are of
+// design, not of result:
+//   * only ceil(key_bits / 8) passes run (the upper digits of tile keys are
+//     zero, so skipping them leaves the permutation unchanged);
+//   * each pass is three kernels: a per-tile digit histogram with
+//     warp-aggregated shared-memory counts, a per-digit scan of the tile
+//     counts (one CTA per digit), and a scatter that ranks keys stably
+//     inside the tile with __match_any_sync and a per-warp prefix;
+//   * pass 0 can generate the identity values (0..n-1) itself.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_sort.cuh"
+
+namespace mpm {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRounds = kSortTile / kThreads;  // 16
+constexpr int kBins = 256;
+
+__global__ void __launch_bounds__(kThreads) k_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
+                                                   uint32_t nblocks, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_h[kBins + 1];
+  const int tid = threadIdx.x;
+  s_h[tid] = 0;
+  if (tid == 0) s_h[kBins] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+  const int lane = tid & 31;
+#pragma unroll 4
+  for (int r = 0; r < kRounds; ++r) {
+    const uint64_t idx = base + (uint64_t)r * kThreads + tid;
+    const uint32_t d = idx < n ? (keys[idx] >> shift) & 0xffu : (uint32_t)kBins;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (lane == __ffs(peers) - 1 && d < (uint32_t)kBins) atomicAdd(&s_h[d], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  hist[(size_t)tid * nblocks + blockIdx.x] = s_h[tid];
+}
+
+// One CTA per digit: exclusive scan of hist[d][0..nblocks) in place, total to
+// totals[d].
+__global__ void __launch_bounds__(1024) k_scan_digit(uint32_t* __restrict__ hist, uint32_t nblocks,
+                                                     uint32_t* __restrict__ totals) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_carry;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  uint32_t* row = hist + (size_t)blockIdx.x * nblocks;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < nblocks; base += 1024) {
+    const uint32_t i = base + tid;
+    const uint32_t x = i < nblocks ? row[i] : 0u;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t carry = s_carry;
+    const uint32_t excl = carry + (warp ? s_warp[warp - 1] : 0u) + inc - x;
+    if (i < nblocks) row[i] = excl;
+    __syncthreads();
+    if (tid == 0) s_carry = carry + s_warp[31];
+    __syncthreads();
+  }
+  if (tid == 0) totals[blockIdx.x] = s_carry;
+}
+
+__global__ void __launch_bounds__(kThreads) k_scatter(const uint32_t* __restrict__ keys_in,
+                                                      const uint32_t* __restrict__ vals_in, int iota,
+                                                      uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+                                                      uint32_t n, int shift, uint32_t nblocks,
+                                                      const uint32_t* __restrict__ hist,
+                                                      const uint32_t* __restrict__ totals) {
+  __shared__ uint32_t s_base[kBins];           // global base of each digit for this tile
+  __shared__ uint32_t s_cnt[kWarps][kBins];    // per-warp digit counts of the current round
+  __shared__ uint32_t s_pre[kWarps][kBins];    // per-warp digit prefix of the current round
+  __shared__ uint32_t s_wsum[kWarps];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+
+  // Exclusive scan of the digit totals (256 values) -> digit base.
+  {
+    const uint32_t x = totals[tid];
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    uint32_t off = 0;
+    for (int w = 0; w < warp; ++w) off += s_wsum[w];
+    s_base[tid] = off + inc - x + hist[(size_t)tid * nblocks + blockIdx.x];
+  }
+  for (int w = 0; w < kWarps; ++w) s_cnt[w][tid] = 0;
+  __syncthreads();
+
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int r = 0; r < kRounds; ++r) {
+    const uint64_t idx = base + (uint64_t)r * kThreads + tid;
+    const bool valid = idx < n;
+    uint32_t key = 0, val = 0, d = kBins;
+    if (valid) {
+      key = keys_in[idx];
+      val = iota ? (uint32_t)idx : vals_in[idx];
+      d = (key >> shift) & 0xffu;
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t lrank = __popc(peers & lt);
+    if (valid && lrank == 0) s_cnt[warp][d] = __popc(peers);
+    __syncthreads();
+    {
+      // Thread tid owns digit tid: prefix of the per-warp counts in warp
+      // order (warp w holds earlier keys than warp w+1 in this round).  The
+      // round total is parked in s_cnt[0][tid] until the base is advanced.
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = s_cnt[w][tid];
+        s_pre[w][tid] = run;
+        run += c;
+        s_cnt[w][tid] = 0;
+      }
+      s_cnt[0][tid] = run;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t pos = s_base[d] + s_pre[warp][d] + lrank;
+      keys_out[pos] = key;
+      vals_out[pos] = val;
+    }
+    __syncthreads();
+    s_base[tid] += s_cnt[0][tid];
+    s_cnt[0][tid] = 0;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+uint32_t sort_blocks(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+size_t sort_hist_words(uint32_t n) { return (size_t)kBins * (sort_blocks(n) ? sort_blocks(n) : 1) + kBins; }
+
+cudaError_t radix_sort_pairs(cudaStream_t stream, const uint32_t* keys_in, const uint32_t* vals_in,
+                             uint32_t* keys_a, uint32_t* keys_b, uint32_t* vals_a, uint32_t* vals_b, uint32_t* hist,
+                             uint32_t n, int key_bits, uint32_t** keys_out, uint32_t** vals_out, uint64_t* launches) {
+  if (key_bits < 1) key_bits = 1;
+  if (key_bits > 32) key_bits = 32;
+  const int passes = (key_bits + 7) / 8;
+  const uint32_t nblocks = sort_blocks(n);
+  uint32_t* totals = hist + (size_t)kBins * (nblocks ? nblocks : 1);
+  if (n == 0) {
+    *keys_out = keys_a;
+    *vals_out = vals_a;
+    return cudaSuccess;
+  }
+  const uint32_t* kin = keys_in;
+  const uint32_t* vin = vals_in;
+  int iota = vals_in == nullptr ? 1 : 0;
+  uint32_t* kout = keys_a;
+  uint32_t* vout = vals_a;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    kout = (p % 2 == 0) ? keys_a : keys_b;
+    vout = (p % 2 == 0) ? vals_a : vals_b;
+    k_hist<<<nblocks, kThreads, 0, stream>>>(kin, n, shift, nblocks, hist);
+    k_scan_digit<<<kBins, 1024, 0, stream>>>(hist, nblocks, totals);
+    k_scatter<<<nblocks, kThreads, 0, stream>>>(kin, vin, iota, kout, vout, n, shift, nblocks, hist, totals);
+    if (launches) *launches += 3;
+    kin = kout;
+    vin = vout;
+    iota = 0;
+  }
+  *keys_out = kout;
+  *vals_out = vout;
+  return cudaGetLastError();
+}
+
+}  // namespace mpm

@@ -1,0 +1,91 @@
+"""CPU checks of the C ABI: the library loads, exports every declared symbol,
+and its host-side logic (presets, material constants, argument validation,
+errors) behaves like the reference without touching a GPU."""
+
+import ctypes
+import math
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import molla_b200 as m
+from molla_b200 import _ffi
+from oracle import oracle as O
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "molla_mpm.h").read_text()
+    return sorted(set(re.findall(r"^MPM_API\s+[\w\s\*]+?\b(mpm_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(str(_ffi.LIB_PATH))
+    syms = declared_symbols()
+    assert len(syms) >= 50
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    # and the Python binding covers them all
+    assert set(syms) == set(_ffi.SIGNATURES), set(syms) ^ set(_ffi.SIGNATURES)
+
+
+def test_abi_version_and_error_channel():
+    L = _ffi.lib()
+    assert L.mpm_abi_version() == 1
+    rc = L.mpm_sim_destroy(None)
+    assert rc == 0
+    c = _ffi.mpm_config()
+    assert L.mpm_config_preset(99, ctypes.byref(c)) == _ffi.MPM_ERR_INVALID
+    assert "preset" in _ffi.last_error()
+
+
+def test_presets_match_reference():
+    sand = m.MpmConfig.sand()  # mpm.rs:540-560
+    assert sand.grid_size == 32 and math.isclose(sand.cell_size, 0.05, rel_tol=1e-7)
+    assert math.isclose(sand.youngs, 5e3) and math.isclose(sand.poisson, 0.3, rel_tol=1e-7)
+    assert sand.rheology.kind == 0 and math.isclose(sand.rheology.friction_angle, math.radians(30), rel_tol=1e-6)
+    snow = m.MpmConfig.snow()  # mpm.rs:609-631
+    assert snow.rheology.kind == 1 and math.isclose(snow.rheology.theta_c, 0.025, rel_tol=1e-6)
+    assert math.isclose(snow.rheology.hardening, 10.0) and math.isclose(snow.youngs, 1.4e5)
+    visc = m.MpmConfig.viscous()  # mpm.rs:637-655
+    assert visc.rheology.kind == 2 and visc.rheology.velocity_damping == 4.0 and visc.rheology.affine_damping == 8.0
+    cal = m.MpmConfig.sand_calibrated()
+    assert cal.grid_size == 48 and cal.time_step == m.MpmTimeStep.IMPLICIT
+
+
+def test_dp_alpha_matches_oracle_material_row():
+    L = _ffi.lib()
+    for phi in (0.0, 0.1, 0.5, math.radians(30), 1.2):
+        assert L.mpm_dp_alpha(phi) == O.lib().orc_dp_alpha_f32(phi)
+
+
+def test_engine_without_gpu_reports_gpu_error():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(m.GpuError):
+        m.Engine(0)
+
+
+def test_struct_layout_matches_c_header(tmp_path):
+    """The ctypes mirror (and any Rust #[repr(C)] mirror) must match the C
+    header: compile the header with the C compiler and compare sizes/offsets."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "molla_mpm.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(mpm_rheology), sizeof(mpm_config),'
+        ' sizeof(mpm_status_info), sizeof(mpm_server_stats), offsetof(mpm_config, rheology),'
+        ' offsetof(mpm_config, grid_window_cells)); return 0;}\n')
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    exp = [ctypes.sizeof(_ffi.mpm_rheology), ctypes.sizeof(_ffi.mpm_config), ctypes.sizeof(_ffi.mpm_status_info),
+           ctypes.sizeof(_ffi.mpm_server_stats), _ffi.mpm_config.rheology.offset,
+           _ffi.mpm_config.grid_window_cells.offset]
+    assert got == exp

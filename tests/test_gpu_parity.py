@@ -1,0 +1,397 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the oracle, the
+reference's known-answer tests and the golden fixtures.
+
+Tolerances (FP32 state; atomic accumulation order on the GPU differs from
+the oracle's particle-index order, and the GPU path reuses the return
+mapping's SVD for the next stress):
+  * sort keys / permutations: bit-exact;
+  * one substep: |dx| <= 1e-6, |dv| <= 1e-5 * max(1, |v|), F/C/jp within
+    2e-5 normalised by max(|a|, 1) (the reference's own `close` bound,
+    crates/molla-solvers/src/mpm_particle_order_tests.rs:44-65);
+  * many substeps: positions within 1e-4 (absolute, unit box) of the FP32
+    oracle and within 1e-4 relative of the FP64 oracle.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import molla_b200 as m
+from molla_b200 import scenes
+from oracle import oracle as O
+from tests.golden import make_golden as G
+
+pytestmark = pytest.mark.gpu
+GOLD = G.HERE
+
+
+def norm_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float((np.abs(a - b) / np.maximum(np.abs(a), 1.0)).max()) if a.size else 0.0
+
+
+def run_both(engine, cfg, rows, pts, ids, dt, steps, vel=None, precision="f32", chunked=None, sort_interval=None):
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(pts, vel)
+    if rows is not None:
+        sim.set_materials(rows, ids)
+    if sort_interval is not None:
+        sim.set_sort_interval(sort_interval)
+    if chunked:
+        for c in chunked:
+            sim.step_n(dt, c)
+    else:
+        sim.step_n(dt, steps)
+    Cg, Fg, jpg = sim.read_particle_state()
+    gpu = {"pos": sim.read_positions(), "vel": sim.read_velocities(), "C": Cg, "F": Fg, "jp": jpg,
+           "status": sim.read_active_grid_status()}
+    eff_rows = rows if rows is not None else [cfg.rheology]
+    sc = O.make_scene(cfg, eff_rows, dt)
+    st = O.init_state(pts, vel, mass=cfg.particle_mass, volume=cfg.particle_volume, ids=ids)
+    O.step(sc, st, steps, precision=precision)
+    return sim, gpu, st
+
+
+# ---- sort: bit-exact permutation ----------------------------------------------
+
+@pytest.mark.parametrize("size", [35, 1536])
+def test_sort_permutation_bit_exact(engine, size):
+    """mpm_particle_order_tests.rs:67-165: exact keys and identities for
+    counts {513, 257, 1, 0, 63} at capacity 513, out-of-grid points clamped."""
+    cfg = m.MpmConfig.sand()
+    cfg.grid_size = size
+    cfg.grid_origin = (-1.0, -1.0, -1.0)
+    cfg.cell_size = 0.0625
+    cfg.max_particles = 513
+    sim = m.MpmSimulation.new(engine, cfg)
+    with pytest.raises(m.SolverError):
+        sim.set_particle_tile_ordering(True)
+    with pytest.raises(m.SolverError):
+        sim.prepare_particle_tile_ordering(0)
+    with pytest.raises(m.SolverError):
+        sim.prepare_particle_tile_ordering(514)
+    for count in (513, 257, 1, 0, 63, 513):
+        g = np.load(GOLD / f"particle_order_{size}_{count}.npz")
+        sim.set_particles(g["positions"][:count])
+        keys, ids = sim.read_sort_permutation(513)
+        assert np.array_equal(keys, g["keys"]), count
+        assert np.array_equal(ids, g["ids"]), count
+
+
+def test_sort_permutation_capacity_rules(engine):
+    """Preparing for 31 then seeding 32 makes step_n fail without moving
+    particles (mpm_particle_order_tests.rs:147-156)."""
+    cfg = m.MpmConfig.sand()
+    cfg.max_particles = 513
+    sim = m.MpmSimulation.new(engine, cfg)
+    pts = G.points(32) * np.float32(0.5)
+    sim.set_particles(pts[:31])
+    sim.prepare_particle_tile_ordering(31)
+    sim.set_particle_tile_ordering(True)
+    sim.set_particles(pts)
+    before = sim.read_positions()
+    with pytest.raises(m.SolverError):
+        sim.step_n(1e-4, 1)
+    assert np.array_equal(before, sim.read_positions())
+    sim.prepare_particle_tile_ordering(64)
+    sim.set_particle_tile_ordering(False)
+
+
+@pytest.mark.parametrize("name", ["random_1k", "all_equal", "sorted", "reverse", "paired", "high_byte"])
+def test_radix_sort_suite(engine, name):
+    """radix_sort_gpu.rs:395-520 (stable-sort bit-exactness)."""
+    g = np.load(GOLD / f"radix_{name}.npz")
+    k, v = m.radix_sort_pairs(engine, g["keys"], g["values"], 32)
+    assert np.array_equal(k, g["sorted_keys"]) and np.array_equal(v, g["sorted_values"])
+
+
+def test_radix_sort_random_100k(engine):
+    r = G.lcg(0xBADC0FFEE0DDF00D)
+    keys = np.array([r() for _ in range(100_000)], np.uint32)
+    vals = np.arange(keys.shape[0], dtype=np.uint32)
+    k, v = m.radix_sort_pairs(engine, keys, vals, 32)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(k, keys[order]) and np.array_equal(v, vals[order])
+
+
+@pytest.mark.parametrize("n,bits", [(1, 8), (4097, 12), (300_000, 18), (2_000_003, 24)])
+def test_radix_sort_sizes_and_widths(engine, n, bits):
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << bits, size=n, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    k, v = m.radix_sort_pairs(engine, keys, vals, bits)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(k, keys[order]) and np.array_equal(v, vals[order])
+
+
+# ---- known-answer tests on the CUDA path ------------------------------------------
+
+def test_free_fall_exact(engine):
+    """mpm_freefall_regression_gpu.rs:76-111."""
+    cfg = m.MpmConfig.snow()
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles([[0.013, 0.2, 0.017]])
+    dt = 1.0 / 480.0
+    for step in range(20):
+        sim.step(dt)
+        pos = sim.read_positions()
+        vel = sim.read_velocities()
+        assert abs(vel[0, 1] - (-9.81 * dt * (step + 1))) < 1e-4
+        assert abs(vel[0, 0]) < 1e-5 and abs(vel[0, 2]) < 1e-5
+        assert abs(pos[0, 0] - 0.013) < 1e-5 and abs(pos[0, 2] - 0.017) < 1e-5
+    assert sim.read_active_grid_status().completed_substeps == 20
+
+
+def test_grid_mass_matches_particle_mass(engine):
+    """mpm_gpu.rs:839-884, plus per-cell parity with the oracle's grid."""
+    cfg = m.MpmConfig.sand()
+    cfg.gravity_y = 0.0
+    cfg.grid_origin = (-1.6, -1.6, -1.6)
+    cfg.grid_size = 32
+    cfg.cell_size = 0.1
+    cfg.particle_mass = 2.5e-3
+    cfg.boundary_friction = 1.0
+    pts = scenes.fill_box_lcg([-0.35] * 3, [0.35] * 3, 7, 19)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(pts)
+    sim.step(1.0 / 240)
+    gm, gp = sim.read_grid_mass_momentum()
+    exp = cfg.particle_mass * len(pts)
+    assert (gm > 0).sum() > 0
+    assert abs(gm.sum(dtype=np.float64) - exp) / exp < 1e-4
+    assert np.abs(gp).max() < 1e-6
+    sc = O.make_scene(cfg, [cfg.rheology], 1.0 / 240)
+    st = O.init_state(pts, mass=cfg.particle_mass, volume=cfg.particle_volume)
+    om, op = O.step(sc, st, 1, want_grid=True)
+    # mpm_perf.rs:364-477 tolerances: per-cell |dm| < 1e-4 or rel < 1e-3
+    dm = np.abs(gm - om)
+    assert np.all((dm < 1e-4) | (dm / np.maximum(om, 1e-30) < 1e-3))
+    assert np.abs(gp - op).max() < 1e-3
+    tot = sim.conservation_totals()
+    assert abs(tot[0] - exp) / exp < 1e-6 and abs(tot[4] - exp) / exp < 1e-6
+
+
+def test_momentum_drift_closed_system(engine):
+    """mpm_gpu.rs:780-837."""
+    cfg = m.MpmConfig.sand()
+    cfg.gravity_y = 0.0
+    cfg.grid_origin = (-1.6, -1.6, -1.6)
+    cfg.grid_size = 32
+    cfg.cell_size = 0.1
+    cfg.boundary_friction = 1.0
+    pts = scenes.fill_box_lcg([-0.4] * 3, [0.4] * 3, 8, 7)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(pts)
+    for _ in range(60):
+        sim.step(1.0 / 240)
+    vel = sim.read_velocities()
+    p = np.linalg.norm(vel.sum(0)) * cfg.particle_mass
+    assert p < 0.01 * cfg.particle_mass * len(pts)
+
+
+def test_sand_block_smoke(engine):
+    """mpm_gpu.rs:201-241."""
+    cfg = m.MpmConfig.sand()
+    pts = scenes.fill_box_lcg([-0.2, 0.6, -0.2], [0.2, 1.0, 0.2], 8, 42)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(pts)
+    for _ in range(60):
+        sim.step(1.0 / 240)
+    pos, vel = sim.read_positions(), sim.read_velocities()
+    assert np.isfinite(pos).all() and np.isfinite(vel).all()
+    assert pos[:, 1].min() < 0.95 and np.linalg.norm(vel, axis=1).max() < 50
+
+
+@pytest.mark.parametrize("preset", ["sand", "snow", "viscous"])
+def test_dropped_block_settles(engine, preset):
+    """mpm_freefall_regression_gpu.rs:113-130 (snow), extended to each rheology."""
+    cfg = getattr(m.MpmConfig, preset)()
+    pts = scenes.fill_box_lcg([-0.075, 0.12, -0.075], [0.075, 0.27, 0.075], 6, 22)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(pts)
+    sim.step_n(1.0 / 480, 300)
+    pos = sim.read_positions()
+    assert pos[:, 1].max() < 0.35 and np.abs(pos[:, 0]).max() < 0.25
+    assert not sim.read_active_grid_status().numerical_fault
+
+
+# ---- step parity against the oracle ------------------------------------------------
+
+@pytest.mark.parametrize("preset", ["sand", "snow", "viscous"])
+def test_one_substep_parity(engine, preset):
+    cfg = getattr(m.MpmConfig, preset)()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 8, 42)
+    rng = np.random.default_rng(1)
+    vel = rng.uniform(-0.5, 0.5, size=pts.shape).astype(np.float32)
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 240, 1, vel=vel)
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 1e-6
+    assert np.abs(gpu["vel"] - st["vel"]).max() < 1e-5
+    assert norm_err(gpu["C"], st["C"]) < 2e-5 * 10
+    assert norm_err(gpu["F"], st["F"]) < 2e-5
+    assert norm_err(gpu["jp"], st["jp"]) < 2e-5
+
+
+@pytest.mark.parametrize("preset", ["sand", "snow", "viscous"])
+def test_many_substeps_parity(engine, preset):
+    cfg = getattr(m.MpmConfig, preset)()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 8, 42)
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 480, 120)
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 1e-4
+    assert np.abs(gpu["vel"] - st["vel"]).max() < 1e-2
+    assert gpu["status"].completed_substeps == 120 and not gpu["status"].numerical_fault
+
+
+def ordering_config(size=35):
+    # mpm_particle_order_tests.rs:7-18
+    cfg = m.MpmConfig.sand()
+    cfg.grid_size = size
+    cfg.grid_origin = (-1.0, -1.0, -1.0)
+    cfg.cell_size = 0.0625
+    cfg.max_particles = 513
+    cfg.youngs = 3000.0
+    cfg.particle_volume = float(np.float32(0.021) ** 3)
+    cfg.particle_mass = float(np.float32(cfg.particle_volume) * np.float32(1600.0))
+    return cfg
+
+
+MIXED_ROWS = [m.MpmRheology.Sand(0.5), m.MpmRheology.Snow(0.025, 0.0075, 10.0), m.MpmRheology.Viscous(0.1, 0.2)]
+
+
+@pytest.mark.parametrize("count", [257, 63])
+def test_mixed_materials_parity(engine, count):
+    """ordered_transfer_preserves_material_state (mpm_particle_order_tests.rs:167-285):
+    three rheologies, initial velocity, 6 substeps in windows of 2, the
+    reference's `close` tolerance (2e-5)."""
+    cfg = ordering_config()
+    pts = G.points(count)
+    ids = (np.arange(count) % 3).astype(np.uint32)
+    vel = np.tile(np.array([0.1, -0.02, 0.03], np.float32), (count, 1))
+    _, gpu, st = run_both(engine, cfg, MIXED_ROWS, pts, ids, 1e-4, 6, vel=vel, chunked=[2, 2, 2])
+    assert np.abs(gpu["pos"] - st["pos"]).max() <= 2e-5
+    assert np.abs(gpu["vel"] - st["vel"]).max() <= 2e-5
+    assert norm_err(gpu["C"], st["C"]) <= 2e-5
+    assert norm_err(gpu["F"], st["F"]) <= 2e-5
+    assert norm_err(gpu["jp"], st["jp"]) <= 2e-5
+
+
+@pytest.mark.parametrize("interval", [1, 4, 64])
+def test_regroup_interval_does_not_change_results(engine, interval):
+    cfg = m.MpmConfig.snow()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 10, 3)
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 480, 40, sort_interval=interval)
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 2e-5
+
+
+def test_fp64_svd_mode_parity(engine):
+    cfg = m.MpmConfig.snow()
+    cfg.svd_precision = 1
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 8, 42)
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 480, 60, precision="f32_svd64")
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 1e-4
+
+
+def test_cube_positions_vs_fp64_oracle(engine):
+    """Accuracy gate on a reduced cube scene: positions within 1e-4 relative
+    of the FP64 oracle after 1000 substeps."""
+    sc_ = scenes.cube_scene(grid_size=16, per_axis=12, seed=0, dt=1e-4)
+    cfg = m.config_for_scene(sc_, svd_precision=1)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(sc_.positions)
+    sim.set_materials(sc_.rows, sc_.ids)
+    sim.step_n(sc_.dt, 1000)
+    pos = sim.read_positions().astype(np.float64)
+    osc = O.make_scene(cfg, sc_.rows, sc_.dt, svd_tol=1e-14, svd_sweeps=30)
+    st = O.cast_state(O.init_state(sc_.positions, mass=cfg.particle_mass, volume=cfg.particle_volume, ids=sc_.ids),
+                      np.float64)
+    O.step(osc, st, 1000, precision="f64")
+    rel = np.abs(pos - st["pos"]) / np.abs(st["pos"])
+    assert rel.max() < 1e-4, rel.max()
+
+
+# ---- fault latch (mpm_numerical_fault_tests.rs:19-100) -----------------------------
+
+@pytest.mark.parametrize("bits", [np.nan, np.inf, -np.inf])
+def test_fault_latches_without_repair(engine, bits):
+    cfg = m.MpmConfig.sand()
+    cfg.max_particles = 4
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles([[0.0, 0.3, 0.0], [0.1, 0.3, 0.0]])
+    sim.step_n(1e-4, 1)
+    C0, F0, jp0 = sim.read_particle_state()
+    F = F0.copy()
+    F[0, 4] = bits
+    sim.write_particle_state(F=F)
+    sim.step_n(1e-4, 1)
+    s = sim.read_active_grid_status()
+    assert s.numerical_fault and s.faulted()
+    before = (sim.read_positions(), sim.read_velocities(), *sim.read_particle_state())
+    sim.step_n(1e-4, 3)
+    after = (sim.read_positions(), sim.read_velocities(), *sim.read_particle_state())
+    for a, b in zip(before, after):
+        assert np.array_equal(a, b, equal_nan=True)
+    assert sim.read_active_grid_status().numerical_fault
+    # restore + reset recovers
+    sim.write_particle_state(C_=C0, F=F0, jp=jp0)
+    sim.reset_active_grid()
+    sim.step_n(1e-4, 1)
+    assert not sim.read_active_grid_status().faulted()
+
+
+# ---- prepared steps / command batches (mpm_command_batch.rs) ---------------------
+
+def test_prepared_batch_matches_step_n_and_goes_stale(engine):
+    cfg = m.MpmConfig.snow()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 8, 5)
+    a = m.MpmSimulation.new(engine, cfg)
+    b = m.MpmSimulation.new(engine, cfg)
+    a.set_particles(pts)
+    b.set_particles(pts)
+    a.set_sort_interval(8)
+    b.set_sort_interval(8)
+    rec = b.prepare_step(1.0 / 480, 10)
+    for _ in range(3):
+        a.step_n(1.0 / 480, 10)
+        batch = b.begin_command_batch()
+        batch.encode_step(rec)
+        batch.submit()
+    pa, pb = a.read_positions(), b.read_positions()
+    assert np.abs(pa - pb).max() < 1e-5
+    assert b.read_active_grid_status().completed_substeps == 30
+    # a dropped batch does nothing
+    batch = b.begin_command_batch()
+    batch.encode_step(rec)
+    del batch
+    assert np.array_equal(pb, b.read_positions())
+    # another simulation's record / a stale record is rejected
+    batch = a.begin_command_batch()
+    with pytest.raises(m.StaleError):
+        batch.encode_step(rec)
+    b.set_rheology(m.MpmRheology.Snow())
+    batch = b.begin_command_batch()
+    with pytest.raises(m.StaleError):
+        batch.encode_step(rec)
+
+
+# ---- multi-material equivalence (mpm_multimaterial_gpu.rs:129-191) ---------------
+
+def test_disjoint_blocks_mixed_equal_separate_runs(engine):
+    cfg = m.MpmConfig.sand()
+    cfg.max_particles = 4096
+    a = scenes.fill_box_lcg([-0.5, 0.2, -0.1], [-0.3, 0.4, 0.1], 6, 1)
+    b = scenes.fill_box_lcg([0.3, 0.2, -0.1], [0.5, 0.4, 0.1], 6, 2)
+    rows = [m.MpmRheology.Sand(math.radians(30)), m.MpmRheology.Snow()]
+    mixed = m.MpmSimulation.new(engine, cfg)
+    mixed.set_particles(np.concatenate([a, b]))
+    mixed.set_materials(rows, np.r_[np.zeros(len(a)), np.ones(len(b))].astype(np.uint32))
+    mixed.step_n(1.0 / 480, 60)
+    pm = mixed.read_positions()
+    outs = []
+    for pts, rid in ((a, 0), (b, 1)):
+        s = m.MpmSimulation.new(engine, cfg)
+        s.set_particles(pts)
+        s.set_materials(rows, np.full(len(pts), rid, np.uint32))
+        s.step_n(1.0 / 480, 60)
+        outs.append(s.read_positions())
+    assert np.abs(pm - np.concatenate(outs)).max() < 1e-5
