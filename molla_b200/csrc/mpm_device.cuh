@@ -34,14 +34,21 @@ constexpr uint32_t kFaultNumerical = 2u;  // mpm.wgsl:229 numerical_fault()
 constexpr uint32_t kStatusWords = 4u;     // [fault bits, completed substeps, spare, spare]
 constexpr int kMaxMaterials = 8;          // MAX_MPM_MATERIALS, mpm.rs:660
 
-// Region of grid nodes a work item accumulates in shared memory: 9^3 nodes
-// starting at 4*tile - 2 along each axis.  A particle whose floor(x) lies in
-// the tile has base = floor(x - 0.5) in [4t-1, 4t+3] and touches nodes
-// [4t-1, 4t+5]; the region leaves one cell of drift on each side for
-// particles that moved since the last regrouping.  Anything further out is
-// deposited with global atomics.
-constexpr int kRegion = 9;
+// Work items cover the particles regrouped under one 4^3 tile of base cells
+// (base = floor(x/dx - 0.5), the lowest node of the quadratic stencil).  A
+// particle whose base lies in tile t touches nodes [4t, 4t+5]; the item
+// accumulates in a shared-memory block of 8^3 nodes starting at 4t - 1, which
+// leaves one cell of drift on each side for particles that moved since the
+// last regrouping.  Anything further out is deposited with global atomics.
+// Node (lx, ly, lz) of the block lives at lx + 8 ly + 68 lz: the 68-float z
+// stride maps a 4x4x2 block of distinct nodes onto 32 distinct banks.
+constexpr int kRegion = 8;
 constexpr int kRegionNodes = kRegion * kRegion * kRegion;
+constexpr int kRsy = 8;
+constexpr int kRsz = 68;
+constexpr int kRegionFloats = kRsz * kRegion;  // 544
+// Bits of the within-cell rank in the regroup key (tile, rank, cell).
+constexpr int kCellBits = 6;
 
 struct MatDev {
   int32_t rheo;      // 0 sand, 1 snow, 2 viscous (mpm.wgsl:556-557)

@@ -29,7 +29,9 @@ cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* sl
 cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
                            uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, uint32_t n_live,
                            cudaStream_t st);
-cudaError_t launch_items(const uint32_t* sorted_keys, uint32_t n_live, uint32_t K, uint32_t* tile_start,
+cudaError_t launch_rank_keys(const uint32_t* sorted, const uint32_t* ids, uint32_t n_live, int rank_bits,
+                             uint32_t* key2, uint32_t* ids2, cudaStream_t st);
+cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
                          Item* items, uint32_t* n_items, cudaStream_t st);
 cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,

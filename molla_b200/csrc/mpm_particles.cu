@@ -1,0 +1,458 @@
+// mpm_particles.cu — the particle kernel of the B200 MLS-MPM substep.
+//
+// One substep of the reference (crates/molla-solvers/src/mpm.rs:2476-2551:
+// reset_grid, p2g, grid_update, g2p, plasticity) runs as two launches:
+//
+//   grid_update(n)   acc[a] -> velocity, clears acc[b]                (grid sweep)
+//   particles(n)     G2P(n) + return mapping(n) + P2G(n+1) into acc[b]
+//
+// The particle kernel is persistent over a work list of (scene, tile, slot
+// range) items built by the last regrouping.  Per item a CTA
+//   1. copies the scene constants to shared memory and stages the 8^3-node
+//      velocity block around the tile (one coalesced pass over HBM),
+//   2. runs the gather, the F update and the return mapping per particle,
+//      writes the particle back (each particle is read and written once per
+//      substep), then deposits the next substep's mass and APIC momentum
+//      into an 8^3-node shared-memory block with shared atomics, and
+//   3. flushes the non-empty nodes to HBM with one float4 atomic each.
+// Particles are regrouped so that the 32 lanes of a warp hold particles of
+// 32 different base cells (rank-major order inside each tile), which makes
+// the shared-memory atomics of one stencil offset conflict-free.
+// The SVD computed by the return mapping is reused for the next substep's
+// stress (F was rebuilt from exactly that U, diag(s), V); the first substep
+// of every step_n call runs a P2G-only launch that computes it from F.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+#include "mpm_kernels.cuh"
+
+namespace mpm {
+
+namespace {
+
+struct SharedScatter {
+  float acc[4][kRegionFloats];
+};
+struct SharedGather {
+  float4 vel[kRegionNodes];
+};
+
+__device__ __forceinline__ int region_index(int lx, int ly, int lz) { return lx + kRsy * ly + kRsz * lz; }
+
+// 27-node APIC scatter of one particle (mpm.wgsl:601-627): the node at offset
+// (i,j,k) from base receives w*m and w*(m v + B d), d = ((i,j,k) - fx) dx.
+__device__ __forceinline__ void scatter_particle(SharedScatter& sh, int rx, int ry, int rz, const SceneDev& sc,
+                                                 float4* __restrict__ acc, const int* base, const float* fx,
+                                                 float mass, const float* v, const float* B) {
+  float w[3][3], d[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    quad_weights(fx[a], w[a]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx[a]) * sc.dx;
+  }
+  const float mv[3] = {mass * v[0], mass * v[1], mass * v[2]};
+  const int n = (int)sc.n;
+  const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+  const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
+                      (unsigned)lz0 <= (unsigned)(kRegion - 3);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float qx[3] = {mv[0] + B[0] * d[0][i], mv[1] + B[1] * d[0][i], mv[2] + B[2] * d[0][i]};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float wij = w[0][i] * w[1][j];
+      const float qy[3] = {qx[0] + B[3] * d[1][j], qx[1] + B[4] * d[1][j], qx[2] + B[5] * d[1][j]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float wt = wij * w[2][k];
+        const float dm = wt * mass;
+        const float px = wt * (qy[0] + B[6] * d[2][k]);
+        const float py = wt * (qy[1] + B[7] * d[2][k]);
+        const float pz = wt * (qy[2] + B[8] * d[2][k]);
+        if (inside) {
+          const int r = region_index(lx0 + i, ly0 + j, lz0 + k);
+          atomicAdd(&sh.acc[0][r], dm);
+          atomicAdd(&sh.acc[1][r], px);
+          atomicAdd(&sh.acc[2][r], py);
+          atomicAdd(&sh.acc[3][r], pz);
+        } else {
+          const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
+          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+            const uint64_t c =
+                sc.grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+            atomicAdd(&acc[c], make_float4(dm, px, py, pz));
+          }
+        }
+      }
+    }
+  }
+}
+
+// Regroup key of a particle from its base cell: ((scene tile offset + tile)
+// << 6) | cell within the tile; base clamped to the grid.
+__device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base) {
+  uint32_t t[3], c[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int b = base[a];
+    b = b < 0 ? 0 : b;
+    b = b > (int)sc.n - 1 ? (int)sc.n - 1 : b;
+    t[a] = (uint32_t)b >> 2;
+    c[a] = (uint32_t)b & 3u;
+  }
+  const uint32_t tile = t[0] + sc.w * (t[1] + sc.w * t[2]);
+  return ((sc.key_off + tile) << kCellBits) | c[0] | (c[1] << 2) | (c[2] << 4);
+}
+
+}  // namespace
+
+// MODE: kP2G (scatter only, SVD from F), kG2P (gather + return mapping, the
+// last substep of a call), kG2P2G (gather + return mapping + next scatter).
+template <int MODE, bool WRITE_KEYS, class SR>
+__global__ void __launch_bounds__(kParticleThreads, 2) k_particles(PoolDev p, int acc_out, double tol, int sweeps,
+                                                                   int reuse_svd) {
+  constexpr bool kGather = MODE != kP2G;
+  constexpr bool kScatter = MODE != kG2P;
+  __shared__ __align__(16) SceneDev s_sc;
+  __shared__ __align__(16) SharedScatter s_scat;
+  __shared__ __align__(16) SharedGather s_gath;
+  __shared__ uint32_t s_fault;
+  float4* __restrict__ acc = p.acc[acc_out];
+  const uint32_t n_items = *p.n_items;
+  const SR stol = (SR)tol;
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item item = p.items[it];
+    {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(p.scenes + item.scene);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
+      for (int k = threadIdx.x; k < (int)(sizeof(SceneDev) / 4); k += blockDim.x) dst[k] = src[k];
+    }
+    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)(p.status + (size_t)item.scene * kStatusWords);
+    __syncthreads();
+    const SceneDev& sc = s_sc;
+    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
+    const uint32_t tx = item.tile % sc.w, ty = (item.tile / sc.w) % sc.w, tz = item.tile / (sc.w * sc.w);
+    const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
+    const int n = (int)sc.n;
+    const bool faulted = s_fault != 0;
+    if constexpr (kScatter) {
+      for (int r = threadIdx.x; r < kRegionFloats; r += blockDim.x) {
+        s_scat.acc[0][r] = 0.f;
+        s_scat.acc[1][r] = 0.f;
+        s_scat.acc[2][r] = 0.f;
+        s_scat.acc[3][r] = 0.f;
+      }
+    }
+    if constexpr (kGather) {
+      if (!faulted) {
+        const float4* __restrict__ gvel = p.vel + sc.grid_off;
+        for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
+          const int ix = rx + (r & 7), iy = ry + ((r >> 3) & 7), iz = rz + (r >> 6);
+          float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
+            g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+          s_gath.vel[r] = g;
+        }
+      }
+    }
+    __syncthreads();
+    if (!faulted) {
+      for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
+        const uint32_t s = item.start + k;
+        float x = plane(p, PX)[s], y = plane(p, PY)[s], z = plane(p, PZ)[s];
+        float F[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = plane(p, F0 + i)[s];
+        float jp = plane(p, JP)[s];
+        const float mass = plane(p, MASS)[s];
+        const float vol = plane(p, VOL)[s];
+        const uint32_t mat = p.meta[s] & 7u;
+        float v[3], C[9];
+        bool ok = true;
+        SvdOut<SR> svd;
+        if constexpr (kGather) {
+          // ---- g2p (mpm.wgsl:1242-1353) ----
+          bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp);
+#pragma unroll
+          for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]);
+          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+          fin = fin && finitef(xp[0]) && finitef(xp[1]) && finitef(xp[2]);
+          if (!fin) {
+            atomicOr(status, kFaultNumerical);
+            ok = false;
+          }
+          if (ok) {
+            float w[3][3], d[3][3];
+            int base[3];
+            const int win[3] = {sc.winx, sc.winy, sc.winz};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const float bf = floorf(xp[a] - 0.5f);
+              base[a] = (int)bf - win[a];
+              const float fx = xp[a] - bf;
+              quad_weights(fx, w[a]);
+#pragma unroll
+              for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * sc.dx;
+            }
+            const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+            const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
+                                (unsigned)lz0 <= (unsigned)(kRegion - 3);
+            const float4* __restrict__ gvel = p.vel + sc.grid_off;
+            // Separable accumulation: v = sum w gv; G = sum (w gv) d^T.
+            float vs[3] = {0.f, 0.f, 0.f};
+            float G[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) G[i] = 0.f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              float si[3] = {0.f, 0.f, 0.f}, syi[3] = {0.f, 0.f, 0.f}, szi[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                float sj[3] = {0.f, 0.f, 0.f}, szj[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                  float4 g;
+                  if (inside) {
+                    g = s_gath.vel[(lx0 + i) + 8 * (ly0 + j) + 64 * (lz0 + kk)];
+                  } else {
+                    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + kk;
+                    g = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
+                      g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+                  }
+                  const float wk = w[2][kk];
+                  sj[0] += wk * g.x;
+                  sj[1] += wk * g.y;
+                  sj[2] += wk * g.z;
+                  const float wdk = wk * d[2][kk];
+                  szj[0] += wdk * g.x;
+                  szj[1] += wdk * g.y;
+                  szj[2] += wdk * g.z;
+                }
+                const float wj = w[1][j];
+                const float wdj = wj * d[1][j];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                  si[r] += wj * sj[r];
+                  syi[r] += wdj * sj[r];
+                  szi[r] += wj * szj[r];
+                }
+              }
+              const float wi = w[0][i];
+              const float wdi = wi * d[0][i];
+#pragma unroll
+              for (int r = 0; r < 3; ++r) {
+                vs[r] += wi * si[r];
+                G[r] += wdi * si[r];      // column x
+                G[3 + r] += wi * syi[r];  // column y
+                G[6 + r] += wi * szi[r];  // column z
+              }
+            }
+            const float four_inv_dx2 = 4.0f * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) C[i] = four_inv_dx2 * G[i];
+            v[0] = vs[0];
+            v[1] = vs[1];
+            v[2] = vs[2];
+            const MatDev& md = sc.mat[mat];
+            if (md.rheo == 2) {
+              v[0] *= md.vfac;
+              v[1] *= md.vfac;
+              v[2] *= md.vfac;
+#pragma unroll
+              for (int i = 0; i < 9; ++i) C[i] *= md.afac;
+            }
+            float np[3] = {x + sc.dt * v[0], y + sc.dt * v[1], z + sc.dt * v[2]};
+            bool fin2 = finitef(np[0]) && finitef(np[1]) && finitef(np[2]) && finitef(v[0]) && finitef(v[1]) &&
+                        finitef(v[2]);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) fin2 = fin2 && finitef(C[i]);
+            if (!fin2) {
+              atomicOr(status, kFaultNumerical);
+              ok = false;
+            }
+            if (ok) {
+#pragma unroll
+              for (int a = 0; a < 3; ++a) {
+                if (np[a] < sc.lo[a] || np[a] > sc.hi[a]) v[a] = 0.f;
+                np[a] = clampf(np[a], sc.lo[a], sc.hi[a]);
+              }
+              // F <- (I + dt C) F
+              float A[9];
+#pragma unroll
+              for (int i = 0; i < 9; ++i) A[i] = sc.dt * C[i] + ((i % 4 == 0) ? 1.f : 0.f);
+              float Fn[9];
+              matmul(A, F, Fn);
+              bool fin3 = true;
+#pragma unroll
+              for (int i = 0; i < 9; ++i) fin3 = fin3 && finitef(Fn[i]);
+              if (!fin3) {
+                atomicOr(status, kFaultNumerical);
+                ok = false;
+              } else {
+                x = np[0];
+                y = np[1];
+                z = np[2];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) F[i] = Fn[i];
+                // ---- plasticity (mpm.wgsl:1366-1479) on the updated F ----
+                SR Fs[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
+                svd3<SR>(Fs, svd, stol, sweeps);
+                float jp_new = jp;
+                if (plasticity_project<SR>(svd, md, jp_new)) {
+                  SR Fr[9];
+                  sandwich(svd.u, svd.s, svd.v, Fr);
+                  bool fin4 = true;
+#pragma unroll
+                  for (int i = 0; i < 9; ++i) fin4 = fin4 && finitef((float)Fr[i]);
+                  if (fin4) {
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
+                    jp = jp_new;
+                  } else {
+                    atomicOr(status, kFaultNumerical);
+                    ok = false;
+                  }
+                } else {
+                  atomicOr(status, kFaultNumerical);
+                  ok = false;
+                }
+                // G2P results are published even when the return mapping
+                // faults (the reference's g2p and plasticity are separate
+                // dispatches); only the plasticity update is withheld.
+                plane(p, PX)[s] = x;
+                plane(p, PY)[s] = y;
+                plane(p, PZ)[s] = z;
+                plane(p, VX)[s] = v[0];
+                plane(p, VY)[s] = v[1];
+                plane(p, VZ)[s] = v[2];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) plane(p, C0 + i)[s] = C[i];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) plane(p, F0 + i)[s] = F[i];
+                plane(p, JP)[s] = jp;
+              }
+            }
+          }
+        } else {
+          // P2G-only: read v and C and validate the whole state (the
+          // reference's g2p checks, mpm.wgsl:1247-1255, moved to the first
+          // launch of the call so that a non-finite upload latches before
+          // anything moves).
+          v[0] = plane(p, VX)[s];
+          v[1] = plane(p, VY)[s];
+          v[2] = plane(p, VZ)[s];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) C[i] = plane(p, C0 + i)[s];
+          bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp) && finitef(v[0]) && finitef(v[1]) &&
+                     finitef(v[2]) && finitef((x - sc.ox) * sc.inv_dx) && finitef((y - sc.oy) * sc.inv_dx) &&
+                     finitef((z - sc.oz) * sc.inv_dx);
+#pragma unroll
+          for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]) && finitef(C[i]);
+          if (!fin) {
+            atomicOr(status, kFaultNumerical);
+            ok = false;
+          }
+        }
+        int nbase[3];
+        {
+          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+          float fx[3];
+          const int win[3] = {sc.winx, sc.winy, sc.winz};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float bf = floorf(xp[a] - 0.5f);
+            nbase[a] = (int)bf - win[a];
+            fx[a] = xp[a] - bf;
+          }
+          if constexpr (kScatter) {
+            if (ok) {
+              if (!kGather || !reuse_svd) {
+                SR Fs[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
+                svd3<SR>(Fs, svd, stol, sweeps);
+              }
+              float B[9];
+              p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
+              scatter_particle(s_scat, rx, ry, rz, sc, acc, nbase, fx, mass, v, B);
+            }
+          }
+        }
+        if constexpr (WRITE_KEYS) {
+          p.keys_by_id[p.orig[s]] = base_key(sc, nbase);
+        }
+      }
+    }
+    if constexpr (kScatter) {
+      __syncthreads();
+      if (!faulted) {
+        for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
+          const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
+          const int q = region_index(lx, ly, lz);
+          const float m = s_scat.acc[0][q], px = s_scat.acc[1][q], py = s_scat.acc[2][q], pz = s_scat.acc[3][q];
+          if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
+            const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
+            if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+              const uint64_t c =
+                  sc.grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+              atomicAdd(&acc[c], make_float4(m, px, py, pz));
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+
+template <int MODE, bool KEYS, class SR>
+static cudaError_t launch_particles_t(const PoolDev& p, int acc_out, double tol, int sweeps, int reuse, int grid,
+                                      cudaStream_t st) {
+  k_particles<MODE, KEYS, SR><<<grid, kParticleThreads, 0, st>>>(p, acc_out, tol, sweeps, reuse);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_particles(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, int acc_out, double tol,
+                             int sweeps, int reuse, int grid, cudaStream_t st) {
+#define MPM_DISPATCH(M)                                                                                   \
+  if (mode == M) {                                                                                        \
+    if (svd_fp64) {                                                                                       \
+      return write_keys ? launch_particles_t<M, true, double>(p, acc_out, tol, sweeps, reuse, grid, st)   \
+                        : launch_particles_t<M, false, double>(p, acc_out, tol, sweeps, reuse, grid, st); \
+    }                                                                                                     \
+    return write_keys ? launch_particles_t<M, true, float>(p, acc_out, tol, sweeps, reuse, grid, st)      \
+                      : launch_particles_t<M, false, float>(p, acc_out, tol, sweeps, reuse, grid, st);    \
+  }
+  MPM_DISPATCH(kP2G)
+  MPM_DISPATCH(kG2P)
+  MPM_DISPATCH(kG2P2G)
+#undef MPM_DISPATCH
+  return cudaErrorInvalidValue;
+}
+
+int particle_grid_size(int mode, bool write_keys, bool svd_fp64) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaErrorInvalidValue;
+#define MPM_OCC(M, K, T)                                                                                     \
+  if (mode == M && write_keys == K && svd_fp64 == (sizeof(T) == 8))                                         \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_particles<M, K, T>, kParticleThreads, 0);
+  MPM_OCC(kP2G, false, float) MPM_OCC(kP2G, true, float) MPM_OCC(kP2G, false, double) MPM_OCC(kP2G, true, double)
+  MPM_OCC(kG2P, false, float) MPM_OCC(kG2P, true, float) MPM_OCC(kG2P, false, double) MPM_OCC(kG2P, true, double)
+  MPM_OCC(kG2P2G, false, float) MPM_OCC(kG2P2G, true, float) MPM_OCC(kG2P2G, false, double)
+  MPM_OCC(kG2P2G, true, double)
+#undef MPM_OCC
+  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (sms < 1) sms = 148;
+  return sms * per_sm;
+}
+
+}  // namespace mpm

@@ -151,7 +151,7 @@ class Group {
   // particle pool (double-buffered for the regroup)
   DevBuf<float> planes[2];
   DevBuf<uint32_t> meta[2], orig[2];
-  DevBuf<uint32_t> slot_of, keys_by_id, ks[2], vs[2], hist;
+  DevBuf<uint32_t> slot_of, keys_by_id, key2, ids2, ks[2], vs[2], hist;
   // grid pool
   DevBuf<float4> acc[2], vel;
   DevBuf<uint32_t> block_scene;
