@@ -273,8 +273,9 @@ MPM_API uint64_t mpm_engine_launch_count(mpm_engine* engine);
  * (prepare_step_profiling / read_step_profile, mpm_profile.rs:542-732):
  * while enabled, each launch of a stage is bracketed by CUDA events on its
  * stream (not inside captured graphs).  Stages: 0 particle ordering (keys,
- * sort, regroup, work list), 1 P2G, 2 grid update, 3 fused G2P + return
- * mapping + next P2G, 4 G2P + return mapping. */
+ * sort, regroup, work list), 1 first-substep stress record (SVD of F),
+ * 2 grid update, 3 G2P + F update + return
+ * mapping, 4 P2G deposit. */
 typedef struct mpm_profile_stage {
   uint64_t launches;
   double total_ms;

@@ -252,7 +252,7 @@ class Engine:
     def launch_count(self) -> int:
         return int(_ffi.lib().mpm_engine_launch_count(self._h))
 
-    STAGES = ("ParticleOrdering", "ParticleToGrid", "GridUpdate", "GatherScatter", "Gather")
+    STAGES = ("ParticleOrdering", "StressRecord", "GridUpdate", "GridToParticle", "ParticleToGrid")
 
     def profile(self, enabled: bool = True):
         _check(_ffi.lib().mpm_profile_enable(self._h, int(bool(enabled))))

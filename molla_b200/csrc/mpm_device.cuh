@@ -94,6 +94,7 @@ struct PoolDev {
   uint32_t* keys_by_id; // sort key per identity (written when a regroup is due)
   float4* acc[2];       // grid accumulators (mass, momentum)
   float4* vel;          // grid velocity (vx, vy, vz, mass)
+  float* rec;           // 10 planes of cap floats: B (9) for the next scatter, deposit flag
   const SceneDev* scenes;
   uint32_t* status;     // kStatusWords per scene
   const Item* items;

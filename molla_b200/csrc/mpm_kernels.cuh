@@ -10,12 +10,14 @@ namespace mpm {
 constexpr int kParticleThreads = 256;
 constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 256-cell block
 
-enum ParticleMode : int { kP2G = 0, kG2P = 1, kG2P2G = 2 };
+enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
 
-cudaError_t launch_particles(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, int acc_out, double tol,
-                             int sweeps, int reuse, int grid, cudaStream_t st);
-// Persistent grid size (SMs x resident CTAs) of a particle-kernel variant.
-int particle_grid_size(int mode, bool write_keys, bool svd_fp64);
+cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
+                          int reuse, int grid, cudaStream_t st);
+cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st);
+// Persistent grid sizes (SMs x resident CTAs).
+int gather_grid_size(bool svd_fp64);
+int scatter_grid_size();
 cudaError_t launch_grid_update(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
                                int count_substep, cudaStream_t st);
 cudaError_t launch_keys(const PoolDev& p, uint32_t n_slots, cudaStream_t st);

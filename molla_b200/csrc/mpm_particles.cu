@@ -1,26 +1,29 @@
-// mpm_particles.cu — the particle kernel of the B200 MLS-MPM substep.
+// mpm_particles.cu — the particle kernels of the B200 MLS-MPM substep.
 //
 // One substep of the reference (crates/molla-solvers/src/mpm.rs:2476-2551:
-// reset_grid, p2g, grid_update, g2p, plasticity) runs as two launches:
+// reset_grid, p2g, grid_update, g2p, plasticity) runs as three launches:
 //
-//   grid_update(n)   acc[a] -> velocity, clears acc[b]                (grid sweep)
-//   particles(n)     G2P(n) + return mapping(n) + P2G(n+1) into acc[b]
+//   grid_update(n)  acc[a] -> velocity, clears acc[b]               (grid sweep)
+//   gather(n)       G2P(n) + F update + return mapping(n); writes the particle
+//                   and, for the next substep, the APIC/stress matrix
+//                   B = m C + 4/dx^2 S (S the fixed-corotated stress term)
+//   scatter(n+1)    27-node deposit of mass and momentum into acc[b]
 //
-// The particle kernel is persistent over a work list of (scene, tile, slot
-// range) items built by the last regrouping.  Per item a CTA
-//   1. copies the scene constants to shared memory and stages the 8^3-node
-//      velocity block around the tile (one coalesced pass over HBM),
-//   2. runs the gather, the F update and the return mapping per particle,
-//      writes the particle back (each particle is read and written once per
-//      substep), then deposits the next substep's mass and APIC momentum
-//      into an 8^3-node shared-memory block with shared atomics, and
-//   3. flushes the non-empty nodes to HBM with one float4 atomic each.
-// Particles are regrouped so that the 32 lanes of a warp hold particles of
-// 32 different base cells (rank-major order inside each tile), which makes
-// the shared-memory atomics of one stencil offset conflict-free.
-// The SVD computed by the return mapping is reused for the next substep's
-// stress (F was rebuilt from exactly that U, diag(s), V); the first substep
-// of every step_n call runs a P2G-only launch that computes it from F.
+// Both particle kernels are persistent over a work list of (scene, tile, slot
+// range) items built by the last regrouping.  The gather stages the 8^3-node
+// velocity block around the tile in shared memory; the scatter accumulates
+// into an 8^3-node shared block and flushes the non-empty nodes to HBM with
+// one float4 atomic each.  They are separate kernels because the gather
+// (SVD, return mapping) needs ~128 registers per thread while the scatter
+// needs few: split, the scatter runs at high occupancy and hides the latency
+// of its shared-memory atomics; the 36-byte B record costs HBM bandwidth the
+// substep does not otherwise use.  Particles are regrouped so that the 32
+// lanes of a warp hold particles of 32 different base cells (rank-major order
+// inside each tile), which makes the atomics of one stencil offset
+// conflict-free.  The SVD computed by the return mapping is reused for the
+// next substep's stress (F was rebuilt from exactly that U, diag(s), V); the
+// first substep of every step_n call runs a record-only gather that computes
+// it from F.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -31,64 +34,11 @@ namespace mpm {
 
 namespace {
 
-struct SharedScatter {
-  float acc[4][kRegionFloats];
-};
 struct SharedGather {
   float4 vel[kRegionNodes];
 };
 
 __device__ __forceinline__ int region_index(int lx, int ly, int lz) { return lx + kRsy * ly + kRsz * lz; }
-
-// 27-node APIC scatter of one particle (mpm.wgsl:601-627): the node at offset
-// (i,j,k) from base receives w*m and w*(m v + B d), d = ((i,j,k) - fx) dx.
-__device__ __forceinline__ void scatter_particle(SharedScatter& sh, int rx, int ry, int rz, const SceneDev& sc,
-                                                 float4* __restrict__ acc, const int* base, const float* fx,
-                                                 float mass, const float* v, const float* B) {
-  float w[3][3], d[3][3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    quad_weights(fx[a], w[a]);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx[a]) * sc.dx;
-  }
-  const float mv[3] = {mass * v[0], mass * v[1], mass * v[2]};
-  const int n = (int)sc.n;
-  const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
-  const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
-                      (unsigned)lz0 <= (unsigned)(kRegion - 3);
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const float qx[3] = {mv[0] + B[0] * d[0][i], mv[1] + B[1] * d[0][i], mv[2] + B[2] * d[0][i]};
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const float wij = w[0][i] * w[1][j];
-      const float qy[3] = {qx[0] + B[3] * d[1][j], qx[1] + B[4] * d[1][j], qx[2] + B[5] * d[1][j]};
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float wt = wij * w[2][k];
-        const float dm = wt * mass;
-        const float px = wt * (qy[0] + B[6] * d[2][k]);
-        const float py = wt * (qy[1] + B[7] * d[2][k]);
-        const float pz = wt * (qy[2] + B[8] * d[2][k]);
-        if (inside) {
-          const int r = region_index(lx0 + i, ly0 + j, lz0 + k);
-          atomicAdd(&sh.acc[0][r], dm);
-          atomicAdd(&sh.acc[1][r], px);
-          atomicAdd(&sh.acc[2][r], py);
-          atomicAdd(&sh.acc[3][r], pz);
-        } else {
-          const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
-          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-            const uint64_t c =
-                sc.grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-            atomicAdd(&acc[c], make_float4(dm, px, py, pz));
-          }
-        }
-      }
-    }
-  }
-}
 
 // Regroup key of a particle from its base cell: ((scene tile offset + tile)
 // << 6) | cell within the tile; base clamped to the grid.
@@ -108,18 +58,17 @@ __device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base
 
 }  // namespace
 
-// MODE: kP2G (scatter only, SVD from F), kG2P (gather + return mapping, the
-// last substep of a call), kG2P2G (gather + return mapping + next scatter).
+// MODE: kRecord (no gather: validate the state and compute B from the SVD of
+// F — the first substep of a call), kG2P (gather + return mapping, the last
+// substep of a call), kG2PRecord (gather + return mapping + B for the next
+// scatter, with the return mapping's SVD reused).
 template <int MODE, bool WRITE_KEYS, class SR>
-__global__ void __launch_bounds__(kParticleThreads, 2) k_particles(PoolDev p, int acc_out, double tol, int sweeps,
-                                                                   int reuse_svd) {
-  constexpr bool kGather = MODE != kP2G;
+__global__ void __launch_bounds__(kParticleThreads, 2) k_gather(PoolDev p, double tol, int sweeps, int reuse_svd) {
+  constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   __shared__ __align__(16) SceneDev s_sc;
-  __shared__ __align__(16) SharedScatter s_scat;
   __shared__ __align__(16) SharedGather s_gath;
   __shared__ uint32_t s_fault;
-  float4* __restrict__ acc = p.acc[acc_out];
   const uint32_t n_items = *p.n_items;
   const SR stol = (SR)tol;
   for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -137,14 +86,6 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_particles(PoolDev p, in
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
     const int n = (int)sc.n;
     const bool faulted = s_fault != 0;
-    if constexpr (kScatter) {
-      for (int r = threadIdx.x; r < kRegionFloats; r += blockDim.x) {
-        s_scat.acc[0][r] = 0.f;
-        s_scat.acc[1][r] = 0.f;
-        s_scat.acc[2][r] = 0.f;
-        s_scat.acc[3][r] = 0.f;
-      }
-    }
     if constexpr (kGather) {
       if (!faulted) {
         const float4* __restrict__ gvel = p.vel + sc.grid_off;
@@ -358,50 +299,137 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_particles(PoolDev p, in
             ok = false;
           }
         }
-        int nbase[3];
-        {
-          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
-          float fx[3];
-          const int win[3] = {sc.winx, sc.winy, sc.winz};
+        if constexpr (kScatter) {
+          // B = m C + 4/dx^2 S for the next scatter (all-zero for a particle
+          // that faulted, which then deposits nothing).
+          float B[9];
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float bf = floorf(xp[a] - 0.5f);
-            nbase[a] = (int)bf - win[a];
-            fx[a] = xp[a] - bf;
-          }
-          if constexpr (kScatter) {
-            if (ok) {
-              if (!kGather || !reuse_svd) {
-                SR Fs[9];
+          for (int i = 0; i < 9; ++i) B[i] = 0.f;
+          if (ok) {
+            if (!kGather || !reuse_svd) {
+              SR Fs[9];
 #pragma unroll
-                for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
-                svd3<SR>(Fs, svd, stol, sweeps);
-              }
-              float B[9];
-              p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
-              scatter_particle(s_scat, rx, ry, rz, sc, acc, nbase, fx, mass, v, B);
+              for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
+              svd3<SR>(Fs, svd, stol, sweeps);
             }
+            p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
           }
+#pragma unroll
+          for (int i = 0; i < 9; ++i) p.rec[(size_t)i * p.cap + s] = B[i];
+          p.rec[(size_t)9 * p.cap + s] = ok ? 1.f : 0.f;
         }
         if constexpr (WRITE_KEYS) {
+          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+          const int win[3] = {sc.winx, sc.winy, sc.winz};
+          int nbase[3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) nbase[a] = (xp[a] == xp[a]) ? (int)floorf(xp[a] - 0.5f) - win[a] : 0;
           p.keys_by_id[p.orig[s]] = base_key(sc, nbase);
         }
       }
     }
-    if constexpr (kScatter) {
-      __syncthreads();
-      if (!faulted) {
-        for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-          const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
-          const int q = region_index(lx, ly, lz);
-          const float m = s_scat.acc[0][q], px = s_scat.acc[1][q], py = s_scat.acc[2][q], pz = s_scat.acc[3][q];
-          if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
-            const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
-            if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-              const uint64_t c =
-                  sc.grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-              atomicAdd(&acc[c], make_float4(m, px, py, pz));
+    __syncthreads();
+  }
+}
+
+// Scatter of the next substep (mpm.wgsl:601-627): particle at slot s with
+// base = floor(x/dx - 0.5) and fx = x/dx - base deposits, at the node of
+// offset (i,j,k), w m and w (m v + B d), d = ((i,j,k) - fx) dx, w the
+// quadratic B-spline weight.  Particles whose record flag is zero (numerical
+// fault this substep) deposit nothing.
+__global__ void __launch_bounds__(kParticleThreads, 4) k_scatter(PoolDev p, int acc_out) {
+  __shared__ float s_acc[4][kRegionFloats];
+  __shared__ uint32_t s_fault;
+  float4* __restrict__ acc = p.acc[acc_out];
+  const uint32_t n_items = *p.n_items;
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item item = p.items[it];
+    const SceneDev* __restrict__ scp = p.scenes + item.scene;
+    const uint32_t w = scp->w;
+    const int n = (int)scp->n;
+    const float ox = scp->ox, oy = scp->oy, oz = scp->oz, inv_dx = scp->inv_dx, dx = scp->dx;
+    const int winx = scp->winx, winy = scp->winy, winz = scp->winz;
+    const uint64_t grid_off = scp->grid_off;
+    const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
+    const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
+    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)(p.status + (size_t)scp->status * kStatusWords);
+    for (int r = threadIdx.x; r < kRegionFloats; r += blockDim.x) {
+      s_acc[0][r] = 0.f;
+      s_acc[1][r] = 0.f;
+      s_acc[2][r] = 0.f;
+      s_acc[3][r] = 0.f;
+    }
+    __syncthreads();
+    // A fault latched before this launch (by an earlier substep) freezes the
+    // scene; one latched by this substep's gather is handled per particle.
+    const bool faulted = s_fault != 0;
+    for (uint32_t k = threadIdx.x; k < item.count && !faulted; k += blockDim.x) {
+      const uint32_t s = item.start + k;
+      if (p.rec[(size_t)9 * p.cap + s] == 0.f) continue;
+      const float xp[3] = {(plane(p, PX)[s] - ox) * inv_dx, (plane(p, PY)[s] - oy) * inv_dx,
+                           (plane(p, PZ)[s] - oz) * inv_dx};
+      const float mass = plane(p, MASS)[s];
+      const float mv[3] = {mass * plane(p, VX)[s], mass * plane(p, VY)[s], mass * plane(p, VZ)[s]};
+      float B[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) B[i] = p.rec[(size_t)i * p.cap + s];
+      float wgt[3][3], d[3][3];
+      int base[3];
+      const int win[3] = {winx, winy, winz};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float bf = floorf(xp[a] - 0.5f);
+        base[a] = (int)bf - win[a];
+        const float fx = xp[a] - bf;
+        quad_weights(fx, wgt[a]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * dx;
+      }
+      const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+      const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
+                          (unsigned)lz0 <= (unsigned)(kRegion - 3);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const float qx[3] = {mv[0] + B[0] * d[0][i], mv[1] + B[1] * d[0][i], mv[2] + B[2] * d[0][i]};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float wij = wgt[0][i] * wgt[1][j];
+          const float qy[3] = {qx[0] + B[3] * d[1][j], qx[1] + B[4] * d[1][j], qx[2] + B[5] * d[1][j]};
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            const float wt = wij * wgt[2][kk];
+            const float dm = wt * mass;
+            const float px = wt * (qy[0] + B[6] * d[2][kk]);
+            const float py = wt * (qy[1] + B[7] * d[2][kk]);
+            const float pz = wt * (qy[2] + B[8] * d[2][kk]);
+            if (inside) {
+              const int r = region_index(lx0 + i, ly0 + j, lz0 + kk);
+              atomicAdd(&s_acc[0][r], dm);
+              atomicAdd(&s_acc[1][r], px);
+              atomicAdd(&s_acc[2][r], py);
+              atomicAdd(&s_acc[3][r], pz);
+            } else {
+              const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + kk;
+              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+                const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+                atomicAdd(&acc[c], make_float4(dm, px, py, pz));
+              }
             }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (!faulted) {
+      for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
+        const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
+        const int q = region_index(lx, ly, lz);
+        const float m = s_acc[0][q], px = s_acc[1][q], py = s_acc[2][q], pz = s_acc[3][q];
+        if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
+          const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
+          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+            const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+            atomicAdd(&acc[c], make_float4(m, px, py, pz));
           }
         }
       }
@@ -413,46 +441,49 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_particles(PoolDev p, in
 // ---------------------------------------------------------------------------
 
 template <int MODE, bool KEYS, class SR>
-static cudaError_t launch_particles_t(const PoolDev& p, int acc_out, double tol, int sweeps, int reuse, int grid,
-                                      cudaStream_t st) {
-  k_particles<MODE, KEYS, SR><<<grid, kParticleThreads, 0, st>>>(p, acc_out, tol, sweeps, reuse);
+static cudaError_t launch_gather_t(const PoolDev& p, double tol, int sweeps, int reuse, int grid, cudaStream_t st) {
+  k_gather<MODE, KEYS, SR><<<grid, kParticleThreads, 0, st>>>(p, tol, sweeps, reuse);
   return cudaGetLastError();
 }
 
-cudaError_t launch_particles(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, int acc_out, double tol,
-                             int sweeps, int reuse, int grid, cudaStream_t st) {
-#define MPM_DISPATCH(M)                                                                                   \
-  if (mode == M) {                                                                                        \
-    if (svd_fp64) {                                                                                       \
-      return write_keys ? launch_particles_t<M, true, double>(p, acc_out, tol, sweeps, reuse, grid, st)   \
-                        : launch_particles_t<M, false, double>(p, acc_out, tol, sweeps, reuse, grid, st); \
-    }                                                                                                     \
-    return write_keys ? launch_particles_t<M, true, float>(p, acc_out, tol, sweeps, reuse, grid, st)      \
-                      : launch_particles_t<M, false, float>(p, acc_out, tol, sweeps, reuse, grid, st);    \
+cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
+                          int reuse, int grid, cudaStream_t st) {
+#define MPM_DISPATCH(M)                                                                        \
+  if (mode == M) {                                                                             \
+    if (svd_fp64) {                                                                            \
+      return write_keys ? launch_gather_t<M, true, double>(p, tol, sweeps, reuse, grid, st)    \
+                        : launch_gather_t<M, false, double>(p, tol, sweeps, reuse, grid, st);  \
+    }                                                                                          \
+    return write_keys ? launch_gather_t<M, true, float>(p, tol, sweeps, reuse, grid, st)       \
+                      : launch_gather_t<M, false, float>(p, tol, sweeps, reuse, grid, st);     \
   }
-  MPM_DISPATCH(kP2G)
+  MPM_DISPATCH(kRecord)
   MPM_DISPATCH(kG2P)
-  MPM_DISPATCH(kG2P2G)
+  MPM_DISPATCH(kG2PRecord)
 #undef MPM_DISPATCH
   return cudaErrorInvalidValue;
 }
 
-int particle_grid_size(int mode, bool write_keys, bool svd_fp64) {
+cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st) {
+  k_scatter<<<grid, kParticleThreads, 0, st>>>(p, acc_out);
+  return cudaGetLastError();
+}
+
+static int persistent(const void* fn) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaErrorInvalidValue;
-#define MPM_OCC(M, K, T)                                                                                     \
-  if (mode == M && write_keys == K && svd_fp64 == (sizeof(T) == 8))                                         \
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_particles<M, K, T>, kParticleThreads, 0);
-  MPM_OCC(kP2G, false, float) MPM_OCC(kP2G, true, float) MPM_OCC(kP2G, false, double) MPM_OCC(kP2G, true, double)
-  MPM_OCC(kG2P, false, float) MPM_OCC(kG2P, true, float) MPM_OCC(kG2P, false, double) MPM_OCC(kG2P, true, double)
-  MPM_OCC(kG2P2G, false, float) MPM_OCC(kG2P2G, true, float) MPM_OCC(kG2P2G, false, double)
-  MPM_OCC(kG2P2G, true, double)
-#undef MPM_OCC
-  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kParticleThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
   if (sms < 1) sms = 148;
   return sms * per_sm;
 }
+
+int gather_grid_size(bool svd_fp64) {
+  return svd_fp64 ? persistent((const void*)k_gather<kG2PRecord, false, double>)
+                  : persistent((const void*)k_gather<kG2PRecord, false, float>);
+}
+
+int scatter_grid_size() { return persistent((const void*)k_scatter); }
 
 }  // namespace mpm

@@ -226,6 +226,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaSetDevice(eng->device));
   planes[0].alloc((size_t)kPlanes * cap);
   planes[1].alloc((size_t)kPlanes * cap);
+  rec.alloc((size_t)10 * cap);
   for (int i = 0; i < 2; ++i) {
     meta[i].alloc(cap);
     orig[i].alloc(cap);
@@ -258,9 +259,9 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaMemsetAsync(scenes_d.ptr, 0, scenes_d.bytes(), stream));
   ids.init(cap);
   cells.init(cell_cap);
-  grid_p2g = particle_grid_size(kP2G, false, false);
-  grid_g2p = particle_grid_size(kG2P, false, false);
-  grid_g2p2g = particle_grid_size(kG2P2G, false, false);
+  grid_gather32 = gather_grid_size(false);
+  grid_gather64 = gather_grid_size(true);
+  grid_scatter = scatter_grid_size();
   MPM_CK(cudaStreamSynchronize(stream));
 }
 
@@ -287,6 +288,7 @@ PoolDev Group::pool() const {
   p.acc[0] = acc[0].ptr;
   p.acc[1] = acc[1].ptr;
   p.vel = vel.ptr;
+  p.rec = rec.ptr;
   p.scenes = scenes_d.ptr;
   p.status = status_d.ptr;
   p.items = items.ptr;
@@ -549,19 +551,32 @@ void Group::regroup(bool compute_keys, cudaStream_t st) {
   eng->prof_end(&pr, st);
 }
 
-void Group::launch_pass(int mode, bool keys, int acc_out, cudaStream_t st) {
-  const int grid = mode == kP2G ? grid_p2g : (mode == kG2P ? grid_g2p : grid_g2p2g);
+void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
+  const int grid = svd_fp64 ? grid_gather64 : grid_gather32;
   const double tol = svd_fp64 ? svd_tol64 : svd_tol32;
   ProfRec pr;
-  eng->prof_begin(mode == kP2G ? kStageP2G : (mode == kG2P ? kStageG2P : kStageG2P2G), st, &pr);
-  MPM_CK(launch_particles(mode, keys, svd_fp64, pool(), acc_out, tol, svd_sweeps, reuse_svd ? 1 : 0, grid, st));
+  eng->prof_begin(mode == kRecord ? kStageRecord : kStageGather, st, &pr);
+  MPM_CK(launch_gather(mode, keys, svd_fp64, pool(), tol, svd_sweeps, reuse_svd ? 1 : 0, grid, st));
   eng->prof_end(&pr, st);
   eng->launches += 1;
 }
 
+void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
+  ProfRec pr;
+  eng->prof_begin(kStageScatter, st, &pr);
+  MPM_CK(launch_scatter(pool(), acc_out, grid_scatter, st));
+  eng->prof_end(&pr, st);
+  eng->launches += 1;
+}
+
+// One call: record + scatter of the first substep, then per substep the grid
+// update, the gather (which also records B for the next substep unless it is
+// the last) and the next scatter.  Regrouping happens after a scatter, every
+// `sort_interval` substeps.
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   if (need_regroup) regroup(true, st);
-  launch_pass(kP2G, false, acc_zero, st);
+  launch_gather_pass(kRecord, false, st);
+  launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
   const uint64_t total_cells = cells.high_water();
   uint32_t since = 0;
@@ -573,12 +588,15 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
     eng->launches += 1;
     const bool last = s + 1 == substeps;
     const bool due = !last && sort_interval > 0 && ++since >= sort_interval;
-    launch_pass(last ? kG2P : kG2P2G, due, a ^ 1, st);
-    if (due) {
-      regroup(false, st);
-      since = 0;
+    launch_gather_pass(last ? kG2P : kG2PRecord, due, st);
+    if (!last) {
+      launch_scatter_pass(a ^ 1, st);
+      if (due) {
+        regroup(false, st);
+        since = 0;
+      }
+      a ^= 1;
     }
-    if (!last) a ^= 1;
   }
   acc_last = a;
   acc_zero = a ^ 1;

@@ -65,7 +65,14 @@ template <class T> struct DevBuf {
 // Per-stage GPU timing (the equivalent of molla's MpmProfileStage timestamp
 // queries, crates/molla-solvers/src/mpm_profile.rs:8-80): when enabled, each
 // launch of a stage is bracketed by CUDA events on the launching stream.
-enum Stage : int { kStageOrdering = 0, kStageP2G = 1, kStageGrid = 2, kStageG2P2G = 3, kStageG2P = 4, kStages = 5 };
+enum Stage : int {
+  kStageOrdering = 0,  // keys, sorts, regroup, work list
+  kStageRecord = 1,    // first-substep stress record (SVD of F)
+  kStageGrid = 2,      // grid update
+  kStageGather = 3,    // G2P + F update + return mapping (+ record)
+  kStageScatter = 4,   // P2G deposit
+  kStages = 5
+};
 
 struct ProfRec {
   int stage;
@@ -150,6 +157,7 @@ class Group {
 
   // particle pool (double-buffered for the regroup)
   DevBuf<float> planes[2];
+  DevBuf<float> rec;  // per-slot scatter record (B matrix + flag), 10 planes
   DevBuf<uint32_t> meta[2], orig[2];
   DevBuf<uint32_t> slot_of, keys_by_id, key2, ids2, ks[2], vs[2], hist;
   // grid pool
@@ -181,7 +189,7 @@ class Group {
   double svd_tol32 = 1.0e-7;
   double svd_tol64 = 1.0e-9;
   int svd_sweeps = 16;
-  int grid_p2g = 0, grid_g2p = 0, grid_g2p2g = 0;
+  int grid_gather32 = 0, grid_gather64 = 0, grid_scatter = 0;
   uint64_t substeps_done = 0;
   uint64_t epoch = 1;  // bumps on every change that invalidates captured graphs
 
@@ -224,7 +232,8 @@ class Group {
  private:
   void rebuild_layout();
   void invalidate_graphs();
-  void launch_pass(int mode, bool keys, int acc_out, cudaStream_t st);
+  void launch_gather_pass(int mode, bool keys, cudaStream_t st);
+  void launch_scatter_pass(int acc_out, cudaStream_t st);
   void run_substeps(uint32_t substeps, cudaStream_t st);
   uint64_t graph_key(uint32_t substeps) const;
 };
