@@ -264,6 +264,24 @@ MPM_API int mpm_radix_sort_pairs(mpm_engine* engine, uint32_t* keys, uint32_t* v
 MPM_API int mpm_radix_sort_pairs_device(mpm_engine* engine, uint32_t* d_keys, uint32_t* d_values, uint32_t n,
                                 uint32_t key_bits, void* stream);
 
+/* Allocation-free variant of mpm_radix_sort_pairs_device; it has no
+ * counterpart in the reference.  It is for callers that cannot allocate
+ * device memory: code inside a stream-ordered pipeline that must not stall
+ * (cudaMalloc/cudaFree can synchronise the device), hosts that reserve the
+ * whole device budget up front, and hot paths held to an allocation-free
+ * guarantee.  Sorts d_keys/d_values (n pairs, device pointers on the current
+ * device) in place on `stream` (NULL: the default stream), stably by the low
+ * key_bits bits, using an 8.3 MiB scratch array that the library keeps in
+ * device memory for the whole process (every GPU that loads the library
+ * holds one).  n above 1,048,576 is rejected with MPM_ERR_INVALID.  It calls
+ * no allocation routine.  The first call on a device looks up the scratch
+ * array's address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the one scratch array, so calls that
+ * overlap on the GPU (different streams, not ordered) race and corrupt each
+ * other; order them on one stream or synchronise between them. */
+MPM_API int mpm_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values, uint32_t n, uint32_t key_bits,
+                                         void* stream);
+
 /* Number of CUDA kernel launches this library issued on the engine since
  * creation (host counter, the equivalent of gpu_metrics::record_dispatch,
  * crates/molla-core/src/gpu_metrics.rs:330-381). */

@@ -143,6 +143,7 @@ SIGNATURES = {
     "mpm_read_sort_permutation": (I, [P, U32P, U32P, U32]),
     "mpm_radix_sort_pairs": (I, [P, U32P, U32P, U32, U32]),
     "mpm_radix_sort_pairs_device": (I, [P, P, P, U32, U32, P]),
+    "mpm_radix_sort_pairs_noalloc": (I, [P, P, U32, U32, P]),
     "mpm_profile_enable": (I, [P, I]),
     "mpm_profile_read": (I, [P, C.POINTER(mpm_profile_stage), U32]),
     "mpm_profile_reset": (I, [P]),

@@ -68,6 +68,10 @@ mpm_rheology sand_row(float phi) {
 
 }  // namespace
 
+namespace mpm {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace mpm
+
 struct mpm_engine {
   std::unique_ptr<mpm::Engine> e;
 };

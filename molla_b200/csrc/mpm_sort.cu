@@ -14,8 +14,11 @@
 //     inside the tile with __match_any_sync and a per-warp prefix;
 //   * pass 0 can generate the identity values (0..n-1) itself.
 #include <cstdint>
+#include <mutex>
+#include <string>
 #include <cuda_runtime.h>
 
+#include "../../include/molla_mpm.h"
 #include "mpm_sort.cuh"
 
 namespace mpm {
@@ -203,4 +206,108 @@ cudaError_t radix_sort_pairs(cudaStream_t stream, const uint32_t* keys_in, const
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free sort: mpm_radix_sort_pairs_noalloc.
+//
+// For callers that cannot allocate device memory: code running inside a
+// stream-ordered pipeline that must not stall (cudaMalloc and cudaFree can
+// synchronise the device), hosts that reserve the whole device budget up
+// front and forbid allocations afterwards, and hot paths held to an
+// allocation-free guarantee.  The sort's ping-pong buffers and digit
+// histograms live in the file-scope array below (8.3 MiB, sized for
+// kNoAllocMaxPairs pairs); every GPU that loads this library holds it until
+// the process exits.
+
+constexpr uint32_t kNoAllocMaxPairs = 1u << 20;  // 1,048,576 (key, value) pairs
+constexpr size_t kNoAllocHistWords = (size_t)256 * ((kNoAllocMaxPairs + kSortTile - 1) / kSortTile) + 256;
+constexpr size_t kNoAllocWords = 2ull * kNoAllocMaxPairs + kNoAllocHistWords;
+
+// One key buffer, one value buffer and the histogram/digit totals.  In host
+// code this name is only a stand-in for the device array, never a device
+// address; the host obtains the address with cudaGetSymbolAddress.
+static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocWords];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device.
+cudaError_t noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    uint32_t* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_sort_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
 }  // namespace mpm
+
+extern "C" int mpm_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values, uint32_t n, uint32_t key_bits,
+                                            void* stream) {
+  using namespace mpm;
+  if (n > kNoAllocMaxPairs) {
+    set_last_error("mpm_radix_sort_pairs_noalloc: n=" + std::to_string(n) + " exceeds the allocation-free limit of " +
+                   std::to_string(kNoAllocMaxPairs) + " pairs; use mpm_radix_sort_pairs_device");
+    return MPM_ERR_INVALID;
+  }
+  if (key_bits < 1 || key_bits > 32) {
+    set_last_error("mpm_radix_sort_pairs_noalloc: key_bits must be in 1..=32");
+    return MPM_ERR_INVALID;
+  }
+  if (n == 0) {
+    set_last_error("");
+    return MPM_OK;
+  }
+  if (!d_keys || !d_values) {
+    set_last_error("mpm_radix_sort_pairs_noalloc: null device pointer");
+    return MPM_ERR_INVALID;
+  }
+  uint32_t* scratch = nullptr;
+  cudaError_t e = noalloc_scratch(&scratch);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("mpm_radix_sort_pairs_noalloc: scratch set-up failed: ") + cudaGetErrorString(e));
+    return MPM_ERR_GPU;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  uint32_t* skeys = scratch;
+  uint32_t* svals = scratch + kNoAllocMaxPairs;
+  uint32_t* hist = scratch + 2ull * kNoAllocMaxPairs;
+  const uint32_t nblocks = sort_blocks(n);
+  uint32_t* totals = hist + (size_t)256 * nblocks;
+  const int passes = ((int)key_bits + 7) / 8;
+  // Even passes read the caller's arrays and write the scratch, odd passes
+  // the reverse; every word of the histogram and totals is rewritten by each
+  // pass, so nothing has to be cleared between calls.
+  for (int p = 0; p < passes; ++p) {
+    const bool to_scratch = (p % 2) == 0;
+    const uint32_t* kin = to_scratch ? d_keys : skeys;
+    const uint32_t* vin = to_scratch ? d_values : svals;
+    uint32_t* kout = to_scratch ? skeys : d_keys;
+    uint32_t* vout = to_scratch ? svals : d_values;
+    k_hist<<<nblocks, kThreads, 0, st>>>(kin, n, 8 * p, nblocks, hist);
+    k_scan_digit<<<kBins, 1024, 0, st>>>(hist, nblocks, totals);
+    k_scatter<<<nblocks, kThreads, 0, st>>>(kin, vin, 0, kout, vout, n, 8 * p, nblocks, hist, totals);
+  }
+  if (passes % 2 == 1) {
+    cudaMemcpyAsync(d_keys, skeys, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d_values, svals, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(std::string("mpm_radix_sort_pairs_noalloc: ") + cudaGetErrorString(e));
+    return MPM_ERR_GPU;
+  }
+  set_last_error("");
+  return MPM_OK;
+}

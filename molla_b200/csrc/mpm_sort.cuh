@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace mpm {
@@ -21,5 +22,8 @@ size_t sort_hist_words(uint32_t n);
 cudaError_t radix_sort_pairs(cudaStream_t stream, const uint32_t* keys_in, const uint32_t* vals_in,
                              uint32_t* keys_a, uint32_t* keys_b, uint32_t* vals_a, uint32_t* vals_b, uint32_t* hist,
                              uint32_t n, int key_bits, uint32_t** keys_out, uint32_t** vals_out, uint64_t* launches);
+
+// Records the message returned by mpm_last_error on the calling thread.
+void set_last_error(const std::string& msg);
 
 }  // namespace mpm
