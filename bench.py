@@ -163,7 +163,7 @@ def make_workload(name: str, rank: int):
              "svd": "fp64", "l2": "inputs (2.6 GB state) exceed the 126 MB L2; no flush needed"}
     if name == "cube128":
         return scenes.cube_scene(grid_size=128, seed=rank), \
-            {"workload": "elastic cube scaled: 128^3 grid, 1M particles, E 1e4, FP32 + FP64 SVD, dt 1e-4",
+            {"workload": "elastic cube scaled: 128^3 grid, 1M particles, E 1e4, FP32 + FP64 SVD, dt 5e-5",
              "grid": 128, "particles": 1_000_000, "svd": "fp64",
              "l2": "state (160 MB) exceeds the 126 MB L2"}
     if name == "cube":

@@ -324,7 +324,8 @@ MPM_API int mpm_group_step_graph(mpm_group* group, uint32_t substeps, uint32_t r
 MPM_API int mpm_group_read_positions(mpm_group* group, uint32_t scene_id, float* out, uint32_t cap, uint32_t* count_out);
 MPM_API int mpm_group_read_status(mpm_group* group, uint32_t scene_id, mpm_status_info* out);
 MPM_API int mpm_group_scene_count(mpm_group* group, uint32_t* count);
-/* Group tuning: particles per work item and sort interval (0 → defaults). */
+/* Group tuning: regroup (sort) interval in substeps (0 → default 32).  The
+ * `chunk` argument is reserved (work items are whole 4^3 tiles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
 /* ---- serving ------------------------------------------------------------- */

@@ -100,7 +100,7 @@ struct mpm_sim {
   }
   void apply_group_settings() {
     group->svd_fp64 = cfg.svd_precision == MPM_SVD_FP64;
-    const uint32_t interval = order_enabled ? 1u : (sort_interval ? sort_interval : 16u);
+    const uint32_t interval = order_enabled ? 1u : (sort_interval ? sort_interval : 32u);
     group->sort_interval = interval;
   }
   void invalidate() { ++epoch; }
@@ -842,18 +842,8 @@ int mpm_group_scene_count(mpm_group* group, uint32_t* count) {
 int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval) {
   return guard([&] {
     REQUIRE(group, MPM_ERR_INVALID, "null group");
-    if (chunk) {
-      REQUIRE(chunk >= 32 && chunk <= 1u << 16, MPM_ERR_INVALID, "chunk must be in 32..=65536");
-      group->g->chunk = chunk;
-      group->g->need_regroup = true;
-      group->g->items.release();
-      group->g->epoch++;
-      group->g->graphs.clear();
-    }
-    group->g->sort_interval = sort_interval ? sort_interval : 16;
-    // re-size the work list for the new chunk
-    const size_t max_items = (size_t)group->g->cap / group->g->chunk + group->g->key_space + 2;
-    if (group->g->items.count < max_items) group->g->items.alloc(max_items);
+    (void)chunk;  // work items are whole 4^3 tiles
+    group->g->sort_interval = sort_interval ? sort_interval : 32;
   });
 }
 

@@ -47,7 +47,7 @@ constexpr int kRegionNodes = kRegion * kRegion * kRegion;
 constexpr int kRsy = 8;
 constexpr int kRsz = 68;
 constexpr int kRegionFloats = kRsz * kRegion;  // 544
-// Bits of the within-cell rank in the regroup key (tile, rank, cell).
+// Bits of the cell-in-tile part of the regroup key (tile, cell).
 constexpr int kCellBits = 6;
 
 struct MatDev {
@@ -94,7 +94,8 @@ struct PoolDev {
   uint32_t* keys_by_id; // sort key per identity (written when a regroup is due)
   float4* acc[2];       // grid accumulators (mass, momentum)
   float4* vel;          // grid velocity (vx, vy, vz, mass)
-  float* rec;           // 10 planes of cap floats: B (9) for the next scatter, deposit flag
+  float* rec;           // per slot 16 floats: (x, y, z, m), (m v, B0), (B1..B4), (B5..B8)
+  const uint32_t* slot_key;  // regroup key of each slot: (tile << 6) | cell in tile
   const SceneDev* scenes;
   uint32_t* status;     // kStatusWords per scene
   const Item* items;

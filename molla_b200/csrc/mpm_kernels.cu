@@ -49,9 +49,10 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
   const uint32_t sid = block_scene[g / kCellBlock];
   if (sid == 0xffffffffu) return;
   const SceneDev& sc = p.scenes[sid];
-  const uint64_t local = g - sc.grid_off;
+  const uint64_t local64 = g - sc.grid_off;
   const uint32_t n = sc.n;
-  if (local >= (uint64_t)n * n * n) return;
+  if (local64 >= (uint64_t)n * n * n) return;
+  const uint32_t local = (uint32_t)local64;  // grids hold fewer than 2^32 cells
   if (count_substep && local == 0) {
     uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
     if (*(volatile uint32_t*)status == 0u) atomicAdd(status + 1, 1u);
@@ -63,7 +64,8 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
   }
   float v[3] = {a.y / m, a.z / m, a.w / m};
   v[1] = v[1] + sc.dt * sc.gy;
-  const int ix = (int)(local % n), iy = (int)((local / n) % n), iz = (int)(local / ((uint64_t)n * n));
+  const uint32_t q = local / n;
+  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
   const int pad = sc.pad, nn = (int)n;
   const float f = sc.friction;
   if (sc.sticky) {
@@ -107,27 +109,6 @@ __global__ void k_keys(PoolDev p, uint32_t n_slots) {
   }
   const uint32_t tile = t[0] + sc.w * (t[1] + sc.w * t[2]);
   p.keys_by_id[p.orig[s]] = ((sc.key_off + tile) << kCellBits) | c[0] | (c[1] << 2) | (c[2] << 4);
-}
-
-// Second regroup key: from the (tile, cell)-sorted keys, the particle's rank
-// inside its cell; key = (tile, min(rank, 2^rank_bits - 1), cell) so that a
-// stable sort lists, per tile, the first particle of every cell, then the
-// second, and so on.  Copies the identities alongside.
-__global__ void k_rank_keys(const uint32_t* __restrict__ sorted, const uint32_t* __restrict__ ids, uint32_t n_live,
-                            int rank_bits, uint32_t* __restrict__ key2, uint32_t* __restrict__ ids2) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_live) return;
-  const uint32_t c = sorted[s];
-  uint32_t lo = 0, hi = s;
-  while (lo < hi) {
-    const uint32_t mid = lo + (hi - lo) / 2;
-    if (sorted[mid] < c) lo = mid + 1;
-    else hi = mid;
-  }
-  const uint32_t rmax = (1u << rank_bits) - 1u;
-  const uint32_t rank = min(s - lo, rmax);
-  key2[s] = ((c >> kCellBits) << (rank_bits + kCellBits)) | (rank << kCellBits) | (c & ((1u << kCellBits) - 1u));
-  ids2[s] = ids[s];
 }
 
 // set_particles_with_velocity (mpm.rs:1458-1519) into pool slots
@@ -182,10 +163,12 @@ __global__ void k_scene_keys(PoolDev p, uint32_t sid, const uint32_t* __restrict
 __global__ void k_reorder(const float* __restrict__ src, float* __restrict__ dst, uint32_t cap,
                           const uint32_t* __restrict__ meta_src, uint32_t* __restrict__ meta_dst,
                           uint32_t* __restrict__ orig_dst, uint32_t* __restrict__ slot_of,
-                          const uint32_t* __restrict__ ids, uint32_t n_live) {
+                          const uint32_t* __restrict__ ids, const uint32_t* __restrict__ keys,
+                          uint32_t* __restrict__ slot_key, uint32_t n_live) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_live) return;
   const uint32_t id = ids[s];
+  slot_key[s] = keys[s];
   const uint32_t old = slot_of[id];
 #pragma unroll
   for (int k = 0; k < kPlanes; ++k) dst[(size_t)k * cap + s] = src[(size_t)k * cap + old];
@@ -225,6 +208,7 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
     else hi = mid;
   }
   const uint32_t cnt = b - a;
+  chunk = chunk ? chunk : cnt;
   const uint32_t pieces = (cnt + chunk - 1) / chunk;
   const uint32_t base = atomicAdd(n_items, pieces);
   for (uint32_t i = 0; i < pieces; ++i) {
@@ -340,17 +324,11 @@ cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* sl
 }
 
 cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
-                           uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, uint32_t n_live,
-                           cudaStream_t st) {
+                           uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, const uint32_t* keys,
+                           uint32_t* slot_key, uint32_t n_live, cudaStream_t st) {
   if (!n_live) return cudaSuccess;
-  k_reorder<<<(n_live + 255) / 256, 256, 0, st>>>(src, dst, cap, meta_src, meta_dst, orig_dst, slot_of, ids, n_live);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_rank_keys(const uint32_t* sorted, const uint32_t* ids, uint32_t n_live, int rank_bits,
-                             uint32_t* key2, uint32_t* ids2, cudaStream_t st) {
-  if (!n_live) return cudaSuccess;
-  k_rank_keys<<<(n_live + 255) / 256, 256, 0, st>>>(sorted, ids, n_live, rank_bits, key2, ids2);
+  k_reorder<<<(n_live + 255) / 256, 256, 0, st>>>(src, dst, cap, meta_src, meta_dst, orig_dst, slot_of, ids, keys,
+                                                  slot_key, n_live);
   return cudaGetLastError();
 }
 

@@ -8,6 +8,8 @@
 namespace mpm {
 
 constexpr int kParticleThreads = 256;
+constexpr int kGatherThreads = 128;
+constexpr int kScatterThreads = 192;  // 64 cells x 3 x-slabs of one tile
 constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 256-cell block
 
 enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
@@ -29,10 +31,8 @@ cudaError_t launch_set_material_ids(const PoolDev& p, const uint32_t* slot_of, u
 cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* slot_of, uint32_t id0, uint32_t n,
                               uint32_t* keys, cudaStream_t st);
 cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
-                           uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, uint32_t n_live,
-                           cudaStream_t st);
-cudaError_t launch_rank_keys(const uint32_t* sorted, const uint32_t* ids, uint32_t n_live, int rank_bits,
-                             uint32_t* key2, uint32_t* ids2, cudaStream_t st);
+                           uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, const uint32_t* keys,
+                           uint32_t* slot_key, uint32_t n_live, cudaStream_t st);
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
                          Item* items, uint32_t* n_items, cudaStream_t st);

@@ -63,7 +63,7 @@ __device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base
 // substep of a call), kG2PRecord (gather + return mapping + B for the next
 // scatter, with the return mapping's SVD reused).
 template <int MODE, bool WRITE_KEYS, class SR>
-__global__ void __launch_bounds__(kParticleThreads, 2) k_gather(PoolDev p, double tol, int sweeps, int reuse_svd) {
+__global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol, int sweeps, int reuse_svd) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   __shared__ __align__(16) SceneDev s_sc;
@@ -78,27 +78,28 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_gather(PoolDev p, doubl
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
       for (int k = threadIdx.x; k < (int)(sizeof(SceneDev) / 4); k += blockDim.x) dst[k] = src[k];
     }
-    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)(p.status + (size_t)item.scene * kStatusWords);
-    __syncthreads();
-    const SceneDev& sc = s_sc;
-    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
-    const uint32_t tx = item.tile % sc.w, ty = (item.tile / sc.w) % sc.w, tz = item.tile / (sc.w * sc.w);
+    const SceneDev* __restrict__ scp = p.scenes + item.scene;
+    uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
+    const uint32_t fault0 = *(volatile uint32_t*)status;
+    const uint32_t w = scp->w;
+    const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
-    const int n = (int)sc.n;
-    const bool faulted = s_fault != 0;
+    const int n = (int)scp->n;
     if constexpr (kGather) {
-      if (!faulted) {
-        const float4* __restrict__ gvel = p.vel + sc.grid_off;
-        for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-          const int ix = rx + (r & 7), iy = ry + ((r >> 3) & 7), iz = rz + (r >> 6);
-          float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
-            g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
-          s_gath.vel[r] = g;
-        }
+      // Stage the 8^3-node velocity block (out-of-grid nodes read as zero).
+      const float4* __restrict__ gvel = p.vel + scp->grid_off;
+      for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
+        const int ix = rx + (r & 7), iy = ry + ((r >> 3) & 7), iz = rz + (r >> 6);
+        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+        if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
+          g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+        s_gath.vel[r] = g;
       }
     }
+    if (threadIdx.x == 0) s_fault = fault0;
     __syncthreads();
+    const SceneDev& sc = s_sc;
+    const bool faulted = s_fault != 0;
     if (!faulted) {
       for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
         const uint32_t s = item.start + k;
@@ -314,9 +315,15 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_gather(PoolDev p, doubl
             }
             p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
           }
-#pragma unroll
-          for (int i = 0; i < 9; ++i) p.rec[(size_t)i * p.cap + s] = B[i];
-          p.rec[(size_t)9 * p.cap + s] = ok ? 1.f : 0.f;
+          // Packed record (x, y, z, m), (m v, B0), (B1..B4), (B5..B8); a
+          // faulted particle gets m = 0 and deposits nothing.
+          const float mr = ok ? mass : 0.f;
+          const float vx = ok ? mass * v[0] : 0.f, vy = ok ? mass * v[1] : 0.f, vz = ok ? mass * v[2] : 0.f;
+          float4* r4 = reinterpret_cast<float4*>(p.rec) + 4 * (size_t)s;
+          r4[0] = make_float4(x, y, z, mr);
+          r4[1] = make_float4(vx, vy, vz, B[0]);
+          r4[2] = make_float4(B[1], B[2], B[3], B[4]);
+          r4[3] = make_float4(B[5], B[6], B[7], B[8]);
         }
         if constexpr (WRITE_KEYS) {
           const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
@@ -332,16 +339,29 @@ __global__ void __launch_bounds__(kParticleThreads, 2) k_gather(PoolDev p, doubl
   }
 }
 
-// Scatter of the next substep (mpm.wgsl:601-627): particle at slot s with
-// base = floor(x/dx - 0.5) and fx = x/dx - base deposits, at the node of
-// offset (i,j,k), w m and w (m v + B d), d = ((i,j,k) - fx) dx, w the
+// Scatter of the next substep (mpm.wgsl:601-627): a particle with base =
+// floor(x/dx - 0.5) and fx = x/dx - base deposits, at the node of offset
+// (i,j,k), w m and w (m v + B d) with d = ((i,j,k) - fx) dx and w the
 // quadratic B-spline weight.  Particles whose record flag is zero (numerical
 // fault this substep) deposit nothing.
-__global__ void __launch_bounds__(kParticleThreads, 4) k_scatter(PoolDev p, int acc_out) {
+//
+// One CTA per tile item, 192 threads: thread t owns cell (t mod 64) of the
+// tile and the x-slab i = t / 64 of the stencil.  It walks the particles the
+// last regrouping put in its cell (contiguous slots), adds their nine slab-i
+// node contributions in registers and then issues 9 x 4 shared-memory atomics
+// for the whole cell — about eight times fewer atomics than one per particle
+// and node, and conflict-free because the 32 lanes of a warp own 32
+// different cells.  A particle that has left its cell since the regrouping
+// deposits its own contributions directly.
+__global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_out) {
   __shared__ float s_acc[4][kRegionFloats];
+  __shared__ uint32_t s_first[64], s_end[64];
+  __shared__ uint8_t s_order[64];
   __shared__ uint32_t s_fault;
   float4* __restrict__ acc = p.acc[acc_out];
+  const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
   const uint32_t n_items = *p.n_items;
+  const int slab = threadIdx.x >> 6;
   for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
     const Item item = p.items[it];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
@@ -359,68 +379,145 @@ __global__ void __launch_bounds__(kParticleThreads, 4) k_scatter(PoolDev p, int 
       s_acc[2][r] = 0.f;
       s_acc[3][r] = 0.f;
     }
+    if (threadIdx.x < 64) {
+      s_first[threadIdx.x] = 0;
+      s_end[threadIdx.x] = 0;
+    }
     __syncthreads();
-    // A fault latched before this launch (by an earlier substep) freezes the
-    // scene; one latched by this substep's gather is handled per particle.
-    const bool faulted = s_fault != 0;
-    for (uint32_t k = threadIdx.x; k < item.count && !faulted; k += blockDim.x) {
+    // Cell segments of this item from the regroup keys (sorted by cell).
+    for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
       const uint32_t s = item.start + k;
-      if (p.rec[(size_t)9 * p.cap + s] == 0.f) continue;
-      const float xp[3] = {(plane(p, PX)[s] - ox) * inv_dx, (plane(p, PY)[s] - oy) * inv_dx,
-                           (plane(p, PZ)[s] - oz) * inv_dx};
-      const float mass = plane(p, MASS)[s];
-      const float mv[3] = {mass * plane(p, VX)[s], mass * plane(p, VY)[s], mass * plane(p, VZ)[s]};
-      float B[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) B[i] = p.rec[(size_t)i * p.cap + s];
-      float wgt[3][3], d[3][3];
-      int base[3];
-      const int win[3] = {winx, winy, winz};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float bf = floorf(xp[a] - 0.5f);
-        base[a] = (int)bf - win[a];
-        const float fx = xp[a] - bf;
-        quad_weights(fx, wgt[a]);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * dx;
+      const uint32_t c = p.slot_key[s] & 63u;
+      if (k == 0 || (p.slot_key[s - 1] & 63u) != c) s_first[c] = s;
+      if (k + 1 == item.count || (p.slot_key[s + 1] & 63u) != c) s_end[c] = s + 1;
+    }
+    __syncthreads();
+    // Cells ranked by particle count (descending, ties by cell index) so
+    // that each warp walks cells of similar length.
+    if (threadIdx.x < 64) {
+      const int c = threadIdx.x;
+      const uint32_t my = s_end[c] - s_first[c];
+      int rank = 0;
+      for (int o = 0; o < 64; ++o) {
+        const uint32_t other = s_end[o] - s_first[o];
+        rank += (other > my) || (other == my && o < c);
       }
-      const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
-      const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
-                          (unsigned)lz0 <= (unsigned)(kRegion - 3);
+      s_order[rank] = (uint8_t)c;
+    }
+    __syncthreads();
+    // A fault latched before this launch freezes the scene; one latched by
+    // this substep's gather is handled per particle (m = 0 in its record).
+    if (s_fault == 0) {
+      const int cell = s_order[threadIdx.x & 63];
+      const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+      // base of this cell's particles in region coordinates
+      const int lbx = 1 + cx, lby = 1 + cy, lbz = 1 + cz;
+      float am[9], apx[9], apy[9], apz[9];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const float qx[3] = {mv[0] + B[0] * d[0][i], mv[1] + B[1] * d[0][i], mv[2] + B[2] * d[0][i]};
+      for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
+      const uint32_t first = s_first[cell], end = s_end[cell];
+      const int win[3] = {winx, winy, winz};
+      // The next particle's record is loaded while this one is deposited.
+      float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0, n2 = n0, n3 = n0;
+      if (first < end) {
+        n0 = __ldg(&rec[4 * (size_t)first]);
+        n1 = __ldg(&rec[4 * (size_t)first + 1]);
+        n2 = __ldg(&rec[4 * (size_t)first + 2]);
+        n3 = __ldg(&rec[4 * (size_t)first + 3]);
+      }
+      for (uint32_t s = first; s < end; ++s) {
+        const float4 r0 = n0, r1 = n1, r2 = n2, r3 = n3;
+        if (s + 1 < end) {
+          n0 = __ldg(&rec[4 * (size_t)s + 4]);
+          n1 = __ldg(&rec[4 * (size_t)s + 5]);
+          n2 = __ldg(&rec[4 * (size_t)s + 6]);
+          n3 = __ldg(&rec[4 * (size_t)s + 7]);
+        }
+        if (r0.w == 0.f) continue;
+        const float mass = r0.w;
+        const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+        const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
+        float wgt[3][3], fx[3];
+        int base[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float bf = floorf(xp[a] - 0.5f);
+          base[a] = (int)bf - win[a];
+          fx[a] = xp[a] - bf;
+          quad_weights(fx[a], wgt[a]);
+        }
+        const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+        // slab i of the stencil: x offset i, all (j, k)
+        const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
+        const float di = ((float)slab - fx[0]) * dx;
+        const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
+        float nm[9], npx[9], npy[9], npz[9];
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-          const float wij = wgt[0][i] * wgt[1][j];
-          const float qy[3] = {qx[0] + B[3] * d[1][j], qx[1] + B[4] * d[1][j], qx[2] + B[5] * d[1][j]};
+          const float wij = wi * wgt[1][j];
+          const float dj = ((float)j - fx[1]) * dx;
+          const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
 #pragma unroll
           for (int kk = 0; kk < 3; ++kk) {
             const float wt = wij * wgt[2][kk];
-            const float dm = wt * mass;
-            const float px = wt * (qy[0] + B[6] * d[2][kk]);
-            const float py = wt * (qy[1] + B[7] * d[2][kk]);
-            const float pz = wt * (qy[2] + B[8] * d[2][kk]);
-            if (inside) {
-              const int r = region_index(lx0 + i, ly0 + j, lz0 + kk);
-              atomicAdd(&s_acc[0][r], dm);
-              atomicAdd(&s_acc[1][r], px);
-              atomicAdd(&s_acc[2][r], py);
-              atomicAdd(&s_acc[3][r], pz);
-            } else {
-              const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + kk;
-              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-                const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-                atomicAdd(&acc[c], make_float4(dm, px, py, pz));
-              }
-            }
+            const float dk = ((float)kk - fx[2]) * dx;
+            nm[3 * j + kk] = wt * mass;
+            npx[3 * j + kk] = wt * (qy[0] + B[6] * dk);
+            npy[3 * j + kk] = wt * (qy[1] + B[7] * dk);
+            npz[3 * j + kk] = wt * (qy[2] + B[8] * dk);
           }
         }
+        if (lx0 == lbx && ly0 == lby && lz0 == lbz) {
+#pragma unroll
+          for (int q = 0; q < 9; ++q) {
+            am[q] += nm[q];
+            apx[q] += npx[q];
+            apy[q] += npy[q];
+            apz[q] += npz[q];
+          }
+        } else if ((unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
+                   (unsigned)lz0 <= (unsigned)(kRegion - 3)) {
+          // left its cell since the regrouping, still inside the block
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              const int r = region_index(lx0 + slab, ly0 + j, lz0 + kk);
+              atomicAdd(&s_acc[0][r], nm[3 * j + kk]);
+              atomicAdd(&s_acc[1][r], npx[3 * j + kk]);
+              atomicAdd(&s_acc[2][r], npy[3 * j + kk]);
+              atomicAdd(&s_acc[3][r], npz[3 * j + kk]);
+            }
+        } else {
+          // outside the block: straight to HBM
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              const int ix = base[0] + slab, iy = base[1] + j, iz = base[2] + kk;
+              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+                const uint64_t c =
+                    grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+                atomicAdd(&acc[c], make_float4(nm[3 * j + kk], npx[3 * j + kk], npy[3 * j + kk], npz[3 * j + kk]));
+              }
+            }
+        }
+      }
+      if (end > first) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            const int r = region_index(lbx + slab, lby + j, lbz + kk);
+            atomicAdd(&s_acc[0][r], am[3 * j + kk]);
+            atomicAdd(&s_acc[1][r], apx[3 * j + kk]);
+            atomicAdd(&s_acc[2][r], apy[3 * j + kk]);
+            atomicAdd(&s_acc[3][r], apz[3 * j + kk]);
+          }
       }
     }
     __syncthreads();
-    if (!faulted) {
+    if (s_fault == 0) {
       for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
         const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
         const int q = region_index(lx, ly, lz);
@@ -442,7 +539,7 @@ __global__ void __launch_bounds__(kParticleThreads, 4) k_scatter(PoolDev p, int 
 
 template <int MODE, bool KEYS, class SR>
 static cudaError_t launch_gather_t(const PoolDev& p, double tol, int sweeps, int reuse, int grid, cudaStream_t st) {
-  k_gather<MODE, KEYS, SR><<<grid, kParticleThreads, 0, st>>>(p, tol, sweeps, reuse);
+  k_g2p<MODE, KEYS, SR><<<grid, kGatherThreads, 0, st>>>(p, tol, sweeps, reuse);
   return cudaGetLastError();
 }
 
@@ -465,25 +562,25 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
 }
 
 cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st) {
-  k_scatter<<<grid, kParticleThreads, 0, st>>>(p, acc_out);
+  k_p2g<<<grid, kScatterThreads, 0, st>>>(p, acc_out);
   return cudaGetLastError();
 }
 
-static int persistent(const void* fn) {
+static int persistent(const void* fn, int threads) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kParticleThreads, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   if (sms < 1) sms = 148;
   return sms * per_sm;
 }
 
 int gather_grid_size(bool svd_fp64) {
-  return svd_fp64 ? persistent((const void*)k_gather<kG2PRecord, false, double>)
-                  : persistent((const void*)k_gather<kG2PRecord, false, float>);
+  return svd_fp64 ? persistent((const void*)k_g2p<kG2PRecord, false, double>, kGatherThreads)
+                  : persistent((const void*)k_g2p<kG2PRecord, false, float>, kGatherThreads);
 }
 
-int scatter_grid_size() { return persistent((const void*)k_scatter); }
+int scatter_grid_size() { return persistent((const void*)k_p2g, kScatterThreads); }
 
 }  // namespace mpm

@@ -226,7 +226,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaSetDevice(eng->device));
   planes[0].alloc((size_t)kPlanes * cap);
   planes[1].alloc((size_t)kPlanes * cap);
-  rec.alloc((size_t)10 * cap);
+  rec.alloc((size_t)16 * cap);
   for (int i = 0; i < 2; ++i) {
     meta[i].alloc(cap);
     orig[i].alloc(cap);
@@ -236,8 +236,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   }
   slot_of.alloc(cap);
   keys_by_id.alloc(cap);
-  key2.alloc(cap);
-  ids2.alloc(cap);
+  slot_key.alloc(cap);
   hist.alloc(sort_hist_words(cap));
   vel.alloc(cell_cap);
   block_scene.alloc(cell_cap / kCellBlock);
@@ -289,6 +288,7 @@ PoolDev Group::pool() const {
   p.acc[1] = acc[1].ptr;
   p.vel = vel.ptr;
   p.rec = rec.ptr;
+  p.slot_key = slot_key.ptr;
   p.scenes = scenes_d.ptr;
   p.status = status_d.ptr;
   p.items = items.ptr;
@@ -325,7 +325,7 @@ void Group::rebuild_layout() {
   }
   key_space = (uint32_t)k;
   if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
-  const size_t max_items = (size_t)cap / std::max<uint32_t>(chunk, 1) + key_space + 2;
+  const size_t max_items = (size_t)key_space + 2;  // one item per occupied tile
   if (items.count < max_items) items.alloc(max_items);
   if (!offs.empty()) {
     MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -515,12 +515,12 @@ static int bits_for(uint64_t values) {
   return b;
 }
 
-// Regrouping: sort (base-cell key, identity) stably, rank each particle
-// inside its cell, then sort again by (tile, rank, cell) so that each tile's
-// particles are listed rank-major (one particle of every cell, then the
-// next).  Consecutive slots — the lanes of a warp — then hold particles of
-// different base cells.  The particle state is physically moved to that order
-// and the work list is rebuilt from the tile boundaries.
+// Regrouping: sort (base-cell key, identity) stably — key = (scene tile
+// offset + 4^3 tile of the base cell, cell inside the tile) — and move the
+// particle state to that order, so that each tile's particles are
+// contiguous and, inside the tile, grouped by base cell.  The sorted key of
+// every slot is kept for the scatter, and the work list is rebuilt from the
+// tile boundaries.
 void Group::regroup(bool compute_keys, cudaStream_t st) {
   ProfRec pr;
   eng->prof_begin(kStageOrdering, st, &pr);
@@ -531,21 +531,14 @@ void Group::regroup(bool compute_keys, cudaStream_t st) {
   const uint32_t n_sort = (uint32_t)ids.high_water();
   uint32_t* skeys = nullptr;
   uint32_t* sids = nullptr;
-  const int key1_bits = bits_for((uint64_t)key_space << kCellBits);
   MPM_CK(radix_sort_pairs(st, keys_by_id.ptr, nullptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n_sort,
-                          key1_bits, &skeys, &sids, &eng->launches));
-  const int tile_bits = bits_for(key_space);
-  const int rank_bits = std::max(0, std::min(4, 31 - kCellBits - tile_bits));
-  MPM_CK(launch_rank_keys(skeys, sids, n_live, rank_bits, key2.ptr, ids2.ptr, st));
-  eng->launches += 1;
-  MPM_CK(radix_sort_pairs(st, key2.ptr, ids2.ptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n_live,
-                          tile_bits + rank_bits + kCellBits, &skeys, &sids, &eng->launches));
+                          bits_for((uint64_t)key_space << kCellBits), &skeys, &sids, &eng->launches));
   MPM_CK(launch_reorder(planes[cur].ptr, planes[cur ^ 1].ptr, cap, meta[cur].ptr, meta[cur ^ 1].ptr,
-                        orig[cur ^ 1].ptr, slot_of.ptr, sids, n_live, st));
+                        orig[cur ^ 1].ptr, slot_of.ptr, sids, skeys, slot_key.ptr, n_live, st));
   eng->launches += 1;
   cur ^= 1;
-  MPM_CK(launch_items(skeys, rank_bits + kCellBits, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(),
-                      scene_ids_d.ptr, chunk, items.ptr, n_items.ptr, st));
+  MPM_CK(launch_items(skeys, kCellBits, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(),
+                      scene_ids_d.ptr, 0, items.ptr, n_items.ptr, st));
   eng->launches += key_space ? 2 : 1;
   need_regroup = false;
   eng->prof_end(&pr, st);

@@ -157,9 +157,9 @@ class Group {
 
   // particle pool (double-buffered for the regroup)
   DevBuf<float> planes[2];
-  DevBuf<float> rec;  // per-slot scatter record (B matrix + flag), 10 planes
+  DevBuf<float> rec;  // per-slot scatter record, 16 floats (64 B) per slot
   DevBuf<uint32_t> meta[2], orig[2];
-  DevBuf<uint32_t> slot_of, keys_by_id, key2, ids2, ks[2], vs[2], hist;
+  DevBuf<uint32_t> slot_of, keys_by_id, slot_key, ks[2], vs[2], hist;
   // grid pool
   DevBuf<float4> acc[2], vel;
   DevBuf<uint32_t> block_scene;
@@ -182,7 +182,7 @@ class Group {
   bool need_regroup = true;
   bool scenes_dirty = true;
   bool keys_dirty = true;  // scene key offsets changed
-  uint32_t sort_interval = 16;
+  uint32_t sort_interval = 32;
   uint32_t chunk = 512;
   bool svd_fp64 = false;
   bool reuse_svd = true;

@@ -30,7 +30,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kRounds = kSortTile / kThreads;  // 16
 constexpr int kBins = 256;
 
-__global__ void __launch_bounds__(kThreads) k_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
+__global__ void __launch_bounds__(kThreads) k_sort_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
                                                    uint32_t nblocks, uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_h[kBins + 1];
   const int tid = threadIdx.x;
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kThreads) k_hist(const uint32_t* __restrict__ 
 
 // One CTA per digit: exclusive scan of hist[d][0..nblocks) in place, total to
 // totals[d].
-__global__ void __launch_bounds__(1024) k_scan_digit(uint32_t* __restrict__ hist, uint32_t nblocks,
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* __restrict__ hist, uint32_t nblocks,
                                                      uint32_t* __restrict__ totals) {
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(1024) k_scan_digit(uint32_t* __restrict__ hist
   if (tid == 0) totals[blockIdx.x] = s_carry;
 }
 
-__global__ void __launch_bounds__(kThreads) k_scatter(const uint32_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kThreads) k_sort_scatter(const uint32_t* __restrict__ keys_in,
                                                       const uint32_t* __restrict__ vals_in, int iota,
                                                       uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                                                       uint32_t n, int shift, uint32_t nblocks,
@@ -193,9 +193,9 @@ cudaError_t radix_sort_pairs(cudaStream_t stream, const uint32_t* keys_in, const
     const int shift = 8 * p;
     kout = (p % 2 == 0) ? keys_a : keys_b;
     vout = (p % 2 == 0) ? vals_a : vals_b;
-    k_hist<<<nblocks, kThreads, 0, stream>>>(kin, n, shift, nblocks, hist);
-    k_scan_digit<<<kBins, 1024, 0, stream>>>(hist, nblocks, totals);
-    k_scatter<<<nblocks, kThreads, 0, stream>>>(kin, vin, iota, kout, vout, n, shift, nblocks, hist, totals);
+    k_sort_hist<<<nblocks, kThreads, 0, stream>>>(kin, n, shift, nblocks, hist);
+    k_sort_scan<<<kBins, 1024, 0, stream>>>(hist, nblocks, totals);
+    k_sort_scatter<<<nblocks, kThreads, 0, stream>>>(kin, vin, iota, kout, vout, n, shift, nblocks, hist, totals);
     if (launches) *launches += 3;
     kin = kout;
     vin = vout;
@@ -295,9 +295,9 @@ extern "C" int mpm_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values
     const uint32_t* vin = to_scratch ? d_values : svals;
     uint32_t* kout = to_scratch ? skeys : d_keys;
     uint32_t* vout = to_scratch ? svals : d_values;
-    k_hist<<<nblocks, kThreads, 0, st>>>(kin, n, 8 * p, nblocks, hist);
-    k_scan_digit<<<kBins, 1024, 0, st>>>(hist, nblocks, totals);
-    k_scatter<<<nblocks, kThreads, 0, st>>>(kin, vin, 0, kout, vout, n, 8 * p, nblocks, hist, totals);
+    k_sort_hist<<<nblocks, kThreads, 0, st>>>(kin, n, 8 * p, nblocks, hist);
+    k_sort_scan<<<kBins, 1024, 0, st>>>(hist, nblocks, totals);
+    k_sort_scatter<<<nblocks, kThreads, 0, st>>>(kin, vin, 0, kout, vout, n, 8 * p, nblocks, hist, totals);
   }
   if (passes % 2 == 1) {
     cudaMemcpyAsync(d_keys, skeys, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);

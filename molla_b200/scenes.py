@@ -71,13 +71,17 @@ def _lattice(lo, count, h, rng, jitter=0.5):
 
 
 def cube_scene(grid_size: int = 64, per_axis: int | None = None, seed: int = 0, walls: int = 0,
-               youngs: float = 1.0e4, poisson: float = 0.2, rho: float = 1.0, dt: float = 1.0e-4,
+               youngs: float = 1.0e4, poisson: float = 0.2, rho: float = 1.0, dt: float | None = None,
                steps: int = 1000) -> Scene:
     """Elastic cube [0.3, 0.7]^3 in the unit box on a 2x2x2-per-cell lattice.
 
     64^3 → 51 particles per axis (132,651); 128^3 defaults to 100 per axis
-    (1,000,000)."""
+    (1,000,000).  dt defaults to 1e-4 at 64^3 (CFL number c_p dt / dx = 0.67
+    for E = 1e4, nu = 0.2, rho = 1) and scales with dx, keeping the same CFL
+    number on finer grids (5e-5 at 128^3)."""
     dx = 1.0 / grid_size
+    if dt is None:
+        dt = 1.0e-4 * 64.0 / grid_size
     if per_axis is None:
         per_axis = 51 if grid_size == 64 else (100 if grid_size == 128 else int(0.4 * grid_size * 2))
     h = 0.4 / per_axis
