@@ -193,9 +193,12 @@ MPM_API int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters
 /* set_p2g_mode (mpm.rs:1642-1650).  Both reference modes map to the same
  * tile-accumulated scatter here; the flag is kept for API parity. */
 MPM_API int mpm_set_p2g_mode(mpm_sim* sim, int two_pass);
-/* set_deterministic_p2g (mpm_deterministic_p2g.rs:550-569): fixed-order
- * grid-centric P2G over the tile-sorted particles, bit-repeatable.
- * Requires prepared and enabled particle ordering (as the reference). */
+/* prepare_deterministic_p2g / set_deterministic_p2g
+ * (mpm_deterministic_p2g.rs:419-569): fixed-order P2G over particles
+ * regrouped by tile after every gather; results are bit-repeatable.
+ * Enabling requires a prepare call and enabled particle ordering (as the
+ * reference).  A deposit that left the fixed order (positions set outside
+ * the grid) sets bit 4 of the status word. */
 MPM_API int mpm_prepare_deterministic_p2g(mpm_sim* sim);
 MPM_API int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled);
 
@@ -324,6 +327,25 @@ MPM_API int mpm_group_step_graph(mpm_group* group, uint32_t substeps, uint32_t r
 MPM_API int mpm_group_read_positions(mpm_group* group, uint32_t scene_id, float* out, uint32_t cap, uint32_t* count_out);
 MPM_API int mpm_group_read_status(mpm_group* group, uint32_t scene_id, mpm_status_info* out);
 MPM_API int mpm_group_scene_count(mpm_group* group, uint32_t* count);
+/* Fixed-order (deterministic) P2G for every scene of the group: a scene's
+ * results are then bit-identical from run to run and alone or in any mix
+ * (the group equivalent of mpm_set_deterministic_p2g). */
+MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
+/* Fixed-order (deterministic) P2G for every scene of the group: a scene's
+ * results are then bit-identical from run to run and alone or in any mix
+ * (the group equivalent of mpm_set_deterministic_p2g). */
+MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
+/* Autotuner: times `probe_substeps` substeps of the group for each candidate
+ * regrouping interval (n_candidates values, NULL → {4, 8, 16, 32, 64, 128})
+ * on a snapshot of the device state, restores the state (the scenes do not
+ * advance) and keeps the fastest interval.  ms_per_substep (may be NULL)
+ * receives one timing per candidate; *chosen the interval kept. */
+MPM_API int mpm_group_autotune(mpm_group* group, uint32_t probe_substeps, const uint32_t* candidates,
+                               uint32_t n_candidates, float* ms_per_substep, uint32_t* chosen);
+/* The same for a single simulation (mpm_set_sort_interval is then the
+ * tuned value). */
+MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const uint32_t* candidates,
+                         uint32_t n_candidates, float* ms_per_substep, uint32_t* chosen);
 /* Group tuning: regroup (sort) interval in substeps (0 → default 32).  The
  * `chunk` argument is reserved (work items are whole 4^3 tiles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);

@@ -397,6 +397,16 @@ class MpmSimulation:
     def set_sort_interval(self, interval: int):
         _check(_ffi.lib().mpm_set_sort_interval(self._h, interval))
 
+    def autotune(self, dt: float, probe_substeps: int = 64, candidates=(4, 8, 16, 32, 64, 128)):
+        """Picks the regrouping interval by timing each candidate on a
+        snapshot of the state (the simulation does not advance).  Returns
+        (chosen, {candidate: ms per substep})."""
+        c = np.ascontiguousarray(np.asarray(candidates, np.uint32))
+        ms = np.zeros(len(c), np.float32)
+        chosen = C.c_uint32()
+        _check(_ffi.lib().mpm_autotune(self._h, dt, probe_substeps, _up(c), len(c), _fp(ms), C.byref(chosen)))
+        return int(chosen.value), dict(zip(c.tolist(), ms.tolist()))
+
     # -- stepping -----------------------------------------------------------
     def step(self, dt: float, engine=None):
         self.step_n(dt, 1)
@@ -526,6 +536,19 @@ class MpmGroup:
 
     def tune(self, chunk: int = 0, sort_interval: int = 0):
         _check(_ffi.lib().mpm_group_tune(self._h, chunk, sort_interval))
+
+    def set_deterministic(self, enabled: bool):
+        _check(_ffi.lib().mpm_group_set_deterministic(self._h, int(bool(enabled))))
+
+    def autotune(self, probe_substeps: int = 64, candidates=(4, 8, 16, 32, 64, 128)):
+        """Picks the regrouping interval by timing each candidate on a
+        snapshot of the state (the scenes do not advance).  Returns
+        (chosen, {candidate: ms per substep})."""
+        c = np.ascontiguousarray(np.asarray(candidates, np.uint32))
+        ms = np.zeros(len(c), np.float32)
+        chosen = C.c_uint32()
+        _check(_ffi.lib().mpm_group_autotune(self._h, probe_substeps, _up(c), len(c), _fp(ms), C.byref(chosen)))
+        return int(chosen.value), dict(zip(c.tolist(), ms.tolist()))
 
     def read_positions(self, sid: int) -> np.ndarray:
         n = self.counts[sid]

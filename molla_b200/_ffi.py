@@ -157,6 +157,9 @@ SIGNATURES = {
     "mpm_group_read_positions": (I, [P, U32, F32P, U32, U32P]),
     "mpm_group_read_status": (I, [P, U32, C.POINTER(mpm_status_info)]),
     "mpm_group_scene_count": (I, [P, U32P]),
+    "mpm_group_set_deterministic": (I, [P, I]),
+    "mpm_group_autotune": (I, [P, U32, U32P, U32, F32P, U32P]),
+    "mpm_autotune": (I, [P, C.c_float, U32, U32P, U32, F32P, U32P]),
     "mpm_group_tune": (I, [P, U32, U32]),
     "mpm_server_create": (I, [P, U64, U32, PP]),
     "mpm_server_destroy": (I, [P]),

@@ -424,6 +424,7 @@ int mpm_set_p2g_mode(mpm_sim* sim, int two_pass) {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
     (void)two_pass;
     sim->det_enabled = false;
+    sim->group->set_deterministic(false);
     sim->invalidate();
   });
 }
@@ -431,19 +432,21 @@ int mpm_set_p2g_mode(mpm_sim* sim, int two_pass) {
 int mpm_prepare_deterministic_p2g(mpm_sim* sim) {
   return guard([&] {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
-    throw Error(MPM_ERR_UNSUPPORTED, "deterministic fixed-order P2G is not available in this build yet");
+    sim->det_prepared = true;
+    sim->invalidate();
   });
 }
 
 int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled) {
   return guard([&] {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
-    if (!enabled) {
-      sim->det_enabled = false;
-      return;
-    }
-    REQUIRE(sim->det_prepared && sim->order_enabled, MPM_ERR_INVALID,
-            "Deterministic P2G requires prepared gather, active or native dense grid, ordering and no deferred scatter");
+    if (enabled)
+      REQUIRE(sim->det_prepared && sim->order_enabled, MPM_ERR_INVALID,
+              "Deterministic P2G requires prepared gather, active or native dense grid, ordering and no deferred "
+              "scatter");
+    sim->det_enabled = enabled != 0;
+    sim->group->set_deterministic(sim->det_enabled);
+    sim->invalidate();
   });
 }
 
@@ -832,6 +835,50 @@ int mpm_group_read_status(mpm_group* group, uint32_t scene_id, mpm_status_info* 
   });
 }
 
+static const uint32_t kDefaultCands[] = {4, 8, 16, 32, 64, 128};
+
+int mpm_group_autotune(mpm_group* group, uint32_t probe_substeps, const uint32_t* candidates, uint32_t n_candidates,
+                       float* ms_per_substep, uint32_t* chosen) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    const uint32_t* c = candidates ? candidates : kDefaultCands;
+    const uint32_t nc = candidates ? n_candidates : 6;
+    REQUIRE(nc >= 1 && nc <= 64, MPM_ERR_INVALID, "1..=64 candidates required");
+    for (uint32_t i = 0; i < nc; ++i) REQUIRE(c[i] >= 1, MPM_ERR_INVALID, "intervals must be >= 1");
+    const uint32_t best = group->g->autotune(probe_substeps, c, (int)nc, ms_per_substep, group->eng->stream);
+    if (chosen) *chosen = best;
+  });
+}
+
+int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const uint32_t* candidates, uint32_t n_candidates,
+                 float* ms_per_substep, uint32_t* chosen) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim_check_step(sim, dt);
+    REQUIRE(!sim->order_enabled, MPM_ERR_INVALID, "particle ordering fixes the interval at one substep");
+    const uint32_t* c = candidates ? candidates : kDefaultCands;
+    const uint32_t nc = candidates ? n_candidates : 6;
+    REQUIRE(nc >= 1 && nc <= 64, MPM_ERR_INVALID, "1..=64 candidates required");
+    for (uint32_t i = 0; i < nc; ++i) REQUIRE(c[i] >= 1, MPM_ERR_INVALID, "intervals must be >= 1");
+    if (sim->count == 0) {
+      if (chosen) *chosen = sim->group->sort_interval;
+      return;
+    }
+    sim->group->set_scene_dt(sim->sid, dt);
+    const uint32_t best = sim->group->autotune(probe_substeps, c, (int)nc, ms_per_substep, sim->eng->stream);
+    sim->sort_interval = best;
+    sim->apply_group_settings();
+    if (chosen) *chosen = best;
+  });
+}
+
+int mpm_group_set_deterministic(mpm_group* group, int enabled) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    group->g->set_deterministic(enabled != 0);
+  });
+}
+
 int mpm_group_scene_count(mpm_group* group, uint32_t* count) {
   return guard([&] {
     REQUIRE(group && count, MPM_ERR_INVALID, "null argument");
@@ -880,6 +927,9 @@ double pct(std::vector<double> v, double q) {
 }
 }  // namespace
 
+// Device bytes a resident particle occupies in a group pool.
+constexpr uint64_t kServerBytesPerParticle = 2ull * mpm::kPlanes * 4ull + 64ull + 44ull;
+
 struct mpm_server {
   mpm::Engine* eng;
   std::unique_ptr<mpm::Group> g;
@@ -903,9 +953,10 @@ int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t ma
     try {
       s->eng = engine->e.get();
       s->budget = hbm_budget_bytes;
-      // Split the budget: particle pool (two 27-plane buffers + ids) 60%,
-      // grid pool (three float4 arrays) 40%.
-      const uint64_t per_particle = 2ull * mpm::kPlanes * 4ull + 40ull;
+      // Split the budget: particle pool 60% (two 27-plane buffers, the
+      // 64-byte scatter record and eleven index/key words per slot), grid
+      // pool 40% (three float4 arrays per cell).
+      const uint64_t per_particle = kServerBytesPerParticle;
       const uint64_t particles = std::min<uint64_t>(hbm_budget_bytes / 5 * 3 / per_particle, 0x7fff0000ull);
       const uint64_t cells = hbm_budget_bytes / 5 * 2 / 48ull;
       s->g.reset(new mpm::Group(s->eng, std::max<uint32_t>(max_scenes, 1), particles, cells));
@@ -945,7 +996,7 @@ int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheol
     t.dt = dt;
     t.steps = t.remaining = steps;
     const uint64_t n3 = (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
-    t.bytes = (uint64_t)n * (2ull * mpm::kPlanes * 4ull + 40ull) + (n3 + 255) / 256 * 256 * 48ull;
+    t.bytes = (uint64_t)n * kServerBytesPerParticle + (n3 + 255) / 256 * 256 * 48ull;
     REQUIRE(n <= server->g->cap && (n3 + 255) / 256 * 256 <= server->g->cell_cap && t.bytes <= server->budget,
             MPM_ERR_INVALID, "scene exceeds the server's HBM budget or pools");
     t.t_submit = now_ms();
@@ -995,7 +1046,7 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         continue;
       }
       MPM_CK(cudaEventRecord(server->e0, server->eng->stream));
-      g.step_graph(len, 1, server->eng->stream);
+      g.step(len, server->eng->stream);
       MPM_CK(cudaEventRecord(server->e1, server->eng->stream));
       MPM_CK(cudaEventSynchronize(server->e1));
       float ms = 0.f;

@@ -164,12 +164,17 @@ __global__ void k_reorder(const float* __restrict__ src, float* __restrict__ dst
                           const uint32_t* __restrict__ meta_src, uint32_t* __restrict__ meta_dst,
                           uint32_t* __restrict__ orig_dst, uint32_t* __restrict__ slot_of,
                           const uint32_t* __restrict__ ids, const uint32_t* __restrict__ keys,
-                          uint32_t* __restrict__ slot_key, uint32_t n_live) {
+                          uint32_t* __restrict__ slot_key, const float4* __restrict__ rec_src,
+                          float4* __restrict__ rec_dst, uint32_t n_live) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_live) return;
   const uint32_t id = ids[s];
   slot_key[s] = keys[s];
   const uint32_t old = slot_of[id];
+  if (rec_src) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rec_dst[4 * (size_t)s + k] = rec_src[4 * (size_t)old + k];
+  }
 #pragma unroll
   for (int k = 0; k < kPlanes; ++k) dst[(size_t)k * cap + s] = src[(size_t)k * cap + old];
   meta_dst[s] = meta_src[old];
@@ -195,7 +200,7 @@ __global__ void k_tile_start(const uint32_t* __restrict__ sorted_keys, uint32_t 
 // scene_of_tile is found by a search over the scene key offsets.
 __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, const uint32_t* __restrict__ key_offs,
                         uint32_t n_scenes, const uint32_t* __restrict__ scene_ids, uint32_t chunk,
-                        Item* __restrict__ items, uint32_t* __restrict__ n_items) {
+                        Item* __restrict__ items, uint32_t* __restrict__ n_items, uint32_t* __restrict__ tile_item) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= K) return;
   const uint32_t a = tile_start[t], b = tile_start[t + 1];
@@ -211,6 +216,7 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
   chunk = chunk ? chunk : cnt;
   const uint32_t pieces = (cnt + chunk - 1) / chunk;
   const uint32_t base = atomicAdd(n_items, pieces);
+  if (tile_item) tile_item[t] = base;
   for (uint32_t i = 0; i < pieces; ++i) {
     Item it;
     it.start = a + i * chunk;
@@ -325,20 +331,23 @@ cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* sl
 
 cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
                            uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, const uint32_t* keys,
-                           uint32_t* slot_key, uint32_t n_live, cudaStream_t st) {
+                           uint32_t* slot_key, const float4* rec_src, float4* rec_dst, uint32_t n_live,
+                           cudaStream_t st) {
   if (!n_live) return cudaSuccess;
   k_reorder<<<(n_live + 255) / 256, 256, 0, st>>>(src, dst, cap, meta_src, meta_dst, orig_dst, slot_of, ids, keys,
-                                                  slot_key, n_live);
+                                                  slot_key, rec_src, rec_dst, n_live);
   return cudaGetLastError();
 }
 
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
-                         Item* items, uint32_t* n_items, cudaStream_t st) {
+                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st) {
   cudaMemsetAsync(n_items, 0, sizeof(uint32_t), st);
+  if (tile_item) cudaMemsetAsync(tile_item, 0xff, (size_t)(K + 1) * sizeof(uint32_t), st);
   k_tile_start<<<(K + 1 + 255) / 256, 256, 0, st>>>(sorted_keys, n_live, K, shift, tile_start);
   if (K > 0)
-    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, chunk, items, n_items);
+    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, chunk, items, n_items,
+                                             tile_item);
   return cudaGetLastError();
 }
 

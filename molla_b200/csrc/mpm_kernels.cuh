@@ -17,6 +17,12 @@ enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
 cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
                           int reuse, int grid, cudaStream_t st);
 cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st);
+// Deterministic (fixed-order) scatter: per-tile blocks, then a combine pass.
+cudaError_t launch_scatter_det(const PoolDev& p, float4* blocks, int acc_out, int grid, cudaStream_t st);
+cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uint32_t* tile_item, uint32_t max_items,
+                               int acc_out, cudaStream_t st);
+constexpr int kTileNodes = 216;  // 6^3 node footprint of a 4^3-cell tile of base cells
+constexpr uint32_t kFaultNondeterministic = 4u;  // a deposit left the fixed-order path
 // Persistent grid sizes (SMs x resident CTAs).
 int gather_grid_size(bool svd_fp64);
 int scatter_grid_size();
@@ -32,10 +38,11 @@ cudaError_t launch_scene_keys(const PoolDev& p, uint32_t sid, const uint32_t* sl
                               uint32_t* keys, cudaStream_t st);
 cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uint32_t* meta_src, uint32_t* meta_dst,
                            uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, const uint32_t* keys,
-                           uint32_t* slot_key, uint32_t n_live, cudaStream_t st);
+                           uint32_t* slot_key, const float4* rec_src, float4* rec_dst, uint32_t n_live,
+                           cudaStream_t st);
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
-                         Item* items, uint32_t* n_items, cudaStream_t st);
+                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);
 cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
                               float* out, cudaStream_t st);
 cudaError_t launch_gather_rows(const PoolDev& p, int first, int count, const uint32_t* slot_of, uint32_t id_base,

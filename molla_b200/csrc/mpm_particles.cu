@@ -535,6 +535,197 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
   }
 }
 
+// Deterministic scatter (the fixed-order P2G of molla's
+// mpm_deterministic_p2g.wgsl:85-150, restructured per tile).  Requires a
+// regrouping after every gather, so that every particle of a tile item sits
+// in its own base cell.  Thread (cell, slab) sums its cell's particles in slot
+// order — (key, identity) order — in registers; the CTA then reduces the
+// (cell, slab) partial sums of each of the tile's 6^3 footprint nodes in a
+// fixed cell order and stores the block, without atomics.  A combine pass
+// adds the blocks of the tiles covering each node, again in a fixed order.
+// The result depends only on the scene's own particles and identities: it is
+// bit-identical from run to run and whether or not other scenes share the
+// launch.
+__global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float4* __restrict__ blocks, int acc_out) {
+  __shared__ uint32_t s_first[64], s_end[64];
+  __shared__ float s_part[3 * 64 * 9 * 4];
+  __shared__ uint32_t s_fault;
+  const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
+  const uint32_t n_items = *p.n_items;
+  const int cell = threadIdx.x & 63;
+  const int slab = threadIdx.x >> 6;
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item item = p.items[it];
+    const SceneDev* __restrict__ scp = p.scenes + item.scene;
+    const uint32_t w = scp->w;
+    const int n = (int)scp->n;
+    const float ox = scp->ox, oy = scp->oy, oz = scp->oz, inv_dx = scp->inv_dx, dx = scp->dx;
+    const int winx = scp->winx, winy = scp->winy, winz = scp->winz;
+    const uint64_t grid_off = scp->grid_off;
+    uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
+    const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
+    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)status;
+    if (threadIdx.x < 64) {
+      s_first[threadIdx.x] = 0;
+      s_end[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
+      const uint32_t s = item.start + k;
+      const uint32_t c = p.slot_key[s] & 63u;
+      if (k == 0 || (p.slot_key[s - 1] & 63u) != c) s_first[c] = s;
+      if (k + 1 == item.count || (p.slot_key[s + 1] & 63u) != c) s_end[c] = s + 1;
+    }
+    __syncthreads();
+    float am[9], apx[9], apy[9], apz[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
+    if (s_fault == 0) {
+      const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+      const int bx = 4 * (int)tx + cx, by = 4 * (int)ty + cy, bz = 4 * (int)tz + cz;  // this cell's base
+      const int win[3] = {winx, winy, winz};
+      for (uint32_t s = s_first[cell]; s < s_end[cell]; ++s) {
+        const float4 r0 = __ldg(&rec[4 * (size_t)s]);
+        if (r0.w == 0.f) continue;
+        const float4 r1 = __ldg(&rec[4 * (size_t)s + 1]);
+        const float4 r2 = __ldg(&rec[4 * (size_t)s + 2]);
+        const float4 r3 = __ldg(&rec[4 * (size_t)s + 3]);
+        const float mass = r0.w;
+        const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+        const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
+        float wgt[3][3], fx[3];
+        int base[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float bf = floorf(xp[a] - 0.5f);
+          base[a] = (int)bf - win[a];
+          fx[a] = xp[a] - bf;
+          quad_weights(fx[a], wgt[a]);
+        }
+        const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
+        const float di = ((float)slab - fx[0]) * dx;
+        const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
+        const bool own = base[0] == bx && base[1] == by && base[2] == bz;
+        if (!own && slab == 0 && threadIdx.x < 64) atomicOr(status, kFaultNondeterministic);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float wij = wi * wgt[1][j];
+          const float dj = ((float)j - fx[1]) * dx;
+          const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            const float wt = wij * wgt[2][kk];
+            const float dk = ((float)kk - fx[2]) * dx;
+            const float dm = wt * mass;
+            const float px = wt * (qy[0] + B[6] * dk);
+            const float py = wt * (qy[1] + B[7] * dk);
+            const float pz = wt * (qy[2] + B[8] * dk);
+            if (own) {
+              am[3 * j + kk] += dm;
+              apx[3 * j + kk] += px;
+              apy[3 * j + kk] += py;
+              apz[3 * j + kk] += pz;
+            } else {
+              // Not in its cell (positions set from outside the grid since
+              // the last regrouping): deposited with an atomic that the
+              // combine pass adds to, outside the fixed order; flagged in
+              // the status word.
+              const int ix = base[0] + slab, iy = base[1] + j, iz = base[2] + kk;
+              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+                const uint64_t c =
+                    grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+                atomicAdd(&p.acc[acc_out][c], make_float4(dm, px, py, pz));
+              }
+            }
+          }
+        }
+      }
+    }
+    {
+      float* dst = s_part + ((slab * 64 + cell) * 9) * 4;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        dst[4 * q] = am[q];
+        dst[4 * q + 1] = apx[q];
+        dst[4 * q + 2] = apy[q];
+        dst[4 * q + 3] = apz[q];
+      }
+    }
+    __syncthreads();
+    // Node (nx, ny, nz) of the 6^3 footprint receives, from cell (cx, cy, cz)
+    // with 0 <= n - c <= 2 per axis, the partial sum stored by thread
+    // (cell, slab = nx - cx) at index 3 (ny - cy) + (nz - cz).
+    float4* blk = blocks + (size_t)it * kTileNodes;
+    for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
+      const int nx = q % 6, ny = (q / 6) % 6, nz = q / 36;
+      float sm = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
+      for (int cz = max(0, nz - 2); cz <= min(3, nz); ++cz)
+        for (int cy = max(0, ny - 2); cy <= min(3, ny); ++cy)
+          for (int cx = max(0, nx - 2); cx <= min(3, nx); ++cx) {
+            const float* src = s_part + (((nx - cx) * 64 + (cx + 4 * cy + 16 * cz)) * 9 + 3 * (ny - cy) + (nz - cz)) * 4;
+            sm += src[0];
+            sx += src[1];
+            sy += src[2];
+            sz += src[3];
+          }
+      blk[q] = make_float4(sm, sx, sy, sz);
+    }
+    __syncthreads();
+  }
+}
+
+// Combine pass of the deterministic scatter: node g of a scene receives the
+// blocks of the (up to 8) occupied tiles whose footprint [4t, 4t+5] contains
+// it, summed in (tz, ty, tx) order by the first such tile's thread.
+__global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, const uint32_t* __restrict__ tile_item,
+                              int acc_out) {
+  const uint32_t it = blockIdx.x;
+  if (it >= *p.n_items) return;
+  const Item item = p.items[it];
+  const SceneDev* __restrict__ scp = p.scenes + item.scene;
+  const int w = (int)scp->w, n = (int)scp->n;
+  const uint32_t key_off = scp->key_off;
+  const int tx = (int)(item.tile % (uint32_t)w), ty = (int)((item.tile / (uint32_t)w) % (uint32_t)w),
+            tz = (int)(item.tile / (uint32_t)(w * w));
+  for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
+    const int g[3] = {4 * tx + q % 6, 4 * ty + (q / 6) % 6, 4 * tz + q / 36};
+    if (g[0] >= n || g[1] >= n || g[2] >= n) continue;
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      hi[a] = g[a] / 4;
+      lo[a] = max(0, (g[a] - 5 + 3) / 4);  // smallest t with 4t + 5 >= g
+      hi[a] = min(hi[a], w - 1);
+    }
+    bool mine = false, found = false;
+    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int cz = lo[2]; cz <= hi[2]; ++cz)
+      for (int cy = lo[1]; cy <= hi[1]; ++cy)
+        for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+          const uint32_t key = key_off + (uint32_t)(cx + w * (cy + w * cz));
+          const uint32_t other = tile_item[key];
+          if (other == 0xffffffffu) continue;
+          if (!found) {
+            found = true;
+            mine = other == it;
+            if (!mine) break;
+          }
+          const int l = (g[0] - 4 * cx) + 6 * ((g[1] - 4 * cy) + 6 * (g[2] - 4 * cz));
+          const float4 b = blocks[(size_t)other * kTileNodes + l];
+          sum.x += b.x;
+          sum.y += b.y;
+          sum.z += b.z;
+          sum.w += b.w;
+        }
+    if (mine) {
+      // One writer per node; the cell holds zero or out-of-order deposits.
+      float4& a = p.acc[acc_out][scp->grid_off + (uint64_t)g[0] + (uint64_t)n * ((uint64_t)g[1] + (uint64_t)n * g[2])];
+      const float4 old = a;
+      a = make_float4(old.x + sum.x, old.y + sum.y, old.z + sum.z, old.w + sum.w);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 
 template <int MODE, bool KEYS, class SR>
@@ -563,6 +754,18 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
 
 cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st) {
   k_p2g<<<grid, kScatterThreads, 0, st>>>(p, acc_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_det(const PoolDev& p, float4* blocks, int acc_out, int grid, cudaStream_t st) {
+  k_p2g_det<<<grid, kScatterThreads, 0, st>>>(p, blocks, acc_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uint32_t* tile_item, uint32_t max_items,
+                               int acc_out, cudaStream_t st) {
+  if (!max_items) return cudaSuccess;
+  k_combine_det<<<max_items, 128, 0, st>>>(p, blocks, tile_item, acc_out);
   return cudaGetLastError();
 }
 

@@ -226,7 +226,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaSetDevice(eng->device));
   planes[0].alloc((size_t)kPlanes * cap);
   planes[1].alloc((size_t)kPlanes * cap);
-  rec.alloc((size_t)16 * cap);
+  rec[0].alloc((size_t)16 * cap);
   for (int i = 0; i < 2; ++i) {
     meta[i].alloc(cap);
     orig[i].alloc(cap);
@@ -287,7 +287,7 @@ PoolDev Group::pool() const {
   p.acc[0] = acc[0].ptr;
   p.acc[1] = acc[1].ptr;
   p.vel = vel.ptr;
-  p.rec = rec.ptr;
+  p.rec = rec[rec_cur].ptr;
   p.slot_key = slot_key.ptr;
   p.scenes = scenes_d.ptr;
   p.status = status_d.ptr;
@@ -305,7 +305,7 @@ uint32_t Group::live_scenes() const {
 uint64_t Group::resident_bytes() const {
   uint64_t b = 0;
   for (const SceneHost& s : scenes)
-    if (s.live) b += (uint64_t)s.n * (2ull * kPlanes * 4ull + 40ull) + s.grid_len * 48ull;
+    if (s.live) b += (uint64_t)s.n * (2ull * kPlanes * 4ull + 64ull + 44ull) + s.grid_len * 48ull;
   return b;
 }
 
@@ -327,6 +327,10 @@ void Group::rebuild_layout() {
   if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
   const size_t max_items = (size_t)key_space + 2;  // one item per occupied tile
   if (items.count < max_items) items.alloc(max_items);
+  if (deterministic) {
+    if (tile_item.count < (size_t)key_space + 2) tile_item.alloc((size_t)key_space + 2);
+    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
+  }
   if (!offs.empty()) {
     MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
     MPM_CK(cudaMemcpyAsync(scene_ids_d.ptr, sids.data(), sids.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -521,7 +525,7 @@ static int bits_for(uint64_t values) {
 // contiguous and, inside the tile, grouped by base cell.  The sorted key of
 // every slot is kept for the scatter, and the work list is rebuilt from the
 // tile boundaries.
-void Group::regroup(bool compute_keys, cudaStream_t st) {
+void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   ProfRec pr;
   eng->prof_begin(kStageOrdering, st, &pr);
   if (compute_keys) {
@@ -533,12 +537,15 @@ void Group::regroup(bool compute_keys, cudaStream_t st) {
   uint32_t* sids = nullptr;
   MPM_CK(radix_sort_pairs(st, keys_by_id.ptr, nullptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n_sort,
                           bits_for((uint64_t)key_space << kCellBits), &skeys, &sids, &eng->launches));
+  const float4* rsrc = move_records ? reinterpret_cast<const float4*>(rec[rec_cur].ptr) : nullptr;
+  float4* rdst = move_records ? reinterpret_cast<float4*>(rec[rec_cur ^ 1].ptr) : nullptr;
   MPM_CK(launch_reorder(planes[cur].ptr, planes[cur ^ 1].ptr, cap, meta[cur].ptr, meta[cur ^ 1].ptr,
-                        orig[cur ^ 1].ptr, slot_of.ptr, sids, skeys, slot_key.ptr, n_live, st));
+                        orig[cur ^ 1].ptr, slot_of.ptr, sids, skeys, slot_key.ptr, rsrc, rdst, n_live, st));
   eng->launches += 1;
   cur ^= 1;
+  if (move_records) rec_cur ^= 1;
   MPM_CK(launch_items(skeys, kCellBits, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(),
-                      scene_ids_d.ptr, 0, items.ptr, n_items.ptr, st));
+                      scene_ids_d.ptr, 0, items.ptr, n_items.ptr, deterministic ? tile_item.ptr : nullptr, st));
   eng->launches += key_space ? 2 : 1;
   need_regroup = false;
   eng->prof_end(&pr, st);
@@ -557,9 +564,117 @@ void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
 void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
   ProfRec pr;
   eng->prof_begin(kStageScatter, st, &pr);
-  MPM_CK(launch_scatter(pool(), acc_out, grid_scatter, st));
+  if (deterministic) {
+    MPM_CK(launch_scatter_det(pool(), det_blocks.ptr, acc_out, grid_scatter, st));
+    MPM_CK(launch_combine_det(pool(), det_blocks.ptr, tile_item.ptr, key_space, acc_out, st));
+    eng->launches += 1;
+  } else {
+    MPM_CK(launch_scatter(pool(), acc_out, grid_scatter, st));
+  }
   eng->prof_end(&pr, st);
   eng->launches += 1;
+}
+
+uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_out, cudaStream_t st) {
+  eng->check();
+  if (!n_live || !probe || n_cands <= 0) return sort_interval;
+  sync_scenes(st);
+  // Snapshot of everything a substep reads or writes.
+  const size_t pbytes = (size_t)kPlanes * cap * sizeof(float);
+  const uint64_t cells_hw = cells.high_water();
+  DevBuf<float> bplanes((size_t)kPlanes * cap);
+  DevBuf<uint32_t> bmeta(cap), borig(cap), bslot(cap), bkey(cap), bstatus(status_d.count);
+  DevBuf<float4> bacc0(cells_hw), bacc1(cells_hw), bvel(cells_hw);
+  auto save = [&](bool to_backup) {
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (bytes) MPM_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
+    };
+    if (to_backup) {
+      cp(bplanes.ptr, planes[cur].ptr, pbytes);
+      cp(bmeta.ptr, meta[cur].ptr, cap * 4);
+      cp(borig.ptr, orig[cur].ptr, cap * 4);
+      cp(bslot.ptr, slot_of.ptr, cap * 4);
+      cp(bkey.ptr, slot_key.ptr, cap * 4);
+      cp(bstatus.ptr, status_d.ptr, status_d.bytes());
+      cp(bacc0.ptr, acc[0].ptr, cells_hw * sizeof(float4));
+      cp(bacc1.ptr, acc[1].ptr, cells_hw * sizeof(float4));
+      cp(bvel.ptr, vel.ptr, cells_hw * sizeof(float4));
+    } else {
+      cp(planes[cur].ptr, bplanes.ptr, pbytes);
+      cp(meta[cur].ptr, bmeta.ptr, cap * 4);
+      cp(orig[cur].ptr, borig.ptr, cap * 4);
+      cp(slot_of.ptr, bslot.ptr, cap * 4);
+      cp(slot_key.ptr, bkey.ptr, cap * 4);
+      cp(status_d.ptr, bstatus.ptr, status_d.bytes());
+      cp(acc[0].ptr, bacc0.ptr, cells_hw * sizeof(float4));
+      cp(acc[1].ptr, bacc1.ptr, cells_hw * sizeof(float4));
+      cp(vel.ptr, bvel.ptr, cells_hw * sizeof(float4));
+    }
+  };
+  const int cur0 = cur, az0 = acc_zero, al0 = acc_last;
+  const bool nr0 = need_regroup;
+  const uint64_t done0 = substeps_done;
+  const uint32_t interval0 = sort_interval;
+  save(true);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MPM_CK(cudaEventCreate(&e0));
+  MPM_CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  uint32_t best_i = interval0;
+  for (int c = 0; c < n_cands; ++c) {
+    cur = cur0;
+    acc_zero = az0;
+    acc_last = al0;
+    need_regroup = true;  // every candidate starts from a fresh regrouping
+    if (c) save(false);
+    sort_interval = cands[c];
+    run_substeps(probe, st);  // warm
+    cur = cur0;
+    acc_zero = az0;
+    acc_last = al0;
+    need_regroup = true;
+    save(false);
+    MPM_CK(cudaEventRecord(e0, st));
+    run_substeps(probe, st);
+    MPM_CK(cudaEventRecord(e1, st));
+    MPM_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    MPM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= (float)probe;
+    if (ms_out) ms_out[c] = ms;
+    if (ms < best) {
+      best = ms;
+      best_i = cands[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cur = cur0;
+  acc_zero = az0;
+  acc_last = al0;
+  save(false);
+  MPM_CK(cudaStreamSynchronize(st));
+  (void)nr0;
+  need_regroup = true;  // the work list belongs to the probes; rebuild it
+  substeps_done = done0;
+  sort_interval = best_i;
+  invalidate_graphs();
+  return best_i;
+}
+
+// Fixed-order P2G: a regrouping after every gather (so every particle sits in
+// its base cell when it is deposited) and the two-pass deterministic scatter.
+void Group::set_deterministic(bool on) {
+  if (on == deterministic) return;
+  deterministic = on;
+  if (on) {
+    if (rec[1].count < (size_t)16 * cap) rec[1].alloc((size_t)16 * cap);
+    const size_t max_items = (size_t)key_space + 2;
+    if (tile_item.count < max_items) tile_item.alloc(max_items);
+    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
+  }
+  need_regroup = true;
+  invalidate_graphs();
 }
 
 // One call: record + scatter of the first substep, then per substep the grid
@@ -567,7 +682,7 @@ void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
 // the last) and the next scatter.  Regrouping happens after a scatter, every
 // `sort_interval` substeps.
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
-  if (need_regroup) regroup(true, st);
+  if (need_regroup || deterministic) regroup(true, st);
   launch_gather_pass(kRecord, false, st);
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
@@ -580,13 +695,20 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
     eng->prof_end(&pr, st);
     eng->launches += 1;
     const bool last = s + 1 == substeps;
-    const bool due = !last && sort_interval > 0 && ++since >= sort_interval;
+    const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
     launch_gather_pass(last ? kG2P : kG2PRecord, due, st);
     if (!last) {
-      launch_scatter_pass(a ^ 1, st);
-      if (due) {
-        regroup(false, st);
-        since = 0;
+      if (deterministic) {
+        // Fixed order: particles (and their records) regrouped into the
+        // cells of their new positions before they are deposited.
+        regroup(false, st, true);
+        launch_scatter_pass(a ^ 1, st);
+      } else {
+        launch_scatter_pass(a ^ 1, st);
+        if (due) {
+          regroup(false, st);
+          since = 0;
+        }
       }
       a ^= 1;
     }
@@ -609,7 +731,8 @@ void Group::step(uint32_t substeps, cudaStream_t st) {
 }
 
 uint64_t Group::graph_key(uint32_t substeps) const {
-  return ((uint64_t)substeps << 8) | ((uint64_t)cur << 2) | ((uint64_t)acc_zero << 1) | (need_regroup ? 1u : 0u);
+  return ((uint64_t)substeps << 8) | ((uint64_t)rec_cur << 3) | ((uint64_t)cur << 2) | ((uint64_t)acc_zero << 1) |
+         (need_regroup ? 1u : 0u);
 }
 
 void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
@@ -661,17 +784,18 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
     eng->launches += g.kernels;
     // Replay the host-side state transition of the captured sequence.
     uint32_t since = 0;
-    if (need_regroup) {
+    if (need_regroup || deterministic) {
       cur ^= 1;
       need_regroup = false;
     }
     int a = acc_zero;
     for (uint32_t s = 0; s < substeps; ++s) {
       const bool last = s + 1 == substeps;
-      const bool due = !last && sort_interval > 0 && ++since >= sort_interval;
+      const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
       if (due) {
         cur ^= 1;
         since = 0;
+        if (deterministic) rec_cur ^= 1;
       }
       if (!last) a ^= 1;
     }

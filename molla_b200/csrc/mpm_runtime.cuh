@@ -157,7 +157,8 @@ class Group {
 
   // particle pool (double-buffered for the regroup)
   DevBuf<float> planes[2];
-  DevBuf<float> rec;  // per-slot scatter record, 16 floats (64 B) per slot
+  DevBuf<float> rec[2];  // per-slot scatter record, 16 floats (64 B) per slot (rec[1]: deterministic mode)
+  int rec_cur = 0;
   DevBuf<uint32_t> meta[2], orig[2];
   DevBuf<uint32_t> slot_of, keys_by_id, slot_key, ks[2], vs[2], hist;
   // grid pool
@@ -168,6 +169,8 @@ class Group {
   DevBuf<uint32_t> status_d;
   DevBuf<uint32_t> tile_start, key_offs_d, scene_ids_d, n_items;
   DevBuf<Item> items;
+  DevBuf<uint32_t> tile_item;  // deterministic mode: item of each occupied tile
+  DevBuf<float4> det_blocks;   // deterministic mode: per-tile 6^3 node blocks
   DevBuf<double> totals_d;
   // pinned staging of scene records
   SceneDev* scenes_h = nullptr;
@@ -185,6 +188,7 @@ class Group {
   uint32_t sort_interval = 32;
   uint32_t chunk = 512;
   bool svd_fp64 = false;
+  bool deterministic = false;
   bool reuse_svd = true;
   double svd_tol32 = 1.0e-7;
   double svd_tol64 = 1.0e-9;
@@ -214,7 +218,7 @@ class Group {
   void step(uint32_t substeps, cudaStream_t st);
   // Same through a cached CUDA graph.
   void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st);
-  void regroup(bool compute_keys, cudaStream_t st);
+  void regroup(bool compute_keys, cudaStream_t st, bool move_records = false);
   void sync_scenes(cudaStream_t st);
 
   PoolDev pool() const;
@@ -234,6 +238,14 @@ class Group {
   void invalidate_graphs();
   void launch_gather_pass(int mode, bool keys, cudaStream_t st);
   void launch_scatter_pass(int acc_out, cudaStream_t st);
+ public:
+  void set_deterministic(bool on);
+  // Picks the regrouping interval: times `probe` substeps for each candidate
+  // on a snapshot of the device state, restores the state and keeps the
+  // fastest interval.  Returns it and fills ms_per_substep (one per
+  // candidate, may be null).
+  uint32_t autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_per_substep, cudaStream_t st);
+ private:
   void run_substeps(uint32_t substeps, cudaStream_t st);
   uint64_t graph_key(uint32_t substeps) const;
 };

@@ -96,7 +96,7 @@ def test_server_results_same_alone_and_in_mix(engine):
 
 def test_server_admission_respects_budget(engine):
     ss = small_scenes()
-    per = [s.n * (2 * 27 * 4 + 40) + ((s.grid_size ** 3 + 255) // 256 * 256) * 48 for s in ss]
+    per = [s.n * (2 * 27 * 4 + 64 + 44) + ((s.grid_size ** 3 + 255) // 256 * 256) * 48 for s in ss]
     budget = 3 * max(per)
     srv = m.MpmServer(engine, hbm_budget_bytes=budget, max_scenes=8)
     tickets = [srv.submit(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt, 30) for s in ss]
@@ -113,3 +113,53 @@ def test_server_admission_respects_budget(engine):
     assert srv.stats()["completed"] == len(ss)
     for t in tickets:
         assert srv.poll(t)[0] == 2
+
+
+def test_deterministic_group_bit_identical_alone_and_in_mix(engine):
+    """Fixed-order P2G: a scene's state is bit-identical alone and in a mix,
+    and from run to run (fixed_order_public_lifecycle_repeatability,
+    crates/molla-solvers/tests/mpm_fixed_order_runtime.rs:65-159)."""
+    ss = small_scenes()
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 256 * len(ss)
+
+    def run(indices, repeat_tag):
+        g = m.MpmGroup(engine, 16, total, cells)
+        g.set_deterministic(True)
+        ids = {i: g.add_scene(m.config_for_scene(ss[i]), ss[i].rows, ss[i].positions, ss[i].ids, ss[i].dt)
+               for i in indices}
+        g.step(12)
+        g.step_graph(6, 2)
+        out = {i: g.read_positions(sid) for i, sid in ids.items()}
+        st = {i: g.read_status(sid) for i, sid in ids.items()}
+        g.close()
+        return out, st
+
+    mix, st_mix = run(range(len(ss)), "mix")
+    again, _ = run(range(len(ss)), "again")
+    for i in range(len(ss)):
+        assert np.array_equal(mix[i], again[i]), i
+        assert st_mix[i].fault_bits == 0 and st_mix[i].completed_substeps == 24
+    for i in (0, 3):
+        alone_pos, _ = run([i], "alone")
+        assert np.array_equal(alone_pos[i], mix[i]), i
+        # and within the atomic path's tolerance of the default (atomic) mode
+        assert np.abs(alone_pos[i] - alone(engine, ss[i], 24)).max() < TOL
+
+
+def test_autotune_keeps_state_and_picks_a_candidate(engine):
+    ss = small_scenes()[:3]
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 1024
+    g = m.MpmGroup(engine, 8, total, cells)
+    ids = [g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt) for s in ss]
+    g.step(5)
+    before = [g.read_positions(i) for i in ids]
+    chosen, timings = g.autotune(probe_substeps=8, candidates=(2, 4, 8))
+    assert chosen in (2, 4, 8) and all(v > 0 for v in timings.values())
+    for i, b in zip(ids, before):
+        assert np.array_equal(g.read_positions(i), b)
+        assert g.read_status(i).completed_substeps == 5
+    g.step(5)
+    for k, i in enumerate(ids):
+        assert np.abs(g.read_positions(i) - alone(engine, ss[k], 10)).max() < TOL

@@ -395,3 +395,40 @@ def test_disjoint_blocks_mixed_equal_separate_runs(engine):
         s.step_n(1.0 / 480, 60)
         outs.append(s.read_positions())
     assert np.abs(pm - np.concatenate(outs)).max() < 1e-5
+
+
+def test_deterministic_p2g_lifecycle_and_repeatability(engine):
+    """mpm_fixed_order_runtime.rs:65-159: preconditions, then two simulations
+    stepped identically are byte-equal; results match the oracle."""
+    cfg = ordering_config()
+    pts = G.points(257)
+    ids = (np.arange(257) % 3).astype(np.uint32)
+    vel = np.tile(np.array([0.1, -0.02, 0.03], np.float32), (257, 1))
+    sims = []
+    for _ in range(2):
+        sim = m.MpmSimulation.new(engine, cfg)
+        sim.set_particles(pts, vel)
+        sim.set_materials(MIXED_ROWS, ids)
+        with pytest.raises(m.SolverError):
+            sim.set_deterministic_p2g(True)  # not prepared, no ordering
+        sim.prepare_deterministic_p2g()
+        with pytest.raises(m.SolverError):
+            sim.set_deterministic_p2g(True)  # ordering not enabled
+        sim.prepare_particle_tile_ordering(257)
+        sim.set_particle_tile_ordering(True)
+        sim.set_deterministic_p2g(True)
+        with pytest.raises(m.SolverError):
+            sim.set_particle_tile_ordering(False)
+        for _ in range(3):
+            sim.step_n(1e-4, 2)
+        sims.append(sim)
+    a = [sims[0].read_positions(), sims[0].read_velocities(), *sims[0].read_particle_state()]
+    b = [sims[1].read_positions(), sims[1].read_velocities(), *sims[1].read_particle_state()]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert sims[0].read_active_grid_status().fault_bits == 0
+    sc = O.make_scene(cfg, MIXED_ROWS, 1e-4)
+    st = O.init_state(pts, vel, mass=cfg.particle_mass, volume=cfg.particle_volume, ids=ids)
+    O.step(sc, st, 6)
+    assert np.abs(a[0] - st["pos"]).max() <= 2e-5
+    assert norm_err(a[3], st["F"]) <= 2e-5
