@@ -139,12 +139,20 @@ __device__ __forceinline__ T det3(const T* a) {
 // sigma_i = |F v_i|, u_i = F v_i / sigma_i; sign fixes so det U = det V = +1.
 //
 // The FP32 form keeps the reference's rotation formulas (theta, t, c with
-// IEEE division and square root).  The FP64 form computes the same rotation
-// as t = sgn(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq
-// (algebraically identical to 1/(theta + sgn(theta) sqrt(1 + theta^2))), and
-// replaces double division and square roots by Newton-Raphson refinement of
-// single-precision seeds (two steps each, quadratic convergence from 2^-22
-// to below 2^-52).
+// IEEE division and square root).
+//
+// The FP64 form (svd3<double>) is mixed precision, built for the
+// small-strain regime where F^T F = I + O(strain): the Jacobi iteration runs
+// on the shifted matrix A' = F^T F - I (same eigenvectors), formed in FP64
+// and held in FP32, where its entries keep full relative precision however
+// small the strain.  Each rotation angle t = sgn(d) e / (|d| + sqrt(d^2+e^2))
+// (d = a'_qq - a'_pp, e = 2 a'_pq; algebraically 1/(theta + sgn(theta)
+// sqrt(1 + theta^2))) is computed in FP32; V accumulates the same rotations
+// in FP64 with c = (1 + t^2)^(-1/2) Newton-refined to FP64 and s = t c, so V
+// stays orthogonal to FP64 rounding.  sigma_i = |F v_i| and u_i = F v_i /
+// sigma_i are FP64.  Double division and square roots are replaced by
+// Newton-Raphson refinement of single-precision seeds (two steps each,
+// quadratic convergence from 2^-22 to below 2^-52).
 template <class T> struct SvdOut {
   T u[9], s[3], v[9];
 };
@@ -173,44 +181,63 @@ __device__ __forceinline__ double nr_rsqrt(double x) {
   return fma(y, e, y);
 }
 
+// One FP32 Jacobi rotation of the (P, Q) pair of the symmetric a[3][3]
+// (reference formulas); V is updated with the same c, s in type T.
 template <class T, int P, int Q>
-__device__ __forceinline__ void jacobi_rot(T (&a)[3][3], T* v, T tol, T& max_off) {
+__device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, float& max_off) {
   constexpr int K = 3 - P - Q;
-  const T apq = a[P][Q];
-  const T aapq = apq < T(0) ? -apq : apq;
+  const float apq = a[P][Q];
+  const float aapq = fabsf(apq);
   if (aapq > max_off) max_off = aapq;
-  if (aapq < tol) return;
-  const T app = a[P][P];
-  const T aqq = a[Q][Q];
-  T t, c, s;
+  if (aapq < tol || apq == 0.0f) return;
+  const float app = a[P][P];
+  const float aqq = a[Q][Q];
+  float t, c, s;
+  T cv, sv;
   if constexpr (sizeof(T) == 4) {
-    const T theta = (aqq - app) / (T(2) * apq);
-    if (theta >= T(0)) {
-      t = T(1) / (theta + sqrtf(T(1) + theta * theta));
+    const float theta = (aqq - app) / (2.0f * apq);
+    if (theta >= 0.0f) {
+      t = 1.0f / (theta + sqrtf(1.0f + theta * theta));
     } else {
-      t = T(1) / (theta - sqrtf(T(1) + theta * theta));
+      t = 1.0f / (theta - sqrtf(1.0f + theta * theta));
     }
-    c = T(1) / sqrtf(T(1) + t * t);
+    c = 1.0f / sqrtf(1.0f + t * t);
     s = t * c;
+    cv = c;
+    sv = s;
   } else {
-    const T d = aqq - app;
-    const T e = T(2) * apq;
-    const T ad = d < T(0) ? -d : d;
-    const T r2 = d * d + e * e;
-    const T hyp = r2 * nr_rsqrt(r2);
-    t = (d >= T(0) ? e : -e) * nr_rcp(ad + hyp);
-    c = nr_rsqrt(T(1) + t * t);
+    float d = aqq - app;
+    float e = 2.0f * apq;
+    // power-of-two rescale keeps d^2 + e^2 inside the normal FP32 range
+    const float m = fmaxf(fabsf(d), fabsf(e));
+    const float k = m > 1.0e18f ? 0x1p-64f : (m < 1.0e-18f ? 0x1p64f : 1.0f);
+    d *= k;
+    e *= k;
+    const float r2 = d * d + e * e;
+    const float hyp = r2 * rsqrtf(r2);
+    t = __fdividef(d >= 0.0f ? e : -e, fabsf(d) + hyp);
+    c = rsqrtf(1.0f + t * t);
     s = t * c;
+    // FP64 rotation for V: exactly orthogonal to FP64 rounding for this t.
+    const double td = (double)t;
+    const double h = 0.5 * fma(td, td, 1.0);
+    double y = (double)c;
+    double r = fma(-h * y, y, 0.5);
+    y = fma(y, r, y);
+    r = fma(-h * y, y, 0.5);
+    y = fma(y, r, y);
+    cv = y;
+    sv = td * y;
   }
   a[P][P] = app - t * apq;
   a[Q][Q] = aqq + t * apq;
-  a[P][Q] = T(0);
-  a[Q][P] = T(0);
+  a[P][Q] = 0.0f;
+  a[Q][P] = 0.0f;
   {
-    const T akp = a[P][K];
-    const T akq = a[Q][K];
-    const T nkp = c * akp - s * akq;
-    const T nkq = s * akp + c * akq;
+    const float akp = a[P][K];
+    const float akq = a[Q][K];
+    const float nkp = c * akp - s * akq;
+    const float nkq = s * akp + c * akq;
     a[P][K] = nkp;
     a[Q][K] = nkq;
     a[K][P] = nkp;
@@ -220,29 +247,38 @@ __device__ __forceinline__ void jacobi_rot(T (&a)[3][3], T* v, T tol, T& max_off
   for (int k = 0; k < 3; ++k) {
     const T vkp = v[3 * P + k];
     const T vkq = v[3 * Q + k];
-    v[3 * P + k] = c * vkp - s * vkq;
-    v[3 * Q + k] = s * vkp + c * vkq;
+    v[3 * P + k] = cv * vkp - sv * vkq;
+    v[3 * Q + k] = sv * vkp + cv * vkq;
   }
 }
 
 template <class T>
 __device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sweeps) {
-  // a[col][row] of A = F^T F (symmetric)
-  T a[3][3];
+  // a[col][row] of A = F^T F (FP32 form) or of A' = F^T F - I formed in
+  // FP64 and held in FP32 (FP64 form); symmetric.
+  float a[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-      a[c][r] = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
+    for (int r = c; r < 3; ++r) {
+      const T acr = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
+      if constexpr (sizeof(T) == 4) {
+        a[c][r] = acr;
+      } else {
+        a[c][r] = (float)(r == c ? acr - 1.0 : acr);
+      }
+      a[r][c] = a[c][r];
+    }
   T* v = o.v;
 #pragma unroll
   for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? T(1) : T(0);
+  const float ftol = (float)tol;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
-    T max_off = T(0);
-    jacobi_rot<T, 0, 1>(a, v, tol, max_off);
-    jacobi_rot<T, 0, 2>(a, v, tol, max_off);
-    jacobi_rot<T, 1, 2>(a, v, tol, max_off);
-    if (max_off < tol) break;
+    float max_off = 0.0f;
+    jacobi_rot<T, 0, 1>(a, v, ftol, max_off);
+    jacobi_rot<T, 0, 2>(a, v, ftol, max_off);
+    jacobi_rot<T, 1, 2>(a, v, ftol, max_off);
+    if (max_off < ftol) break;
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -323,58 +359,103 @@ __device__ __forceinline__ void quad_weights(float fx, float* w) {
 // s_c = clamp(s, 0.1, 10), R = U V^T, J = prod s_c, hardening h by rheology,
 // P = 2 mu h (Fc - R) + lam h (J - 1) cof, S = -dt vol P Fc^T.  Returns
 // B = m C + 4/dx^2 S so that a node at offset d receives w (m v + B d).
-template <class T>
-__device__ __forceinline__ void p2g_affine(const SvdOut<T>& svd, const MatDev& md, float jp, float mass, float vol,
-                                           const float* C, float dt, float inv_dx, float* B) {
-  float u[9], v[9], sc[3];
+__device__ __forceinline__ void p2g_affine_principal(const SvdOut<double>& svd, const MatDev& md, float jp,
+                                                     float mass, float vol, const float* C, float dt, float inv_dx,
+                                                     float* B) {
+  // FP64-SVD form.  With Fc = U Sc V^T, R = U V^T and cof = U diag(J/sc) V^T
+  // the same stress is S = -dt vol P Fc^T = -dt vol U diag(tau) U^T,
+  // tau_i = 2 mu h (sc_i - 1) sc_i + lam h (J - 1) J (Kirchhoff stress in
+  // the principal frame).  sc_i - 1 and J - 1 are formed in FP64, so the
+  // small-strain stress keeps full FP32 relative precision instead of
+  // cancelling in Fc - R.
+  double scd[3];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    u[i] = (float)svd.u[i];
-    v[i] = (float)svd.v[i];
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) sc[i] = clampf((float)svd.s[i], 0.1f, 10.0f);
+  for (int i = 0; i < 3; ++i) scd[i] = fmin(fmax(svd.s[i], 0.1), 10.0);
+  const double Jd = scd[0] * scd[1] * scd[2];
+  const float J = (float)Jd;
+  const float jm1 = (float)(Jd - 1.0);
   float h = 1.0f;
   if (md.rheo == 1) {
     h = expf(clampf(-md.hardening * jp, -3.0f, 3.0f));
   } else if (md.rheo == 0) {
     h = expf(clampf(jp, -3.0f, 3.0f));
   }
-  const float mu_h = md.mu * h;
-  const float lam_h = md.lam * h;
-  const float J = sc[0] * sc[1] * sc[2];
-  const float cofd[3] = {sc[1] * sc[2], sc[0] * sc[2], sc[0] * sc[1]};
-  float Fc[9], cof[9];
-  sandwich(u, sc, v, Fc);
-  sandwich(u, cofd, v, cof);
-  const float k1 = 2.0f * mu_h;
-  const float k2 = lam_h * (J - 1.0f);
-  const float k3 = -dt * vol;
-  float P[9];
+  const float k1 = 2.0f * md.mu * h;
+  const float kv = md.lam * h * jm1 * J;
+  float tau[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) tau[i] = k1 * (float)(scd[i] - 1.0) * (float)scd[i] + kv;
+  float u[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) u[i] = (float)svd.u[i];
+  const float k = -dt * vol * 4.0f * inv_dx * inv_dx;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      // R = U V^T
-      const float Rcr = u[r] * v[c] + u[3 + r] * v[3 + c] + u[6 + r] * v[6 + c];
-      P[3 * c + r] = k3 * (k1 * (Fc[3 * c + r] - Rcr) + k2 * cof[3 * c + r]);
+    for (int r = c; r < 3; ++r) {
+      const float S = k * (u[r] * tau[0] * u[c] + u[3 + r] * tau[1] * u[3 + c] + u[6 + r] * tau[2] * u[6 + c]);
+      B[3 * c + r] = mass * C[3 * c + r] + S;
+      if (r != c) B[3 * r + c] = mass * C[3 * r + c] + S;
     }
-  // S = P Fc^T : S[c][r] = sum_k P[k][r] * Fc[k][c]
-  const float four_inv_dx2 = 4.0f * inv_dx * inv_dx;
+}
+
+// Reference form (FP32 SVD); the FP64-SVD mode takes the principal form.
+template <class T>
+__device__ __forceinline__ void p2g_affine(const SvdOut<T>& svd, const MatDev& md, float jp, float mass, float vol,
+                                           const float* C, float dt, float inv_dx, float* B) {
+  if constexpr (sizeof(T) == 8) {
+    p2g_affine_principal(svd, md, jp, mass, vol, C, dt, inv_dx, B);
+  } else {
+    float u[9], v[9], sc[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const float S = P[r] * Fc[c] + P[3 + r] * Fc[3 + c] + P[6 + r] * Fc[6 + c];
-      B[3 * c + r] = mass * C[3 * c + r] + four_inv_dx2 * S;
+    for (int i = 0; i < 9; ++i) {
+      u[i] = (float)svd.u[i];
+      v[i] = (float)svd.v[i];
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sc[i] = clampf((float)svd.s[i], 0.1f, 10.0f);
+    float h = 1.0f;
+    if (md.rheo == 1) {
+      h = expf(clampf(-md.hardening * jp, -3.0f, 3.0f));
+    } else if (md.rheo == 0) {
+      h = expf(clampf(jp, -3.0f, 3.0f));
+    }
+    const float mu_h = md.mu * h;
+    const float lam_h = md.lam * h;
+    const float J = sc[0] * sc[1] * sc[2];
+    const float cofd[3] = {sc[1] * sc[2], sc[0] * sc[2], sc[0] * sc[1]};
+    float Fc[9], cof[9];
+    sandwich(u, sc, v, Fc);
+    sandwich(u, cofd, v, cof);
+    const float k1 = 2.0f * mu_h;
+    const float k2 = lam_h * (J - 1.0f);
+    const float k3 = -dt * vol;
+    float P[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        // R = U V^T
+        const float Rcr = u[r] * v[c] + u[3 + r] * v[3 + c] + u[6 + r] * v[6 + c];
+        P[3 * c + r] = k3 * (k1 * (Fc[3 * c + r] - Rcr) + k2 * cof[3 * c + r]);
+      }
+    // S = P Fc^T : S[c][r] = sum_k P[k][r] * Fc[k][c]
+    const float four_inv_dx2 = 4.0f * inv_dx * inv_dx;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const float S = P[r] * Fc[c] + P[3 + r] * Fc[3 + c] + P[6 + r] * Fc[6 + c];
+        B[3 * c + r] = mass * C[3 * c + r] + four_inv_dx2 * S;
+      }
+  }
 }
 
 // Plasticity return mapping on (U, s, V), mpm.wgsl:1366-1479.  Writes the
 // projected, safety-clamped singular values into s (in place), updates jp.
 // Returns false on a numerical fault.
 template <class T>
-__device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev& md, float& jp) {
+__device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev& md, float& jp, bool& changed) {
   float s[3] = {(float)svd.s[0], (float)svd.s[1], (float)svd.s[2]};
   if (!finitef(s[0]) || !finitef(s[1]) || !finitef(s[2])) return false;
 #pragma unroll
@@ -431,11 +512,13 @@ __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev&
   if (!finitef((float)ns[0]) || !finitef((float)ns[1]) || !finitef((float)ns[2]) || !finitef(dq) ||
       !finitef(jp + dq))
     return false;
+  changed = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     T x = ns[a];
     x = x < T(0.05) ? T(0.05) : x;
     x = x > T(20) ? T(20) : x;
+    changed = changed || x != svd.s[a];
     svd.s[a] = x;
   }
   jp = jp_replace ? jp_new : clampf(jp + dq, 0.0f, 5.0f);

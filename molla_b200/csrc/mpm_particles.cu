@@ -245,15 +245,22 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
                 for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
                 svd3<SR>(Fs, svd, stol, sweeps);
                 float jp_new = jp;
-                if (plasticity_project<SR>(svd, md, jp_new)) {
+                bool changed = true;
+                if (plasticity_project<SR>(svd, md, jp_new, changed)) {
+                  // FP32 mode rebuilds F = U s V^T every substep (the
+                  // reference); the FP64-SVD mode keeps the trial F when
+                  // the return mapping left every singular value unchanged.
                   SR Fr[9];
-                  sandwich(svd.u, svd.s, svd.v, Fr);
+                  const bool rebuild = sizeof(SR) == 4 || changed;
+                  if (rebuild) sandwich(svd.u, svd.s, svd.v, Fr);
                   bool fin4 = true;
 #pragma unroll
-                  for (int i = 0; i < 9; ++i) fin4 = fin4 && finitef((float)Fr[i]);
+                  for (int i = 0; i < 9; ++i) fin4 = fin4 && (!rebuild || finitef((float)Fr[i]));
                   if (fin4) {
+                    if (rebuild) {
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
+                      for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
+                    }
                     jp = jp_new;
                   } else {
                     atomicOr(status, kFaultNumerical);

@@ -390,11 +390,6 @@ static void p2g_particle(const orc_scene& sc, const Params<R>& p, const State<R>
     fx[a] = xp[a] - bf[a];
     quad_weights(fx[a], w[a]);
   }
-  Svd<R> svd = svd_in<R, SR>(F, sc);
-  R sc3[3];
-  for (int i = 0; i < 3; ++i) sc3[i] = clampr(svd.s[i], R(0.1), R(10));
-  const M3<R> Rm = mul(svd.u, transpose(svd.v));
-  const R J = sc3[0] * sc3[1] * sc3[2];
   const MatConst<R> mc = mat_const<R>(sc, st.mat[pid], p);
   R h = R(1);
   if (mc.rheo == 1) {
@@ -402,6 +397,33 @@ static void p2g_particle(const orc_scene& sc, const Params<R>& p, const State<R>
   } else if (mc.rheo == 0) {
     h = std::exp(clampr(st.jp[pid], R(-3), R(3)));
   }
+  M3<R> stress;
+  if constexpr (sizeof(SR) > sizeof(R)) {
+    // FP32 state with the FP64 SVD: the same stress in the principal frame,
+    // S = -dt vol U diag(tau) U^T with tau_i = 2 mu h (sc_i - 1) sc_i +
+    // lam h (J - 1) J, evaluated in FP64 and rounded once (the product's
+    // FP64-SVD mode; identical to the PK1 form below in exact arithmetic).
+    const int sweeps = sc.svd_sweeps ? (int)sc.svd_sweeps : 16;
+    const Svd<SR> sv = svd3_jacobi<SR>(cvt<SR>(F), sc.svd_tol > 0 ? (SR)sc.svd_tol : (SR)1.0e-7, sweeps);
+    SR scd[3];
+    for (int i = 0; i < 3; ++i) scd[i] = clampr(sv.s[i], SR(0.1), SR(10));
+    const SR J = scd[0] * scd[1] * scd[2];
+    SR tau[3];
+    for (int i = 0; i < 3; ++i)
+      tau[i] = SR(2) * SR(mc.mu) * SR(h) * (scd[i] - SR(1)) * scd[i] + SR(mc.lam) * SR(h) * (J - SR(1)) * J;
+    const SR k = -SR(p.dt) * SR(vol);
+    M3<SR> sd;
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r)
+        sd.m[c][r] = k * (sv.u.m[0][r] * tau[0] * sv.u.m[0][c] + sv.u.m[1][r] * tau[1] * sv.u.m[1][c] +
+                          sv.u.m[2][r] * tau[2] * sv.u.m[2][c]);
+    stress = cvt<R>(sd);
+  } else {
+  Svd<R> svd = svd_in<R, SR>(F, sc);
+  R sc3[3];
+  for (int i = 0; i < 3; ++i) sc3[i] = clampr(svd.s[i], R(0.1), R(10));
+  const M3<R> Rm = mul(svd.u, transpose(svd.v));
+  const R J = sc3[0] * sc3[1] * sc3[2];
   const R mu_h = mc.mu * h;
   const R lam_h = mc.lam * h;
   const M3<R> Fc = diag_sandwich(svd.u, sc3, svd.v);
@@ -416,7 +438,8 @@ static void p2g_particle(const orc_scene& sc, const Params<R>& p, const State<R>
   const R k3 = -p.dt * vol;
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) spk.m[c][r] = k3 * pk1.m[c][r];
-  const M3<R> stress = mul(spk, transpose(Fc));
+  stress = mul(spk, transpose(Fc));
+  }
   const R dx = p.dx;
   const R inv_dx2 = p.inv_dx * p.inv_dx;
   const R four_inv_dx2 = R(4) * inv_dx2;
@@ -604,10 +627,18 @@ static bool plasticity_particle(const orc_scene& sc, const Params<R>& p, State<R
   }
   if (!finite_vec(ns) || !std::isfinite(dq) || !std::isfinite(st.jp[pid] + dq)) return false;
   R ss[3];
-  for (int a = 0; a < 3; ++a) ss[a] = clampr(ns[a], R(0.05), R(20));
-  const M3<R> Fn = diag_sandwich(svd.u, ss, svd.v);
-  if (!finite_m(Fn)) return false;
-  store_m(st.F + 9 * pid, Fn);
+  bool changed = false;
+  for (int a = 0; a < 3; ++a) {
+    ss[a] = clampr(ns[a], R(0.05), R(20));
+    changed = changed || ss[a] != s[a];
+  }
+  // The FP64-SVD mode keeps the trial F when no singular value moved; the
+  // reference (FP32 and FP64 runs) rebuilds F = U s V^T every substep.
+  if (sizeof(SR) == sizeof(R) || changed) {
+    const M3<R> Fn = diag_sandwich(svd.u, ss, svd.v);
+    if (!finite_m(Fn)) return false;
+    store_m(st.F + 9 * pid, Fn);
+  }
   if (jp_replace) {
     st.jp[pid] = jp_new;
   } else {
