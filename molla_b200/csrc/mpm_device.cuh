@@ -100,6 +100,7 @@ struct PoolDev {
   uint32_t* status;     // kStatusWords per scene
   const Item* items;
   const uint32_t* n_items;
+  const uint8_t* item_order;  // per item: its tile's 64 cells by descending count at the regrouping
 };
 
 __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }

@@ -227,6 +227,38 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
   }
 }
 
+// One 64-thread block per item: thread c counts cell c in the item's slot
+// keys (sorted by cell within a tile) by binary search, then ranks it.
+__global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ items,
+                                                   const uint32_t* __restrict__ n_items,
+                                                   const uint32_t* __restrict__ slot_key,
+                                                   uint8_t* __restrict__ item_order) {
+  __shared__ uint32_t s_cnt[64];
+  const uint32_t it = blockIdx.x;
+  if (it >= *n_items) return;
+  const Item item = items[it];
+  const uint32_t c = threadIdx.x;
+  const uint32_t* keys = slot_key + item.start;
+  auto lower = [&](uint32_t cell) {
+    uint32_t lo = 0, hi = item.count;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((keys[mid] & 63u) < cell) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo;
+  };
+  const uint32_t cnt = (c == 63 ? item.count : lower(c + 1)) - lower(c);
+  s_cnt[c] = cnt;
+  __syncthreads();
+  uint32_t rank = 0;
+  for (uint32_t o = 0; o < 64; ++o) {
+    const uint32_t oc = s_cnt[o];
+    rank += (oc > cnt) || (oc == cnt && o < c);
+  }
+  item_order[(size_t)it * 64 + rank] = (uint8_t)c;
+}
+
 // Copy one scene's positions / velocities (3 planes from `first`) into a
 // packed xyz buffer in identity order.
 __global__ void k_gather_xyz(PoolDev p, int first, const uint32_t* __restrict__ slot_of, uint32_t id_base,
@@ -348,6 +380,13 @@ cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live
   if (K > 0)
     k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, chunk, items, n_items,
                                              tile_item);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, const uint32_t* slot_key,
+                              uint8_t* item_order, uint32_t max_items, cudaStream_t st) {
+  if (!max_items) return cudaSuccess;
+  k_item_order<<<max_items, 64, 0, st>>>(items, n_items, slot_key, item_order);
   return cudaGetLastError();
 }
 

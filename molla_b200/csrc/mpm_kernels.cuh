@@ -23,6 +23,8 @@ cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uin
                                int acc_out, cudaStream_t st);
 constexpr int kTileNodes = 216;  // 6^3 node footprint of a 4^3-cell tile of base cells
 constexpr uint32_t kFaultNondeterministic = 4u;  // a deposit left the fixed-order path
+constexpr uint32_t kFaultDeviceWait = 8u;        // a bounded device-side wait gave up (or an item was malformed)
+constexpr int kStageMax = 1008;                  // particles per scatter item (records staged in shared memory)
 // Persistent grid sizes (SMs x resident CTAs).
 int gather_grid_size(bool svd_fp64);
 int scatter_grid_size();
@@ -40,6 +42,10 @@ cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uin
                            uint32_t* orig_dst, uint32_t* slot_of, const uint32_t* ids, const uint32_t* keys,
                            uint32_t* slot_key, const float4* rec_src, float4* rec_dst, uint32_t n_live,
                            cudaStream_t st);
+// Per item the 64 cells of its tile ranked by particle count at this
+// regrouping (descending, ties by cell index): the scatter's lane order.
+cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, const uint32_t* slot_key,
+                              uint8_t* item_order, uint32_t max_items, cudaStream_t st);
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
                          Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);

@@ -10,20 +10,19 @@
 //   scatter(n+1)    27-node deposit of mass and momentum into acc[b]
 //
 // Both particle kernels are persistent over a work list of (scene, tile, slot
-// range) items built by the last regrouping.  The gather stages the 8^3-node
-// velocity block around the tile in shared memory; the scatter accumulates
-// into an 8^3-node shared block and flushes the non-empty nodes to HBM with
-// one float4 atomic each.  They are separate kernels because the gather
-// (SVD, return mapping) needs ~128 registers per thread while the scatter
-// needs few: split, the scatter runs at high occupancy and hides the latency
-// of its shared-memory atomics; the 36-byte B record costs HBM bandwidth the
-// substep does not otherwise use.  Particles are regrouped so that the 32
-// lanes of a warp hold particles of 32 different base cells (rank-major order
-// inside each tile), which makes the atomics of one stencil offset
-// conflict-free.  The SVD computed by the return mapping is reused for the
-// next substep's stress (F was rebuilt from exactly that U, diag(s), V); the
-// first substep of every step_n call runs a record-only gather that computes
-// it from F.
+// range) items built by the last regrouping (a stable radix sort of the
+// particles by base-cell key; tiles of 4^3 base cells, cut into items of at
+// most kStageMax particles).  The gather stages the 8^3-node velocity block
+// around the tile in shared memory; the scatter stages the item's 64-byte
+// records with one bulk copy, bins them by their current base cell and
+// accumulates into an 8^3-node shared block that it flushes to HBM with one
+// float4 atomic per non-empty node.  They are separate kernels because the
+// gather (SVD, return mapping) needs ~128 registers per thread while the
+// scatter needs fewer: split, each runs at its own occupancy; the B record
+// costs HBM bandwidth the substep does not otherwise use.  The SVD computed
+// by the return mapping is reused for the next substep's stress; the first
+// substep of every step_n call runs a record-only gather that computes it
+// from F.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -54,6 +53,78 @@ __device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base
   }
   const uint32_t tile = t[0] + sc.w * (t[1] + sc.w * t[2]);
   return ((sc.key_off + tile) << kCellBits) | c[0] | (c[1] << 2) | (c[2] << 4);
+}
+
+// Gather for a particle whose stencil is not inside the staged 8^3 block
+// (it left its tile since the last regrouping): 27 global reads with the
+// reference's out-of-grid skip.  Kept out of line and rolled so that the
+// unrolled shared-memory path stays small.
+__device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int n, const int* base,
+                                           const float (*w)[3], const float (*d)[3], float* vs, float* G) {
+  for (int i = 0; i < 3; ++i) vs[i] = 0.f;
+  for (int i = 0; i < 9; ++i) G[i] = 0.f;
+  for (int q = 0; q < 27; ++q) {
+    const int i = q / 9, j = (q / 3) % 3, k = q % 3;
+    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
+    if ((unsigned)ix >= (unsigned)n || (unsigned)iy >= (unsigned)n || (unsigned)iz >= (unsigned)n) continue;
+    const float4 g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+    const float wt = w[0][i] * w[1][j] * w[2][k];
+    const float gv[3] = {wt * g.x, wt * g.y, wt * g.z};
+    for (int r = 0; r < 3; ++r) {
+      vs[r] += gv[r];
+      G[r] += gv[r] * d[0][i];
+      G[3 + r] += gv[r] * d[1][j];
+      G[6 + r] += gv[r] * d[2][k];
+    }
+  }
+}
+
+// mbarrier + bulk-copy (TMA engine) helpers for the scatter's record stage.
+__device__ __forceinline__ uint32_t smem_addr(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Orders this CTA's earlier generic-proxy accesses of shared memory before
+// later async-proxy (bulk copy) writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned) completing on `bar`, which expects those bytes.
+__device__ __forceinline__ void bulk_load_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of `bar` with the given parity to complete; gives up
+// (returns false) after about one second.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > 1000000000ull) return false;
+  }
+  return true;
 }
 
 }  // namespace
@@ -141,56 +212,52 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
             const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
             const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
                                 (unsigned)lz0 <= (unsigned)(kRegion - 3);
-            const float4* __restrict__ gvel = p.vel + sc.grid_off;
             // Separable accumulation: v = sum w gv; G = sum (w gv) d^T.
             float vs[3] = {0.f, 0.f, 0.f};
             float G[9];
+            if (inside) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) G[i] = 0.f;
+              for (int i = 0; i < 9; ++i) G[i] = 0.f;
+              const float4* __restrict__ blk = &s_gath.vel[lx0 + 8 * ly0 + 64 * lz0];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              float si[3] = {0.f, 0.f, 0.f}, syi[3] = {0.f, 0.f, 0.f}, szi[3] = {0.f, 0.f, 0.f};
+              for (int i = 0; i < 3; ++i) {
+                float si[3] = {0.f, 0.f, 0.f}, syi[3] = {0.f, 0.f, 0.f}, szi[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-              for (int j = 0; j < 3; ++j) {
-                float sj[3] = {0.f, 0.f, 0.f}, szj[3] = {0.f, 0.f, 0.f};
+                for (int j = 0; j < 3; ++j) {
+                  float sj[3] = {0.f, 0.f, 0.f}, szj[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int kk = 0; kk < 3; ++kk) {
-                  float4 g;
-                  if (inside) {
-                    g = s_gath.vel[(lx0 + i) + 8 * (ly0 + j) + 64 * (lz0 + kk)];
-                  } else {
-                    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + kk;
-                    g = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
-                      g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+                  for (int kk = 0; kk < 3; ++kk) {
+                    const float4 g = blk[i + 8 * j + 64 * kk];
+                    const float wk = w[2][kk];
+                    sj[0] += wk * g.x;
+                    sj[1] += wk * g.y;
+                    sj[2] += wk * g.z;
+                    const float wdk = wk * d[2][kk];
+                    szj[0] += wdk * g.x;
+                    szj[1] += wdk * g.y;
+                    szj[2] += wdk * g.z;
                   }
-                  const float wk = w[2][kk];
-                  sj[0] += wk * g.x;
-                  sj[1] += wk * g.y;
-                  sj[2] += wk * g.z;
-                  const float wdk = wk * d[2][kk];
-                  szj[0] += wdk * g.x;
-                  szj[1] += wdk * g.y;
-                  szj[2] += wdk * g.z;
+                  const float wj = w[1][j];
+                  const float wdj = wj * d[1][j];
+#pragma unroll
+                  for (int r = 0; r < 3; ++r) {
+                    si[r] += wj * sj[r];
+                    syi[r] += wdj * sj[r];
+                    szi[r] += wj * szj[r];
+                  }
                 }
-                const float wj = w[1][j];
-                const float wdj = wj * d[1][j];
+                const float wi = w[0][i];
+                const float wdi = wi * d[0][i];
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
-                  si[r] += wj * sj[r];
-                  syi[r] += wdj * sj[r];
-                  szi[r] += wj * szj[r];
+                  vs[r] += wi * si[r];
+                  G[r] += wdi * si[r];      // column x
+                  G[3 + r] += wi * syi[r];  // column y
+                  G[6 + r] += wi * szi[r];  // column z
                 }
               }
-              const float wi = w[0][i];
-              const float wdi = wi * d[0][i];
-#pragma unroll
-              for (int r = 0; r < 3; ++r) {
-                vs[r] += wi * si[r];
-                G[r] += wdi * si[r];      // column x
-                G[3 + r] += wi * syi[r];  // column y
-                G[6 + r] += wi * szi[r];  // column z
-              }
+            } else {
+              gather_global(p.vel + sc.grid_off, n, base, w, d, vs, G);
             }
             const float four_inv_dx2 = 4.0f * sc.inv_dx * sc.inv_dx;
 #pragma unroll
@@ -349,195 +416,273 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 // Scatter of the next substep (mpm.wgsl:601-627): a particle with base =
 // floor(x/dx - 0.5) and fx = x/dx - base deposits, at the node of offset
 // (i,j,k), w m and w (m v + B d) with d = ((i,j,k) - fx) dx and w the
-// quadratic B-spline weight.  Particles whose record flag is zero (numerical
+// quadratic B-spline weight.  Particles whose record mass is zero (numerical
 // fault this substep) deposit nothing.
 //
-// One CTA per tile item, 192 threads: thread t owns cell (t mod 64) of the
-// tile and the x-slab i = t / 64 of the stencil.  It walks the particles the
-// last regrouping put in its cell (contiguous slots), adds their nine slab-i
-// node contributions in registers and then issues 9 x 4 shared-memory atomics
-// for the whole cell — about eight times fewer atomics than one per particle
-// and node, and conflict-free because the 32 lanes of a warp own 32
-// different cells.  A particle that has left its cell since the regrouping
-// deposits its own contributions directly.
+// Persistent CTAs over items (a tile's particles from the last regrouping,
+// at most kStageMax), 192 threads.  Per item:
+//  1. stage: the item's 64-byte records (contiguous slots) arrive in shared
+//     memory by one bulk copy (the TMA engine: cp.async.bulk completing on
+//     an mbarrier), issued while the previous item's block was flushed;
+//  2. bin: every particle is binned by its current base cell among the 6^3
+//     cells whose stencils fit the tile's 8^3-node block (a counting sort in
+//     shared memory with warp-aggregated counters), so particles that moved
+//     since the regrouping are grouped with their new cell-mates; one whose
+//     stencil leaves the block deposits straight to HBM;
+//  3. deposit: thread t takes x-slab i = t / 64 of the stencil and one cell
+//     (t mod 64): the tile's own cells in the order of their particle counts
+//     at the regrouping, so that the lanes of a warp walk lists of similar
+//     length, then the margin cells particles moved into.  It adds the nine
+//     slab-i node contributions of its cell's particles in registers and
+//     issues 9 x 4 shared-memory atomics for the whole cell, not per
+//     particle; the lanes of a warp own different cells, so those atomics
+//     do not collide;
+//  4. flush: every non-empty node of the 8^3 block goes to HBM with one
+//     float4 atomic and is cleared for the next item.
+// Every wait on the stage is bounded (about one second); a wait that gives
+// up sets kFaultDeviceWait in the scene's status word and ends the CTA after
+// a second bounded wait for its copy in flight.
+__device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4* __restrict__ acc, uint64_t grid_off,
+                                            int n, float ox, float oy, float oz, float inv_dx, float dx,
+                                            const int* win) {
+  const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+  const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+  const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
+  float wgt[3][3], fx[3];
+  int base[3];
+  for (int a = 0; a < 3; ++a) {
+    const float bf = floorf(xp[a] - 0.5f);
+    base[a] = (int)bf - win[a];
+    fx[a] = xp[a] - bf;
+    quad_weights(fx[a], wgt[a]);
+  }
+  for (int q = 0; q < 27; ++q) {
+    const int i = q / 9, j = (q / 3) % 3, k = q % 3;
+    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
+    if ((unsigned)ix >= (unsigned)n || (unsigned)iy >= (unsigned)n || (unsigned)iz >= (unsigned)n) continue;
+    const float wt = wgt[0][i] * wgt[1][j] * wgt[2][k];
+    const float d0 = ((float)i - fx[0]) * dx, d1 = ((float)j - fx[1]) * dx, d2 = ((float)k - fx[2]) * dx;
+    const float4 v = make_float4(wt * r0.w, wt * (r1.x + B[0] * d0 + B[3] * d1 + B[6] * d2),
+                                 wt * (r1.y + B[1] * d0 + B[4] * d1 + B[7] * d2),
+                                 wt * (r1.z + B[2] * d0 + B[5] * d1 + B[8] * d2));
+    atomicAdd(&acc[grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz)], v);
+  }
+}
+
+constexpr int kLocalCells = 216;  // 6^3 base cells whose stencils fit the 8^3 block
+constexpr int kBinRounds = (kStageMax + kScatterThreads - 1) / kScatterThreads;
+
 __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_out) {
+  extern __shared__ __align__(128) float4 s_stage[];  // [kStageMax * 4]
   __shared__ float s_acc[4][kRegionFloats];
-  __shared__ uint32_t s_first[64], s_end[64];
-  __shared__ uint8_t s_order[64];
-  __shared__ uint32_t s_fault;
+  __shared__ uint32_t s_cell[kLocalCells];  // counts, then exclusive starts
+  __shared__ uint16_t s_idx[kStageMax];     // item particles sorted by local cell
+  __shared__ uint32_t s_total;
+  __shared__ __align__(8) uint64_t s_bar;
   float4* __restrict__ acc = p.acc[acc_out];
   const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
   const uint32_t n_items = *p.n_items;
   const int slab = threadIdx.x >> 6;
+  const uint32_t lane64 = threadIdx.x & 63u;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (int r = threadIdx.x; r < 4 * kRegionFloats; r += blockDim.x) (&s_acc[0][0])[r] = 0.f;
+  for (int r = threadIdx.x; r < kLocalCells; r += blockDim.x) s_cell[r] = 0u;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // Thread 0 stages item `it` (items of 1..kStageMax particles).
+  auto stage = [&](uint32_t it) {
+    const Item nx = p.items[it];
+    if (nx.count - 1u < (uint32_t)kStageMax) {
+      fence_proxy_async_smem();
+      bulk_load_g2s(s_stage, rec + 4 * (size_t)nx.start, nx.count * 64u, &s_bar);
+    }
+  };
+  if (threadIdx.x == 0 && blockIdx.x < n_items) stage(blockIdx.x);
+  uint32_t parity = 0;
   for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
     const Item item = p.items[it];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
+    uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
+    // A fault latched before this launch freezes the scene; one latched by
+    // this substep's gather is handled per particle (m = 0 in its record).
+    const uint32_t fault0 = *(volatile uint32_t*)status;
     const uint32_t w = scp->w;
     const int n = (int)scp->n;
     const float ox = scp->ox, oy = scp->oy, oz = scp->oz, inv_dx = scp->inv_dx, dx = scp->dx;
-    const int winx = scp->winx, winy = scp->winy, winz = scp->winz;
+    const int win[3] = {scp->winx, scp->winy, scp->winz};
     const uint64_t grid_off = scp->grid_off;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
-    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)(p.status + (size_t)scp->status * kStatusWords);
-    for (int r = threadIdx.x; r < kRegionFloats; r += blockDim.x) {
-      s_acc[0][r] = 0.f;
-      s_acc[1][r] = 0.f;
-      s_acc[2][r] = 0.f;
-      s_acc[3][r] = 0.f;
+    const bool staged = item.count - 1u < (uint32_t)kStageMax;
+    bool ok = staged;
+    if (staged) {
+      ok = mbar_wait_bounded(&s_bar, parity);
+      parity ^= 1u;
     }
-    if (threadIdx.x < 64) {
-      s_first[threadIdx.x] = 0;
-      s_end[threadIdx.x] = 0;
-    }
-    __syncthreads();
-    // Cell segments of this item from the regroup keys (sorted by cell).
-    for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
-      const uint32_t s = item.start + k;
-      const uint32_t c = p.slot_key[s] & 63u;
-      if (k == 0 || (p.slot_key[s - 1] & 63u) != c) s_first[c] = s;
-      if (k + 1 == item.count || (p.slot_key[s + 1] & 63u) != c) s_end[c] = s + 1;
-    }
-    __syncthreads();
-    // Cells ranked by particle count (descending, ties by cell index) so
-    // that each warp walks cells of similar length.
-    if (threadIdx.x < 64) {
-      const int c = threadIdx.x;
-      const uint32_t my = s_end[c] - s_first[c];
-      int rank = 0;
-      for (int o = 0; o < 64; ++o) {
-        const uint32_t other = s_end[o] - s_first[o];
-        rank += (other > my) || (other == my && o < c);
+    const bool live = ok && fault0 == 0;
+    // ---- 2. bin by current base cell (rank within the cell from the
+    //         warp-aggregated counter) ----
+    uint32_t bin[kBinRounds];  // local cell << 16 | rank, or 0xffffffff
+#pragma unroll
+    for (int q = 0; q < kBinRounds; ++q) {
+      const uint32_t j = threadIdx.x + q * kScatterThreads;
+      uint32_t lc = 0xffffu;
+      if (live && j < item.count) {
+        const float4 r0 = s_stage[4 * j];
+        if (r0.w != 0.f) {
+          const int lx = (int)floorf((r0.x - ox) * inv_dx - 0.5f) - win[0] - rx;
+          const int ly = (int)floorf((r0.y - oy) * inv_dx - 0.5f) - win[1] - ry;
+          const int lz = (int)floorf((r0.z - oz) * inv_dx - 0.5f) - win[2] - rz;
+          if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
+            lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
+          } else {
+            deposit_global(s_stage + 4 * j, acc, grid_off, n, ox, oy, oz, inv_dx, dx, win);
+          }
+        }
       }
-      s_order[rank] = (uint8_t)c;
+      const uint32_t peers = __match_any_sync(0xffffffffu, lc);
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t base = 0;
+      if (lc != 0xffffu && lane == leader) base = atomicAdd(&s_cell[lc], (uint32_t)__popc(peers));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      bin[q] = lc == 0xffffu ? 0xffffffffu : (lc << 16) | (base + __popc(peers & ((1u << lane) - 1u)));
     }
     __syncthreads();
-    // A fault latched before this launch freezes the scene; one latched by
-    // this substep's gather is handled per particle (m = 0 in its record).
-    if (s_fault == 0) {
-      const int cell = s_order[threadIdx.x & 63];
-      const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
-      // base of this cell's particles in region coordinates
-      const int lbx = 1 + cx, lby = 1 + cy, lbz = 1 + cz;
+    // exclusive scan of the 216 cell counts (warp 0, 7 cells per lane)
+    if (threadIdx.x < 32) {
+      uint32_t c[7], sum = 0;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const int cell = (int)lane * 7 + k;
+        c[k] = cell < kLocalCells ? s_cell[cell] : 0u;
+        sum += c[k];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      uint32_t run = incl - sum;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const int cell = (int)lane * 7 + k;
+        if (cell < kLocalCells) s_cell[cell] = run;
+        run += c[k];
+      }
+      if (lane == 31) s_total = incl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kBinRounds; ++q) {
+      if (bin[q] != 0xffffffffu)
+        s_idx[s_cell[bin[q] >> 16] + (bin[q] & 0xffffu)] = (uint16_t)(threadIdx.x + q * kScatterThreads);
+    }
+    __syncthreads();
+    // ---- 3. deposit: one cell per lane, the tile's own 64 cells first in the
+    //         order of their counts at the regrouping (so the lanes of a warp
+    //         walk lists of similar length), then the margin cells that
+    //         particles moved into ----
+    if (live) {
+      const uint32_t total = s_total;
       float am[9], apx[9], apy[9], apz[9];
+      // Accumulates the particles of local cell lc in registers; returns
+      // whether it had any.
+      auto accumulate = [&](int lc) {
 #pragma unroll
-      for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
-      const uint32_t first = s_first[cell], end = s_end[cell];
-      const int win[3] = {winx, winy, winz};
-      // The next particle's record is loaded while this one is deposited.
-      float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0, n2 = n0, n3 = n0;
-      if (first < end) {
-        n0 = __ldg(&rec[4 * (size_t)first]);
-        n1 = __ldg(&rec[4 * (size_t)first + 1]);
-        n2 = __ldg(&rec[4 * (size_t)first + 2]);
-        n3 = __ldg(&rec[4 * (size_t)first + 3]);
-      }
-      for (uint32_t s = first; s < end; ++s) {
-        const float4 r0 = n0, r1 = n1, r2 = n2, r3 = n3;
-        if (s + 1 < end) {
-          n0 = __ldg(&rec[4 * (size_t)s + 4]);
-          n1 = __ldg(&rec[4 * (size_t)s + 5]);
-          n2 = __ldg(&rec[4 * (size_t)s + 6]);
-          n3 = __ldg(&rec[4 * (size_t)s + 7]);
-        }
-        if (r0.w == 0.f) continue;
-        const float mass = r0.w;
-        const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
-        const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
-        float wgt[3][3], fx[3];
-        int base[3];
+        for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
+        const uint32_t first = s_cell[lc], end = lc == kLocalCells - 1 ? total : s_cell[lc + 1];
+        for (uint32_t t = first; t < end; ++t) {
+          const float4* __restrict__ rp = s_stage + 4 * (uint32_t)s_idx[t];
+          const float4 r0 = rp[0], r1 = rp[1], r2 = rp[2], r3 = rp[3];
+          const float mass = r0.w;
+          const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+          const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
+          float wgt[3][3], fx[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float bf = floorf(xp[a] - 0.5f);
-          base[a] = (int)bf - win[a];
-          fx[a] = xp[a] - bf;
-          quad_weights(fx[a], wgt[a]);
-        }
-        const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
-        // slab i of the stencil: x offset i, all (j, k)
-        const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
-        const float di = ((float)slab - fx[0]) * dx;
-        const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
-        float nm[9], npx[9], npy[9], npz[9];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const float wij = wi * wgt[1][j];
-          const float dj = ((float)j - fx[1]) * dx;
-          const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
-#pragma unroll
-          for (int kk = 0; kk < 3; ++kk) {
-            const float wt = wij * wgt[2][kk];
-            const float dk = ((float)kk - fx[2]) * dx;
-            nm[3 * j + kk] = wt * mass;
-            npx[3 * j + kk] = wt * (qy[0] + B[6] * dk);
-            npy[3 * j + kk] = wt * (qy[1] + B[7] * dk);
-            npz[3 * j + kk] = wt * (qy[2] + B[8] * dk);
+          for (int a = 0; a < 3; ++a) {
+            const float bf = floorf(xp[a] - 0.5f);
+            fx[a] = xp[a] - bf;
+            quad_weights(fx[a], wgt[a]);
           }
-        }
-        if (lx0 == lbx && ly0 == lby && lz0 == lbz) {
+          // slab i of the stencil: x offset i, all (j, k)
+          const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
+          const float di = ((float)slab - fx[0]) * dx;
+          const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
 #pragma unroll
-          for (int q = 0; q < 9; ++q) {
-            am[q] += nm[q];
-            apx[q] += npx[q];
-            apy[q] += npy[q];
-            apz[q] += npz[q];
-          }
-        } else if ((unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
-                   (unsigned)lz0 <= (unsigned)(kRegion - 3)) {
-          // left its cell since the regrouping, still inside the block
-#pragma unroll
-          for (int j = 0; j < 3; ++j)
+          for (int j = 0; j < 3; ++j) {
+            const float wij = wi * wgt[1][j];
+            const float dj = ((float)j - fx[1]) * dx;
+            const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
 #pragma unroll
             for (int kk = 0; kk < 3; ++kk) {
-              const int r = region_index(lx0 + slab, ly0 + j, lz0 + kk);
-              atomicAdd(&s_acc[0][r], nm[3 * j + kk]);
-              atomicAdd(&s_acc[1][r], npx[3 * j + kk]);
-              atomicAdd(&s_acc[2][r], npy[3 * j + kk]);
-              atomicAdd(&s_acc[3][r], npz[3 * j + kk]);
+              const float wt = wij * wgt[2][kk];
+              const float dk = ((float)kk - fx[2]) * dx;
+              am[3 * j + kk] += wt * mass;
+              apx[3 * j + kk] += wt * (qy[0] + B[6] * dk);
+              apy[3 * j + kk] += wt * (qy[1] + B[7] * dk);
+              apz[3 * j + kk] += wt * (qy[2] + B[8] * dk);
             }
-        } else {
-          // outside the block: straight to HBM
-#pragma unroll
-          for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-              const int ix = base[0] + slab, iy = base[1] + j, iz = base[2] + kk;
-              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-                const uint64_t c =
-                    grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-                atomicAdd(&acc[c], make_float4(nm[3 * j + kk], npx[3 * j + kk], npy[3 * j + kk], npz[3 * j + kk]));
-              }
-            }
+          }
         }
-      }
-      if (end > first) {
+        return end > first;
+      };
+      // Adds the accumulated slab of local cell lc to the shared block.
+      auto flush = [&](int lc) {
+        const int r0 = region_index(lc % 6, (lc / 6) % 6, lc / 36) + slab;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
           for (int kk = 0; kk < 3; ++kk) {
-            const int r = region_index(lbx + slab, lby + j, lbz + kk);
+            const int r = r0 + kRsy * j + kRsz * kk;
             atomicAdd(&s_acc[0][r], am[3 * j + kk]);
             atomicAdd(&s_acc[1][r], apx[3 * j + kk]);
             atomicAdd(&s_acc[2][r], apy[3 * j + kk]);
             atomicAdd(&s_acc[3][r], apz[3 * j + kk]);
           }
+      };
+      {
+        const uint32_t c = p.item_order[(size_t)it * 64 + lane64];
+        const int lc = (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
+        if (accumulate(lc)) flush(lc);
+      }
+#pragma unroll 1
+      for (int lc = (int)lane64; lc < kLocalCells; lc += 64) {
+        const int lx = lc % 6, ly = (lc / 6) % 6, lz = lc / 36;
+        const bool core = lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4;
+        if (!core && accumulate(lc)) flush(lc);
       }
     }
-    __syncthreads();
-    if (s_fault == 0) {
-      for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-        const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
-        const int q = region_index(lx, ly, lz);
-        const float m = s_acc[0][q], px = s_acc[1][q], py = s_acc[2][q], pz = s_acc[3][q];
-        if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
-          const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
-          if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-            const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-            atomicAdd(&acc[c], make_float4(m, px, py, pz));
-          }
+    if (__syncthreads_or(!ok)) {
+      // The stage did not arrive (or the item exceeds the stage): report it,
+      // wait once more (bounded) for the copy in flight and stop this CTA.
+      if (threadIdx.x == 0) atomicOr(status, kFaultDeviceWait);
+      if (staged) mbar_wait_bounded(&s_bar, parity ^ 1u);
+      return;
+    }
+    // Every thread is done with the stage: the next item's copy goes now.
+    if (threadIdx.x == 0 && it + gridDim.x < n_items) stage(it + gridDim.x);
+    // ---- 4. flush the block, clear it and the cell counters ----
+    for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
+      const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
+      const int q = region_index(lx, ly, lz);
+      const float m = s_acc[0][q], px = s_acc[1][q], py = s_acc[2][q], pz = s_acc[3][q];
+      if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
+        s_acc[0][q] = 0.f;
+        s_acc[1][q] = 0.f;
+        s_acc[2][q] = 0.f;
+        s_acc[3][q] = 0.f;
+        const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
+        if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
+          const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+          atomicAdd(&acc[c], make_float4(m, px, py, pz));
         }
       }
     }
+    for (int r = threadIdx.x; r < kLocalCells; r += blockDim.x) s_cell[r] = 0u;
     __syncthreads();
   }
 }
@@ -759,8 +904,10 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
   return cudaErrorInvalidValue;
 }
 
+constexpr size_t kStageBytes = (size_t)kStageMax * 64;
+
 cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st) {
-  k_p2g<<<grid, kScatterThreads, 0, st>>>(p, acc_out);
+  k_p2g<<<grid, kScatterThreads, kStageBytes, st>>>(p, acc_out);
   return cudaGetLastError();
 }
 
@@ -776,11 +923,11 @@ cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uin
   return cudaGetLastError();
 }
 
-static int persistent(const void* fn, int threads) {
+static int persistent(const void* fn, int threads, size_t dyn_smem = 0) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, dyn_smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   if (sms < 1) sms = 148;
   return sms * per_sm;
@@ -791,6 +938,10 @@ int gather_grid_size(bool svd_fp64) {
                   : persistent((const void*)k_g2p<kG2PRecord, false, float>, kGatherThreads);
 }
 
-int scatter_grid_size() { return persistent((const void*)k_p2g, kScatterThreads); }
+int scatter_grid_size() {
+  // the record stage needs more than the default 48 KB of dynamic shared memory
+  cudaFuncSetAttribute((const void*)k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+  return persistent((const void*)k_p2g, kScatterThreads, kStageBytes);
+}
 
 }  // namespace mpm

@@ -293,6 +293,7 @@ PoolDev Group::pool() const {
   p.status = status_d.ptr;
   p.items = items.ptr;
   p.n_items = n_items.ptr;
+  p.item_order = item_order.ptr;
   return p;
 }
 
@@ -325,11 +326,13 @@ void Group::rebuild_layout() {
   }
   key_space = (uint32_t)k;
   if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
-  const size_t max_items = (size_t)key_space + 2;  // one item per occupied tile
+  const size_t max_items = max_item_count();
   if (items.count < max_items) items.alloc(max_items);
+  if (item_order.count < 64 * max_items) item_order.alloc(64 * max_items);
   if (deterministic) {
-    if (tile_item.count < (size_t)key_space + 2) tile_item.alloc((size_t)key_space + 2);
-    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
+    const size_t tiles = (size_t)key_space + 2;
+    if (tile_item.count < tiles) tile_item.alloc(tiles);
+    if (det_blocks.count < tiles * kTileNodes) det_blocks.alloc(tiles * kTileNodes);
   }
   if (!offs.empty()) {
     MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -544,9 +547,17 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   eng->launches += 1;
   cur ^= 1;
   if (move_records) rec_cur ^= 1;
+  // Items: whole tiles for the fixed-order scatter (one item per tile);
+  // otherwise tiles cut into pieces of at most kStageMax particles, whose
+  // scatter records fit the shared-memory stage.
   MPM_CK(launch_items(skeys, kCellBits, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(),
-                      scene_ids_d.ptr, 0, items.ptr, n_items.ptr, deterministic ? tile_item.ptr : nullptr, st));
+                      scene_ids_d.ptr, deterministic ? 0u : (uint32_t)kStageMax, items.ptr, n_items.ptr,
+                      deterministic ? tile_item.ptr : nullptr, st));
   eng->launches += key_space ? 2 : 1;
+  if (!deterministic && key_space) {
+    MPM_CK(launch_item_order(items.ptr, n_items.ptr, slot_key.ptr, item_order.ptr, (uint32_t)max_item_count(), st));
+    eng->launches += 1;
+  }
   need_regroup = false;
   eng->prof_end(&pr, st);
 }

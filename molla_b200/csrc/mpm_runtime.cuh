@@ -169,6 +169,7 @@ class Group {
   DevBuf<uint32_t> status_d;
   DevBuf<uint32_t> tile_start, key_offs_d, scene_ids_d, n_items;
   DevBuf<Item> items;
+  DevBuf<uint8_t> item_order;  // scatter lane order, 64 cells per item
   DevBuf<uint32_t> tile_item;  // deterministic mode: item of each occupied tile
   DevBuf<float4> det_blocks;   // deterministic mode: per-tile 6^3 node blocks
   DevBuf<double> totals_d;
@@ -219,6 +220,8 @@ class Group {
   // Same through a cached CUDA graph.
   void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st);
   void regroup(bool compute_keys, cudaStream_t st, bool move_records = false);
+  // one item per occupied tile, plus one per kStageMax particles of a tile
+  size_t max_item_count() const { return (size_t)key_space + cap / kStageMax + 2; }
   void sync_scenes(cudaStream_t st);
 
   PoolDev pool() const;
