@@ -335,9 +335,10 @@ MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
  * results are then bit-identical from run to run and alone or in any mix
  * (the group equivalent of mpm_set_deterministic_p2g). */
 MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
-/* Autotuner: times `probe_substeps` substeps of the group for each candidate
- * regrouping interval (n_candidates values, NULL → {4, 8, 16, 32, 64, 128})
- * on a snapshot of the device state, restores the state (the scenes do not
+/* Autotuner: times max(probe_substeps, 2 x candidate) substeps of the group
+ * for each candidate regrouping interval (n_candidates values, NULL → {4, 8,
+ * 16, 32, 64, 128}) — so every candidate regroups at least twice — on a
+ * snapshot of the device state, restores the state (the scenes do not
  * advance) and keeps the fastest interval.  ms_per_substep (may be NULL)
  * receives one timing per candidate; *chosen the interval kept. */
 MPM_API int mpm_group_autotune(mpm_group* group, uint32_t probe_substeps, const uint32_t* candidates,
@@ -347,7 +348,8 @@ MPM_API int mpm_group_autotune(mpm_group* group, uint32_t probe_substeps, const 
 MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const uint32_t* candidates,
                          uint32_t n_candidates, float* ms_per_substep, uint32_t* chosen);
 /* Group tuning: regroup (sort) interval in substeps (0 → default 32).  The
- * `chunk` argument is reserved (work items are whole 4^3 tiles). */
+ * `chunk` argument is reserved (work items are 4^3 tiles of at most 1008
+ * particles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
 /* ---- serving ------------------------------------------------------------- */

@@ -639,19 +639,21 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
     need_regroup = true;  // every candidate starts from a fresh regrouping
     if (c) save(false);
     sort_interval = cands[c];
-    run_substeps(probe, st);  // warm
+    // at least two regroupings inside the timed window
+    const uint32_t n = std::max<uint32_t>(probe, 2u * cands[c]);
+    run_substeps(n, st);  // warm
     cur = cur0;
     acc_zero = az0;
     acc_last = al0;
     need_regroup = true;
     save(false);
     MPM_CK(cudaEventRecord(e0, st));
-    run_substeps(probe, st);
+    run_substeps(n, st);
     MPM_CK(cudaEventRecord(e1, st));
     MPM_CK(cudaEventSynchronize(e1));
     float ms = 0.f;
     MPM_CK(cudaEventElapsedTime(&ms, e0, e1));
-    ms /= (float)probe;
+    ms /= (float)n;
     if (ms_out) ms_out[c] = ms;
     if (ms < best) {
       best = ms;
