@@ -10,7 +10,7 @@ modulus log-uniform in [1e4, 1e5] or snow with theta_c 2.5e-2, theta_s
 steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload large|cube|batched]
+                    [--workload large|medium|cube|cube128|batched|served]
 
 N > 1 runs under torchrun: every rank steps its own replica of the scene
 (independent scenes, no data-path collective; "scaling": "weak"); time is the
@@ -42,13 +42,20 @@ UNIT = "particle-steps/s"
 # Algorithmic bytes per launch of the two particle kernels (FP32 state):
 #  gather (G2P + F update + return mapping + stress record): reads pos 12,
 #    F 36, jp 4, mass 4, volume 4, material 4 = 64 B and writes pos 12, vel 12,
-#    C 36, F 36, jp 4, B record 36, flag 4 = 140 B per particle; reads the grid
-#    velocity once per active node (16 B).
-#  scatter (P2G deposit): reads pos 12, vel 12, mass 4, B 36, flag 4 = 68 B per
-#    particle; adds one float4 accumulator per active node (16 B).
+#    C 36, F 36, jp 4 and the 64-byte scatter record (x, m, m v, B) = 164 B per
+#    particle; reads the grid velocity once per active node (16 B).
+#  scatter (P2G deposit): reads the 64-byte record per particle; adds one
+#    float4 accumulator per active node (16 B).
 KERNEL_BYTES = {
-    "GridToParticle": (204, 16),
-    "ParticleToGrid": (68, 16),
+    "GridToParticle": (228, 16),
+    "ParticleToGrid": (64, 16),
+}
+# DRAM bytes per particle per launch (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one ncu capture of each kernel on the medium
+# workload (128^3 grid, 2M particles, substep ~280), scaled by particle count.
+MEASURED_TRAFFIC_PER_PARTICLE = {
+    "GridToParticle": 215.1,
+    "ParticleToGrid": 74.3,
 }
 # Whole-step model of the survey (separate P2G and G2P passes):
 # 268 B per particle-step + 56 B per active cell-step.
@@ -161,6 +168,11 @@ def make_workload(name: str, rank: int):
             {"workload": "single large scene: 256^3 grid, 16M particles in 4 seeded boxes (elastic E 1e4..1e5 / "
                          "snow), FP32 + FP64 SVD, dt 2e-5", "grid": 256, "particles": 16_000_000,
              "svd": "fp64", "l2": "inputs (2.6 GB state) exceed the 126 MB L2; no flush needed"}
+    if name == "medium":
+        return scenes.boxes_scene(grid_size=128, n_particles=2_000_000, n_boxes=4, seed=1 + rank, dt=4.0e-5), \
+            {"workload": "profiling case: the large scene's generator at 128^3 grid, 2M particles, FP32 + FP64 SVD, "
+                         "dt 4e-5 (same CFL number)", "grid": 128, "particles": 2_000_000, "svd": "fp64",
+             "l2": "state (330 MB) exceeds the 126 MB L2"}
     if name == "cube128":
         return scenes.cube_scene(grid_size=128, seed=rank), \
             {"workload": "elastic cube scaled: 128^3 grid, 1M particles, E 1e4, FP32 + FP64 SVD, dt 5e-5",
@@ -361,9 +373,12 @@ def run_ours(args):
             "p99_step_ms": float(np.percentile(lat, 99)) if lat else None,
             "stages_ms_per_step": {k: v[1] / max(args.steps, 1) for k, v in prof.items()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": {"GridToParticle": "k_gather<G2P + return mapping + record>",
-                                    "ParticleToGrid": "k_scatter"}[dom],
+                         "frac": achieved / hbm, "traffic": MEASURED_TRAFFIC_PER_PARTICLE[dom] * n,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on the medium "
+                                           "workload, scaled by particle count",
+                         "peak_kind": peak_kind,
+                         "kernel": {"GridToParticle": "k_g2p<G2P + return mapping + record>",
+                                    "ParticleToGrid": "k_p2g"}[dom],
                          "bytes_per_launch": fused_bytes, "avg_launch_ms": fused_ms},
             "kernels": kernels,
             "step_roofline": {"achieved": step_achieved, "frac": step_achieved / hbm,
@@ -544,7 +559,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "cube", "cube128", "batched", "served"])
+    ap.add_argument("--workload", default="large", choices=["large", "medium", "cube", "cube128", "batched", "served"])
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--arrival-rate", type=float, default=200.0)
