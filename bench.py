@@ -218,7 +218,7 @@ def run_reference(args):
     # Size the sample so the whole run stays within about two minutes.
     probe = cpu_sample_scene(200_000)
     rate, _ = time_cpu_oracle(probe, 1, 0, threads)
-    budget_s = 120.0
+    budget_s = float(args.reference_budget_s)
     per_step = budget_s / max(args.steps + args.warmup, 1)
     n_sample = int(min(16_000_000, max(20_000, rate * per_step * 0.8)))
     scene = cpu_sample_scene(n_sample)
@@ -571,6 +571,8 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-budget-s", type=float, default=120.0,
+                    help="CPU seconds the reference arm sizes its sample for")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

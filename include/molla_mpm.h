@@ -331,10 +331,6 @@ MPM_API int mpm_group_scene_count(mpm_group* group, uint32_t* count);
  * results are then bit-identical from run to run and alone or in any mix
  * (the group equivalent of mpm_set_deterministic_p2g). */
 MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
-/* Fixed-order (deterministic) P2G for every scene of the group: a scene's
- * results are then bit-identical from run to run and alone or in any mix
- * (the group equivalent of mpm_set_deterministic_p2g). */
-MPM_API int mpm_group_set_deterministic(mpm_group* group, int enabled);
 /* Autotuner: times max(probe_substeps, 2 x candidate) substeps of the group
  * for each candidate regrouping interval (n_candidates values, NULL → {4, 8,
  * 16, 32, 64, 128}) — so every candidate regroups at least twice — on a
