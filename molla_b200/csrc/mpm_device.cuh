@@ -93,6 +93,7 @@ struct PoolDev {
   uint32_t* orig;       // identity per slot
   uint32_t* keys_by_id; // sort key per identity (written when a regroup is due)
   float4* acc[2];       // grid accumulators (mass, momentum)
+  uint8_t* touched[2];  // per 256-cell block of the grid pool: acc[i] holds deposits there
   float4* vel;          // grid velocity (vx, vy, vz, mass)
   float* rec;           // per slot 16 floats: (x, y, z, m), (m v, B0), (B1..B4), (B5..B8)
   const uint32_t* slot_key;  // regroup key of each slot: (tile << 6) | cell in tile
@@ -104,6 +105,10 @@ struct PoolDev {
 };
 
 __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }
+
+// Marks the 256-cell block of grid-pool cell g as holding deposits (the grid
+// update then converts and later clears only marked blocks).
+__device__ __forceinline__ void touch(uint8_t* touched, uint64_t g) { touched[g >> 8] = 1; }
 
 __device__ __forceinline__ bool finitef(float x) {
   return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u;  // mpm.wgsl:217-219

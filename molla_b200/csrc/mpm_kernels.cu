@@ -38,25 +38,34 @@ __device__ __forceinline__ uint32_t tile_key_of(const SceneDev& sc, float x, flo
 
 }  // namespace
 
-// grid_update (mpm.wgsl:1013-1058) over the grid pool, clearing the other
-// accumulator for the next scatter and counting completed substeps.
+// grid_update (mpm.wgsl:1013-1058) over the grid pool, one block per
+// 256-cell block.  Only blocks the last scatter touched are converted; the
+// blocks touched by the scatter before it are cleared in the other
+// accumulator (ready for the next scatter) and unmarked.  Counts completed
+// substeps.
 __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
                                                               uint64_t total_cells, int acc_in, int count_substep) {
-  const uint64_t g = (uint64_t)blockIdx.x * kCellThreads + threadIdx.x;
-  if (g >= total_cells) return;
-  const float4 a = p.acc[acc_in][g];
-  p.acc[acc_in ^ 1][g] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t sid = block_scene[g / kCellBlock];
+  static_assert(kCellThreads == kCellBlock, "one thread block per grid-pool block");
+  const uint64_t blk = blockIdx.x;
+  const uint64_t g = blk * kCellThreads + threadIdx.x;
+  if (blk * kCellThreads >= total_cells) return;
+  const uint32_t sid = block_scene[blk];
   if (sid == 0xffffffffu) return;
+  const bool in_a = p.touched[acc_in][blk] != 0;
+  const bool in_b = p.touched[acc_in ^ 1][blk] != 0;
+  if (in_b) p.acc[acc_in ^ 1][g] = make_float4(0.f, 0.f, 0.f, 0.f);
   const SceneDev& sc = p.scenes[sid];
   const uint64_t local64 = g - sc.grid_off;
   const uint32_t n = sc.n;
-  if (local64 >= (uint64_t)n * n * n) return;
-  const uint32_t local = (uint32_t)local64;  // grids hold fewer than 2^32 cells
-  if (count_substep && local == 0) {
+  if (count_substep && local64 == 0) {
     uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
     if (*(volatile uint32_t*)status == 0u) atomicAdd(status + 1, 1u);
   }
+  __syncthreads();  // every thread has read the marks
+  if (threadIdx.x == 0 && in_b) p.touched[acc_in ^ 1][blk] = 0;
+  if (!in_a || local64 >= (uint64_t)n * n * n) return;
+  const uint32_t local = (uint32_t)local64;  // grids hold fewer than 2^32 cells
+  const float4 a = p.acc[acc_in][g];
   const float m = a.x;
   if (m <= 1.0e-9f || !(m == m)) {
     p.vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -442,9 +442,9 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 // Every wait on the stage is bounded (about one second); a wait that gives
 // up sets kFaultDeviceWait in the scene's status word and ends the CTA after
 // a second bounded wait for its copy in flight.
-__device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4* __restrict__ acc, uint64_t grid_off,
-                                            int n, float ox, float oy, float oz, float inv_dx, float dx,
-                                            const int* win) {
+__device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4* __restrict__ acc,
+                                            uint8_t* __restrict__ touched, uint64_t grid_off, int n, float ox,
+                                            float oy, float oz, float inv_dx, float dx, const int* win) {
   const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
   const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
   const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
@@ -465,7 +465,9 @@ __device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4
     const float4 v = make_float4(wt * r0.w, wt * (r1.x + B[0] * d0 + B[3] * d1 + B[6] * d2),
                                  wt * (r1.y + B[1] * d0 + B[4] * d1 + B[7] * d2),
                                  wt * (r1.z + B[2] * d0 + B[5] * d1 + B[8] * d2));
-    atomicAdd(&acc[grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz)], v);
+    const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+    atomicAdd(&acc[c], v);
+    touch(touched, c);
   }
 }
 
@@ -480,6 +482,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
   __shared__ uint32_t s_total;
   __shared__ __align__(8) uint64_t s_bar;
   float4* __restrict__ acc = p.acc[acc_out];
+  uint8_t* __restrict__ touched = p.touched[acc_out];
   const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
   const uint32_t n_items = *p.n_items;
   const int slab = threadIdx.x >> 6;
@@ -539,7 +542,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
           if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
             lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
           } else {
-            deposit_global(s_stage + 4 * j, acc, grid_off, n, ox, oy, oz, inv_dx, dx, win);
+            deposit_global(s_stage + 4 * j, acc, touched, grid_off, n, ox, oy, oz, inv_dx, dx, win);
           }
         }
       }
@@ -679,6 +682,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
         if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
           const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
           atomicAdd(&acc[c], make_float4(m, px, py, pz));
+          touch(touched, c);
         }
       }
     }
@@ -787,6 +791,7 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
                 const uint64_t c =
                     grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
                 atomicAdd(&p.acc[acc_out][c], make_float4(dm, px, py, pz));
+                touch(p.touched[acc_out], c);
               }
             }
           }
@@ -871,9 +876,11 @@ __global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, cons
         }
     if (mine) {
       // One writer per node; the cell holds zero or out-of-order deposits.
-      float4& a = p.acc[acc_out][scp->grid_off + (uint64_t)g[0] + (uint64_t)n * ((uint64_t)g[1] + (uint64_t)n * g[2])];
+      const uint64_t c = scp->grid_off + (uint64_t)g[0] + (uint64_t)n * ((uint64_t)g[1] + (uint64_t)n * g[2]);
+      float4& a = p.acc[acc_out][c];
       const float4 old = a;
       a = make_float4(old.x + sum.x, old.y + sum.y, old.z + sum.z, old.w + sum.w);
+      touch(p.touched[acc_out], c);
     }
   }
 }

@@ -240,6 +240,8 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   hist.alloc(sort_hist_words(cap));
   vel.alloc(cell_cap);
   block_scene.alloc(cell_cap / kCellBlock);
+  touched[0].alloc(cell_cap / kCellBlock);
+  touched[1].alloc(cell_cap / kCellBlock);
   scenes_d.alloc(max_scenes);
   status_d.alloc((size_t)kStatusWords * max_scenes);
   key_offs_d.alloc(max_scenes);
@@ -251,6 +253,8 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaMemsetAsync(acc[0].ptr, 0, acc[0].bytes(), stream));
   MPM_CK(cudaMemsetAsync(acc[1].ptr, 0, acc[1].bytes(), stream));
   MPM_CK(cudaMemsetAsync(vel.ptr, 0, vel.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(touched[0].ptr, 0, touched[0].bytes(), stream));
+  MPM_CK(cudaMemsetAsync(touched[1].ptr, 0, touched[1].bytes(), stream));
   MPM_CK(cudaMemsetAsync(keys_by_id.ptr, 0xff, keys_by_id.bytes(), stream));
   MPM_CK(cudaMemsetAsync(block_scene.ptr, 0xff, block_scene.bytes(), stream));
   MPM_CK(cudaMemsetAsync(status_d.ptr, 0, status_d.bytes(), stream));
@@ -286,6 +290,8 @@ PoolDev Group::pool() const {
   p.keys_by_id = keys_by_id.ptr;
   p.acc[0] = acc[0].ptr;
   p.acc[1] = acc[1].ptr;
+  p.touched[0] = touched[0].ptr;
+  p.touched[1] = touched[1].ptr;
   p.vel = vel.ptr;
   p.rec = rec[rec_cur].ptr;
   p.slot_key = slot_key.ptr;
@@ -433,6 +439,8 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   MPM_CK(cudaMemsetAsync(acc[0].ptr + g0, 0, glen * sizeof(float4), stream));
   MPM_CK(cudaMemsetAsync(acc[1].ptr + g0, 0, glen * sizeof(float4), stream));
   MPM_CK(cudaMemsetAsync(vel.ptr + g0, 0, glen * sizeof(float4), stream));
+  MPM_CK(cudaMemsetAsync(touched[0].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
+  MPM_CK(cudaMemsetAsync(touched[1].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   {
     std::vector<uint32_t> bs(glen / kCellBlock, sid);
     MPM_CK(cudaMemcpyAsync(block_scene.ptr + g0 / kCellBlock, bs.data(), bs.size() * 4, cudaMemcpyHostToDevice,
@@ -596,6 +604,7 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
   DevBuf<float> bplanes((size_t)kPlanes * cap);
   DevBuf<uint32_t> bmeta(cap), borig(cap), bslot(cap), bkey(cap), bstatus(status_d.count);
   DevBuf<float4> bacc0(cells_hw), bacc1(cells_hw), bvel(cells_hw);
+  DevBuf<uint8_t> btouch0(cells_hw / kCellBlock + 1), btouch1(cells_hw / kCellBlock + 1);
   auto save = [&](bool to_backup) {
     auto cp = [&](void* dst, const void* src, size_t bytes) {
       if (bytes) MPM_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
@@ -610,6 +619,8 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
       cp(bacc0.ptr, acc[0].ptr, cells_hw * sizeof(float4));
       cp(bacc1.ptr, acc[1].ptr, cells_hw * sizeof(float4));
       cp(bvel.ptr, vel.ptr, cells_hw * sizeof(float4));
+      cp(btouch0.ptr, touched[0].ptr, cells_hw / kCellBlock);
+      cp(btouch1.ptr, touched[1].ptr, cells_hw / kCellBlock);
     } else {
       cp(planes[cur].ptr, bplanes.ptr, pbytes);
       cp(meta[cur].ptr, bmeta.ptr, cap * 4);
@@ -620,6 +631,8 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
       cp(acc[0].ptr, bacc0.ptr, cells_hw * sizeof(float4));
       cp(acc[1].ptr, bacc1.ptr, cells_hw * sizeof(float4));
       cp(vel.ptr, bvel.ptr, cells_hw * sizeof(float4));
+      cp(touched[0].ptr, btouch0.ptr, cells_hw / kCellBlock);
+      cp(touched[1].ptr, btouch1.ptr, cells_hw / kCellBlock);
     }
   };
   const int cur0 = cur, az0 = acc_zero, al0 = acc_last;

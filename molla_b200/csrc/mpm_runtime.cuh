@@ -163,6 +163,7 @@ class Group {
   DevBuf<uint32_t> slot_of, keys_by_id, slot_key, ks[2], vs[2], hist;
   // grid pool
   DevBuf<float4> acc[2], vel;
+  DevBuf<uint8_t> touched[2];  // per 256-cell block: acc[i] is nonzero there
   DevBuf<uint32_t> block_scene;
   // scenes
   DevBuf<SceneDev> scenes_d;
