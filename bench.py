@@ -413,6 +413,103 @@ def _stage_roofline(prof, n, active, hbm):
     return dom, kernels
 
 
+def run_precision(args):
+    """Precision study: the cube scene (config 0 geometry, sticky walls) at
+    --precision-grid (128: 1M particles, dt 5e-5) run on the GPU as all-FP32,
+    FP32 + FP64 SVD and all-FP64, against the FP64 CPU oracle (FP64 Jacobi
+    SVD, tol 1e-14); position and grid-momentum errors every 100 substeps."""
+    import torch
+
+    import molla_b200 as m
+    from molla_b200 import scenes
+    from oracle import oracle as O
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU (the MPM path has no CPU fallback)")
+    g = args.precision_grid
+    scene = scenes.cube_scene(grid_size=g, seed=0, walls=1)
+    total = args.precision_steps
+    every = 100
+    engine = m.Engine(0)
+    runs = {}
+    for name, prec in (("fp32", 0), ("fp32_svd64", 1)):
+        cfg = m.config_for_scene(scene, svd_precision=prec)
+        sim = m.MpmSimulation.new(engine, cfg)
+        sim.set_particles(scene.positions)
+        sim.set_materials(scene.rows, scene.ids)
+        runs[name] = (sim, cfg)
+    cfg64 = m.config_for_scene(scene, svd_precision=1)
+    sim64 = m.MpmSimulation64(engine, cfg64)
+    sim64.set_particles(scene.positions.astype(np.float64))
+    sim64.set_materials(scene.rows, scene.ids)
+    osc = O.make_scene(cfg64, scene.rows, scene.dt, svd_tol=1e-14, svd_sweeps=30)
+    st = O.cast_state(O.init_state(scene.positions, mass=cfg64.particle_mass, volume=cfg64.particle_volume,
+                                   ids=scene.ids), np.float64)
+    threads = O.max_threads()
+    mass0 = float(np.float32(cfg64.particle_mass)) * scene.n
+    dt = float(np.float32(scene.dt))
+    rows = []
+    gpu_ms = {k: 0.0 for k in ("fp32", "fp32_svd64", "fp64_gpu")}
+    cpu_s = 0.0
+    done = 0
+    while done < total:
+        k = min(every, total - done)
+        for name, (sim, _) in runs.items():
+            engine.synchronize()
+            t = time.perf_counter()
+            sim.step_n(scene.dt, k)
+            engine.synchronize()
+            gpu_ms[name] += 1000.0 * (time.perf_counter() - t)
+        engine.synchronize()
+        t = time.perf_counter()
+        sim64.step_n(dt, k)
+        engine.synchronize()
+        gpu_ms["fp64_gpu"] += 1000.0 * (time.perf_counter() - t)
+        t = time.perf_counter()
+        gm, gp = O.step(osc, st, k, precision="f64", nthreads=threads, want_grid=True)
+        cpu_s += time.perf_counter() - t
+        done += k
+        ref = st["pos"]
+        ref_mom = gp.reshape(-1, 3).sum(axis=0)
+        ref_norm = float(np.linalg.norm(ref_mom)) or 1.0
+        row = {"step": done, "oracle_grid_mass_drift": float(gm.sum() / mass0 - 1.0)}
+        outs = {name: (sim.read_positions().astype(np.float64), sim.conservation_totals())
+                for name, (sim, _) in runs.items()}
+        m64 = sim64.grid_totals()
+        outs["fp64_gpu"] = (sim64.read_positions(), np.array([m64[0], *m64[1], 0, 0, 0, 0]))
+        for name, (pos, tot) in outs.items():
+            d = pos - ref
+            row[name] = {
+                "pos_rel_max": float((np.abs(d) / np.maximum(np.abs(ref), 1e-30)).max()),
+                "pos_rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+                "pos_abs_max": float(np.abs(d).max()),
+                "grid_momentum_rel": float(np.linalg.norm(tot[1:4] - ref_mom) / ref_norm),
+                "grid_mass_drift": float(tot[0] / mass0 - 1.0),
+            }
+        rows.append(row)
+        print(json.dumps({"progress": row}), file=sys.stderr, flush=True)
+    last = rows[-1]
+    line = {
+        "metric": "position / grid-momentum error vs the FP64 CPU oracle per 100 substeps", "unit": "relative",
+        "value": last["fp32_svd64"]["pos_rel_max"], "higher_is_better": False, "n_gpus": 1,
+        "steps": total, "warmup": 0, "dtype": "f32 | f32 (fp64 svd) | f64",
+        "data": "synthetic (seeded jittered cube; no dataset)",
+        "config": {"workload": f"precision study: elastic cube [0.3,0.7]^3, {g}^3 grid, {scene.n} particles, "
+                               f"E 1e4, nu 0.2, rho 1, sticky walls 3 cells, dt {scene.dt:g}",
+                   "oracle": "FP64 CPU restatement, FP64 Jacobi SVD tol 1e-14 / 30 sweeps",
+                   "modes": ["fp32", "fp32_svd64", "fp64_gpu"]},
+        "gate_pos_rel_1e-4_at_end": {k: last[k]["pos_rel_max"] < 1e-4 for k in ("fp32", "fp32_svd64", "fp64_gpu")},
+        "gpu_ms_per_step": {k: v / total for k, v in gpu_ms.items()},
+        "oracle_s_per_step": cpu_s / total, "oracle_threads": threads,
+        "errors": rows,
+    }
+    print(json.dumps(line), flush=True)
+    for sim, _ in runs.values():
+        sim.close()
+    sim64.close()
+    engine.close()
+
+
 def run_batched(args):
     """64 independent scenes of uneven size (grids log-uniform 32^3..128^3,
     10k..2M particles at 8 per cell, half elastic half snow) stepped in the
@@ -559,7 +656,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "medium", "cube", "cube128", "batched", "served"])
+    ap.add_argument("--workload", default="large", choices=["large", "medium", "cube", "cube128", "batched", "served", "precision"])
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--arrival-rate", type=float, default=200.0)
@@ -571,6 +668,8 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-grid", type=int, default=128)
+    ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--reference-budget-s", type=float, default=120.0,
                     help="CPU seconds the reference arm sizes its sample for")
     args = ap.parse_args()
@@ -582,6 +681,8 @@ def main():
         run_batched(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "precision":
+        run_precision(args)
     else:
         run_ours(args)
 

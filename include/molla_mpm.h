@@ -348,6 +348,29 @@ MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const 
  * particles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
+/* ---- all-FP64 simulation (precision studies) -------------------------------
+ * No reference counterpart as an API: it runs the reference substep
+ * (reset, p2g, grid_update, g2p, plasticity; mpm.rs:2476-2551) with FP64
+ * particle state, FP64 grid and the FP64 Jacobi SVD (tol 1e-14, 30 sweeps),
+ * one GPU thread per particle or node.  It exists to measure the error of
+ * the FP32 and FP32 + FP64-SVD modes against an all-FP64 run on the same
+ * device; it is not tuned.  Explicit time step only; no groups, graphs or
+ * ordering. */
+typedef struct mpm_sim64 mpm_sim64;
+MPM_API int mpm_sim64_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim64** out);
+MPM_API int mpm_sim64_destroy(mpm_sim64* sim);
+/* Particles at rest with F = I, C = 0, jp = 0 and the config's mass/volume. */
+MPM_API int mpm_sim64_set_particles(mpm_sim64* sim, const double* xyz, uint32_t n);
+MPM_API int mpm_sim64_set_materials(mpm_sim64* sim, const mpm_rheology* rows, uint32_t n_rows, const uint32_t* ids,
+                                    uint32_t n);
+MPM_API int mpm_sim64_step_n(mpm_sim64* sim, double dt, uint32_t substeps);
+/* Blocking; any of pos[3n], vel[3n], F[9n] (column-major) may be NULL. */
+MPM_API int mpm_sim64_read_state(mpm_sim64* sim, double* pos, double* vel, double* F, uint32_t cap,
+                                 uint32_t* count_out);
+/* Grid mass and momentum totals of the last P2G: out4 = {m, px, py, pz}. */
+MPM_API int mpm_sim64_grid_totals(mpm_sim64* sim, double* out4);
+MPM_API int mpm_sim64_read_status(mpm_sim64* sim, mpm_status_info* out);
+
 /* ---- serving ------------------------------------------------------------- */
 
 /* A request loop over a group: scenes are admitted as HBM budget and slots

@@ -27,7 +27,8 @@ from ._ffi import (MPM_ERR_BUSY, MPM_ERR_FAULT, MPM_ERR_GPU, MPM_ERR_INVALID, MP
 
 __all__ = [
     "Engine", "MpmConfig", "MpmRheology", "MpmTimeStep", "MpmSimulation", "PreparedMpmStep", "MpmCommandBatch",
-    "MpmActiveGridStats", "MpmGroup", "MpmServer", "MollaError", "SolverError", "GpuError", "radix_sort_pairs",
+    "MpmActiveGridStats", "MpmGroup", "MpmServer", "MpmSimulation64", "MollaError", "SolverError", "GpuError",
+    "radix_sort_pairs",
     "MAX_MPM_MATERIALS", "library_path",
 ]
 
@@ -500,6 +501,73 @@ def _rows_c(rows):
     for i, m in enumerate(rows):
         arr[i] = (m if isinstance(m, MpmRheology) else MpmRheology.from_dict(m)).to_c()
     return arr
+
+
+class MpmSimulation64:
+    """All-FP64 run of the reference substep on the GPU (FP64 state, grid and
+    Jacobi SVD), for precision studies of the FP32 and FP32 + FP64-SVD modes.
+    Positions are set and read in float64."""
+
+    def __init__(self, engine: Engine, cfg: MpmConfig):
+        self.engine = engine
+        self.cfg = cfg
+        h = C.c_void_p()
+        c = cfg.to_c()
+        _check(_ffi.lib().mpm_sim64_create(engine._h, C.byref(c), C.byref(h)))
+        self._h = h
+        self.particle_count = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _ffi.lib().mpm_sim64_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_particles(self, positions):
+        x = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        _check(_ffi.lib().mpm_sim64_set_particles(self._h, x.ctypes.data_as(_ffi.F64P), x.shape[0]))
+        self.particle_count = x.shape[0]
+
+    def set_materials(self, materials, particle_material):
+        rows = (_ffi.mpm_rheology * max(len(materials), 1))()
+        for i, m in enumerate(materials):
+            rows[i] = (m if isinstance(m, MpmRheology) else MpmRheology.from_dict(m)).to_c()
+        ids = np.ascontiguousarray(np.asarray(particle_material, dtype=np.uint32))
+        _check(_ffi.lib().mpm_sim64_set_materials(self._h, rows, len(materials), _up(ids), ids.shape[0]))
+
+    def step_n(self, dt: float, substeps: int):
+        _check(_ffi.lib().mpm_sim64_step_n(self._h, float(dt), substeps))
+
+    def read_state(self):
+        """(positions (n,3), velocities (n,3), F (n,9) column-major), float64."""
+        n = max(self.particle_count, 1)
+        pos = np.empty((n, 3), np.float64)
+        vel = np.empty((n, 3), np.float64)
+        F = np.empty((n, 9), np.float64)
+        cnt = C.c_uint32()
+        _check(_ffi.lib().mpm_sim64_read_state(self._h, pos.ctypes.data_as(_ffi.F64P), vel.ctypes.data_as(_ffi.F64P),
+                                               F.ctypes.data_as(_ffi.F64P), n, C.byref(cnt)))
+        k = cnt.value
+        return pos[:k], vel[:k], F[:k]
+
+    def read_positions(self):
+        return self.read_state()[0]
+
+    def grid_totals(self):
+        """(mass, momentum[3]) of the last P2G, FP64."""
+        out = np.zeros(4, np.float64)
+        _check(_ffi.lib().mpm_sim64_grid_totals(self._h, out.ctypes.data_as(_ffi.F64P)))
+        return float(out[0]), out[1:].copy()
+
+    def read_active_grid_status(self) -> MpmActiveGridStats:
+        s = _ffi.mpm_status_info()
+        _check(_ffi.lib().mpm_sim64_read_status(self._h, C.byref(s)))
+        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
 
 
 class MpmGroup:

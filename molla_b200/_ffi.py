@@ -161,6 +161,14 @@ SIGNATURES = {
     "mpm_group_autotune": (I, [P, U32, U32P, U32, F32P, U32P]),
     "mpm_autotune": (I, [P, C.c_float, U32, U32P, U32, F32P, U32P]),
     "mpm_group_tune": (I, [P, U32, U32]),
+    "mpm_sim64_create": (I, [P, C.POINTER(mpm_config), PP]),
+    "mpm_sim64_destroy": (I, [P]),
+    "mpm_sim64_set_particles": (I, [P, F64P, U32]),
+    "mpm_sim64_set_materials": (I, [P, C.POINTER(mpm_rheology), U32, U32P, U32]),
+    "mpm_sim64_step_n": (I, [P, C.c_double, U32]),
+    "mpm_sim64_read_state": (I, [P, F64P, F64P, F64P, U32, U32P]),
+    "mpm_sim64_grid_totals": (I, [P, F64P]),
+    "mpm_sim64_read_status": (I, [P, C.POINTER(mpm_status_info)]),
     "mpm_server_create": (I, [P, U64, U32, PP]),
     "mpm_server_destroy": (I, [P]),
     "mpm_server_submit": (I, [P, C.POINTER(mpm_config), C.POINTER(mpm_rheology), U32, F32P, U32P, U32, C.c_float,

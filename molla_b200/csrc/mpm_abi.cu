@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "mpm_runtime.cuh"
+#include "mpm_f64.cuh"
 
 using mpm::Error;
 
@@ -104,6 +105,53 @@ struct mpm_sim {
     group->sort_interval = interval;
   }
   void invalidate() { ++epoch; }
+};
+
+// All-FP64 simulation (precision studies): FP64 state and grid.
+struct mpm_sim64 {
+  mpm::Engine* eng = nullptr;
+  mpm_config cfg{};
+  mpm::Scene64 sc{};
+  uint32_t count = 0;
+  mpm::DevBuf<double> pos, vel, C, F, mass, vol, jp, gmass, gmom, gvel, totals;
+  mpm::DevBuf<uint32_t> mat, status;
+
+  mpm::State64 state() {
+    mpm::State64 st;
+    st.n = (int)count;
+    st.pos = pos.ptr;
+    st.vel = vel.ptr;
+    st.C = C.ptr;
+    st.F = F.ptr;
+    st.mass = mass.ptr;
+    st.vol = vol.ptr;
+    st.jp = jp.ptr;
+    st.mat = mat.ptr;
+    st.gmass = gmass.ptr;
+    st.gmom = gmom.ptr;
+    st.gvel = gvel.ptr;
+    st.status = status.ptr;
+    return st;
+  }
+  void set_rows(const mpm_rheology* rows, uint32_t n_rows) {
+    sc.n_mat = (int)n_rows;
+    for (uint32_t r = 0; r < n_rows; ++r) {
+      const mpm_rheology& m = rows[r];
+      const double e = m.youngs > 0.f ? (double)m.youngs : (double)cfg.youngs;
+      const double nu = m.youngs > 0.f ? (double)m.poisson : (double)cfg.poisson;
+      mpm::Mat64& d = sc.mat[r];
+      d.rheo = (int)m.kind;
+      d.mu = e / (2.0 * (1.0 + nu));
+      d.lam = e * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+      d.kappa = (3.0 * d.lam + 2.0 * d.mu) / (2.0 * d.mu);
+      d.dp_alpha = m.kind == MPM_RHEOLOGY_SAND ? (double)mpm_dp_alpha(m.friction_angle) : 0.0;
+      d.theta_c = m.kind == MPM_RHEOLOGY_SNOW ? (double)m.theta_c : 0.0;
+      d.theta_s = m.kind == MPM_RHEOLOGY_SNOW ? (double)m.theta_s : 0.0;
+      d.hardening = m.kind == MPM_RHEOLOGY_SNOW ? (double)m.hardening : 0.0;
+      d.vdamp = m.kind == MPM_RHEOLOGY_VISCOUS ? (double)m.velocity_damping : 0.0;
+      d.adamp = m.kind == MPM_RHEOLOGY_VISCOUS ? (double)m.affine_damping : 0.0;
+    }
+  }
 };
 
 struct mpm_prepared {
@@ -1084,6 +1132,145 @@ int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float*
       REQUIRE(cap >= t.n, MPM_ERR_INVALID, "output capacity below the particle count");
       std::memcpy(positions_out, t.result.data(), 12 * (size_t)t.n);
     }
+  });
+}
+
+int mpm_sim64_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim64** out) {
+  return guard([&] {
+    REQUIRE(engine && engine->e && cfg && out, MPM_ERR_INVALID, "null argument");
+    validate_config(*cfg);
+    engine->e->check();
+    auto s = std::make_unique<mpm_sim64>();
+    s->eng = engine->e.get();
+    s->cfg = *cfg;
+    mpm::Scene64& sc = s->sc;
+    sc.n = (int)cfg->grid_size;
+    sc.dx = (double)cfg->cell_size;
+    sc.inv_dx = (double)(1.0f / cfg->cell_size);  // f32 1/dx from the host, as the reference (mpm.rs:2389)
+    for (int a = 0; a < 3; ++a) {
+      sc.o[a] = (double)cfg->grid_origin[a];
+      sc.win[a] = cfg->grid_window_cells[a];
+    }
+    sc.gy = (double)cfg->gravity_y;
+    sc.friction = (double)cfg->boundary_friction;
+    sc.pad = cfg->boundary_pad ? (int)cfg->boundary_pad : 2;
+    sc.sticky = cfg->walls == MPM_WALLS_STICKY ? 1 : 0;
+    for (int a = 0; a < 3; ++a) {
+      sc.lo[a] = sc.o[a] + (double)(sc.win[a] + sc.pad) * sc.dx;
+      sc.hi[a] = sc.o[a] + (double)(sc.win[a] + (sc.n - sc.pad - 1)) * sc.dx;
+    }
+    sc.tol = 1.0e-14;
+    sc.sweeps = 30;
+    s->set_rows(&cfg->rheology, 1);
+    const size_t n3 = (size_t)sc.n * sc.n * sc.n;
+    s->gmass.alloc(n3);
+    s->gmom.alloc(3 * n3);
+    s->gvel.alloc(3 * n3);
+    s->totals.alloc(4);
+    s->status.alloc(4);
+    MPM_CK(cudaMemsetAsync(s->status.ptr, 0, 16, s->eng->stream));
+    MPM_CK(cudaMemsetAsync(s->gmass.ptr, 0, n3 * 8, s->eng->stream));
+    MPM_CK(cudaMemsetAsync(s->gmom.ptr, 0, 3 * n3 * 8, s->eng->stream));
+    *out = s.release();
+  });
+}
+
+int mpm_sim64_destroy(mpm_sim64* sim) {
+  return guard([&] { delete sim; });
+}
+
+int mpm_sim64_set_particles(mpm_sim64* sim, const double* xyz, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim && (xyz || n == 0), MPM_ERR_INVALID, "null argument");
+    REQUIRE(n <= sim->cfg.max_particles || sim->cfg.max_particles == 0, MPM_ERR_INVALID,
+            "particle count exceeds max_particles");
+    for (size_t i = 0; i < 3 * (size_t)n; ++i)
+      REQUIRE(std::isfinite(xyz[i]), MPM_ERR_INVALID, "MPM particle positions must be finite");
+    sim->count = n;
+    const size_t m = n ? n : 1;
+    sim->pos.alloc(3 * m);
+    sim->vel.alloc(3 * m);
+    sim->C.alloc(9 * m);
+    sim->F.alloc(9 * m);
+    sim->mass.alloc(m);
+    sim->vol.alloc(m);
+    sim->jp.alloc(m);
+    sim->mat.alloc(m);
+    std::vector<double> F(9 * m, 0.0), mass(m, (double)sim->cfg.particle_mass), vol(m, (double)sim->cfg.particle_volume);
+    for (size_t i = 0; i < m; ++i) F[9 * i] = F[9 * i + 4] = F[9 * i + 8] = 1.0;
+    cudaStream_t st = sim->eng->stream;
+    if (n) MPM_CK(cudaMemcpyAsync(sim->pos.ptr, xyz, 3 * (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    MPM_CK(cudaMemsetAsync(sim->vel.ptr, 0, 3 * m * 8, st));
+    MPM_CK(cudaMemsetAsync(sim->C.ptr, 0, 9 * m * 8, st));
+    MPM_CK(cudaMemsetAsync(sim->jp.ptr, 0, m * 8, st));
+    MPM_CK(cudaMemsetAsync(sim->mat.ptr, 0, m * 4, st));
+    MPM_CK(cudaMemcpyAsync(sim->F.ptr, F.data(), F.size() * 8, cudaMemcpyHostToDevice, st));
+    MPM_CK(cudaMemcpyAsync(sim->mass.ptr, mass.data(), m * 8, cudaMemcpyHostToDevice, st));
+    MPM_CK(cudaMemcpyAsync(sim->vol.ptr, vol.data(), m * 8, cudaMemcpyHostToDevice, st));
+    MPM_CK(cudaMemsetAsync(sim->status.ptr, 0, 16, st));
+    MPM_CK(cudaStreamSynchronize(st));
+  });
+}
+
+int mpm_sim64_set_materials(mpm_sim64* sim, const mpm_rheology* rows, uint32_t n_rows, const uint32_t* ids,
+                            uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim && rows && n_rows >= 1 && n_rows <= 8, MPM_ERR_INVALID, "MPM materials need 1..8 rows");
+    REQUIRE(n == sim->count && (ids || n == 0), MPM_ERR_INVALID, "material ids must cover every particle");
+    for (uint32_t i = 0; i < n; ++i) REQUIRE(ids[i] < n_rows, MPM_ERR_INVALID, "material id out of range");
+    for (uint32_t r = 0; r < n_rows; ++r) REQUIRE(rows[r].kind <= MPM_RHEOLOGY_VISCOUS, MPM_ERR_INVALID, "unknown MPM rheology");
+    sim->set_rows(rows, n_rows);
+    if (n) {
+      MPM_CK(cudaMemcpyAsync(sim->mat.ptr, ids, (size_t)n * 4, cudaMemcpyHostToDevice, sim->eng->stream));
+      MPM_CK(cudaStreamSynchronize(sim->eng->stream));
+    }
+  });
+}
+
+int mpm_sim64_step_n(mpm_sim64* sim, double dt, uint32_t substeps) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(std::isfinite(dt) && dt > 0.0, MPM_ERR_INVALID, "MPM dt must be finite and > 0");
+    sim->eng->check();
+    sim->sc.dt = dt;
+    sim->sc.gy = (double)sim->cfg.gravity_y;
+    MPM_CK(mpm::launch_step64(sim->sc, sim->state(), substeps, sim->eng->stream));
+    sim->eng->launches += (uint64_t)substeps * 4;
+  });
+}
+
+int mpm_sim64_read_state(mpm_sim64* sim, double* pos, double* vel, double* F, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    const uint32_t n = std::min(cap, sim->count);
+    cudaStream_t st = sim->eng->stream;
+    if (pos && n) MPM_CK(cudaMemcpyAsync(pos, sim->pos.ptr, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    if (vel && n) MPM_CK(cudaMemcpyAsync(vel, sim->vel.ptr, 3 * (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    if (F && n) MPM_CK(cudaMemcpyAsync(F, sim->F.ptr, 9 * (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    MPM_CK(cudaStreamSynchronize(st));
+    if (count_out) *count_out = n;
+  });
+}
+
+int mpm_sim64_grid_totals(mpm_sim64* sim, double* out4) {
+  return guard([&] {
+    REQUIRE(sim && out4, MPM_ERR_INVALID, "null argument");
+    MPM_CK(mpm::launch_totals64(sim->sc, sim->state(), sim->totals.ptr, sim->eng->stream));
+    MPM_CK(cudaMemcpyAsync(out4, sim->totals.ptr, 32, cudaMemcpyDeviceToHost, sim->eng->stream));
+    MPM_CK(cudaStreamSynchronize(sim->eng->stream));
+  });
+}
+
+int mpm_sim64_read_status(mpm_sim64* sim, mpm_status_info* out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    uint32_t w[4];
+    MPM_CK(cudaMemcpyAsync(w, sim->status.ptr, 16, cudaMemcpyDeviceToHost, sim->eng->stream));
+    MPM_CK(cudaStreamSynchronize(sim->eng->stream));
+    out->numerical_fault = (w[0] & 2u) ? 1u : 0u;
+    out->completed_substeps = w[1];
+    out->fault_bits = w[0];
+    out->reserved = 0;
   });
 }
 

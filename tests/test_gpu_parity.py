@@ -310,6 +310,32 @@ def test_cube_positions_vs_fp64_oracle(engine):
     assert rel.max() < 1e-4, rel.max()
 
 
+@pytest.mark.parametrize("preset", ["snow", "sand"])
+def test_all_fp64_gpu_matches_fp64_oracle(engine, preset):
+    """The all-FP64 GPU mode (precision studies) against the FP64 oracle:
+    both run the reference substep in FP64 with the FP64 Jacobi SVD (tol
+    1e-14, 30 sweeps); only the order of the grid atomics and FMA
+    contraction differ."""
+    cfg = getattr(m.MpmConfig, preset)()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 8, 7).astype(np.float64)
+    sim = m.MpmSimulation64(engine, cfg)
+    sim.set_particles(pts)
+    rows = [cfg.rheology]
+    sim.set_materials(rows, np.zeros(len(pts), np.uint32))
+    dt = float(np.float32(1.0 / 480))  # the oracle's scene holds dt in FP32
+    sim.step_n(dt, 40)
+    pos, vel, F = sim.read_state()
+    assert not sim.read_active_grid_status().numerical_fault
+    sc = O.make_scene(cfg, rows, dt, svd_tol=1e-14, svd_sweeps=30)
+    st = O.cast_state(O.init_state(pts, mass=cfg.particle_mass, volume=cfg.particle_volume), np.float64)
+    O.step(sc, st, 40, precision="f64")
+    assert np.abs(pos - st["pos"]).max() < 1e-9
+    assert np.abs(vel - st["vel"]).max() < 1e-7
+    assert np.abs(F - st["F"]).max() < 1e-8
+    mass, mom = sim.grid_totals()
+    assert abs(mass - cfg.particle_mass * len(pts)) / (cfg.particle_mass * len(pts)) < 1e-12
+
+
 # ---- fault latch (mpm_numerical_fault_tests.rs:19-100) -----------------------------
 
 @pytest.mark.parametrize("bits", [np.nan, np.inf, -np.inf])
