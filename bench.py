@@ -386,7 +386,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "substeps_per_call": args.e2e_substeps,
                     "h2d_bytes_per_step": int(pos_host.nbytes + ids_host.nbytes),
-                    "d2h_bytes_per_step": int(out.nbytes)},
+                    "d2h_bytes_per_step": int(out.nbytes), "call_s": [round(x, 4) for x in e2e_times]},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "wall_s": wall,

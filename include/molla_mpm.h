@@ -348,6 +348,33 @@ MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const 
  * particles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
+/* ---- soil checkpoints -------------------------------------------------------
+ * The reference's lossless particle checkpoint byte format
+ * (crates/molla-solvers/src/mpm_checkpoint.rs:71-92, :187-275): magic
+ * "MOLLSOIL", LE u32 version (1, or 2 with a grid window), BLAKE3 digest of
+ * the payload, configuration words, material table, then the particle
+ * streams (position 4, velocity 4, C 12, F 12, volume, mass, log-Jp,
+ * material id, tire compaction 4 words per particle).  Checkpoints written
+ * by molla load here and the other way round.  Tire compaction is written
+ * as zeros (no tire coupling on this path); per-material Young's modulus
+ * and Poisson ratio (an extension) cannot be archived. */
+/* checkpoint_soil_with (mpm_checkpoint.rs:388-434): with out == NULL only
+ * *size_out is set; otherwise the state is encoded into out[cap].  Blocking.
+ * A latched fault is rejected (MPM_ERR_FAULT). */
+MPM_API int mpm_checkpoint_save(mpm_sim* sim, uint8_t* out, size_t cap, size_t* size_out);
+/* from_bytes + restore_soil_with (mpm_checkpoint.rs:218-275, 436-542):
+ * decodes under the simulation's max_particles, rejects corrupt, non-finite,
+ * oversized, trailing or incompatible data (the physical configuration must
+ * match word for word, capacities aside) and replaces the particle state. */
+MPM_API int mpm_checkpoint_load(mpm_sim* sim, const uint8_t* bytes, size_t len);
+/* Decodes and validates a checkpoint without a GPU and re-encodes it into
+ * out (NULL: only *size_out / *count_out); the encoding is lossless, so the
+ * output equals the input for every valid checkpoint. */
+MPM_API int mpm_checkpoint_reencode(const uint8_t* bytes, size_t len, uint32_t max_particles, uint8_t* out,
+                                    size_t cap, size_t* size_out, uint32_t* count_out);
+/* BLAKE3 (unkeyed, 32-byte output) of data[len], the checkpoint digest. */
+MPM_API int mpm_blake3(const void* data, size_t len, uint8_t* out32);
+
 /* ---- all-FP64 simulation (precision studies) -------------------------------
  * No reference counterpart as an API: it runs the reference substep
  * (reset, p2g, grid_update, g2p, plasticity; mpm.rs:2476-2551) with FP64

@@ -28,7 +28,7 @@ from ._ffi import (MPM_ERR_BUSY, MPM_ERR_FAULT, MPM_ERR_GPU, MPM_ERR_INVALID, MP
 __all__ = [
     "Engine", "MpmConfig", "MpmRheology", "MpmTimeStep", "MpmSimulation", "PreparedMpmStep", "MpmCommandBatch",
     "MpmActiveGridStats", "MpmGroup", "MpmServer", "MpmSimulation64", "MollaError", "SolverError", "GpuError",
-    "radix_sort_pairs",
+    "radix_sort_pairs", "blake3", "checkpoint_reencode",
     "MAX_MPM_MATERIALS", "library_path",
 ]
 
@@ -460,6 +460,24 @@ class MpmSimulation:
         _check(_ffi.lib().mpm_read_grid_mass_momentum(self._h, _fp(m), _fp(p), n3))
         return m, p
 
+    def checkpoint_soil(self) -> bytes:
+        """checkpoint_soil_with (mpm_checkpoint.rs:388-434): the particle state
+        in molla's versioned soil-checkpoint bytes (BLAKE3 digest)."""
+        size = C.c_size_t()
+        _check(_ffi.lib().mpm_checkpoint_save(self._h, None, 0, C.byref(size)))
+        out = (C.c_ubyte * max(size.value, 1))()
+        _check(_ffi.lib().mpm_checkpoint_save(self._h, out, size.value, C.byref(size)))
+        return bytes(out)[: size.value]
+
+    def restore_soil(self, data: bytes):
+        """from_bytes + restore_soil_with (mpm_checkpoint.rs:218-275, 436-542)."""
+        raw = bytes(data)
+        _check(_ffi.lib().mpm_checkpoint_load(self._h, raw, len(raw)))
+        words = np.frombuffer(raw[44:], dtype="<u4")
+        off = (3 if int.from_bytes(raw[8:12], "little") == 2 else 0) + 21
+        rows = int(words[off])
+        self.particle_count = int(words[off + 1 + 4 * rows])
+
     def conservation_totals(self) -> np.ndarray:
         out = np.zeros(8, np.float64)
         _check(_ffi.lib().mpm_conservation_totals(self._h, out.ctypes.data_as(_ffi.F64P)))
@@ -501,6 +519,27 @@ def _rows_c(rows):
     for i, m in enumerate(rows):
         arr[i] = (m if isinstance(m, MpmRheology) else MpmRheology.from_dict(m)).to_c()
     return arr
+
+
+def blake3(data: bytes) -> bytes:
+    """BLAKE3 (unkeyed, 32 bytes) of data: the soil-checkpoint digest."""
+    buf = (C.c_ubyte * 32)()
+    raw = bytes(data)
+    _check(_ffi.lib().mpm_blake3(raw, len(raw), buf))
+    return bytes(buf)
+
+
+def checkpoint_reencode(data: bytes, max_particles: int):
+    """Decodes and validates a soil checkpoint (no GPU) and encodes it again;
+    returns (bytes, particle count).  Raises SolverError on invalid data."""
+    raw = bytes(data)
+    size = C.c_size_t()
+    count = C.c_uint32()
+    _check(_ffi.lib().mpm_checkpoint_reencode(raw, len(raw), max_particles, None, 0, C.byref(size), C.byref(count)))
+    out = (C.c_ubyte * max(size.value, 1))()
+    _check(_ffi.lib().mpm_checkpoint_reencode(raw, len(raw), max_particles, out, size.value, C.byref(size),
+                                              C.byref(count)))
+    return bytes(out)[: size.value], int(count.value)
 
 
 class MpmSimulation64:

@@ -161,6 +161,10 @@ SIGNATURES = {
     "mpm_group_autotune": (I, [P, U32, U32P, U32, F32P, U32P]),
     "mpm_autotune": (I, [P, C.c_float, U32, U32P, U32, F32P, U32P]),
     "mpm_group_tune": (I, [P, U32, U32]),
+    "mpm_checkpoint_save": (I, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "mpm_checkpoint_load": (I, [P, P, C.c_size_t]),
+    "mpm_checkpoint_reencode": (I, [P, C.c_size_t, U32, P, C.c_size_t, C.POINTER(C.c_size_t), U32P]),
+    "mpm_blake3": (I, [P, C.c_size_t, P]),
     "mpm_sim64_create": (I, [P, C.POINTER(mpm_config), PP]),
     "mpm_sim64_destroy": (I, [P]),
     "mpm_sim64_set_particles": (I, [P, F64P, U32]),

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "mpm_runtime.cuh"
+#include "mpm_checkpoint.cuh"
 #include "mpm_f64.cuh"
 
 using mpm::Error;
@@ -1132,6 +1133,168 @@ int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float*
       REQUIRE(cap >= t.n, MPM_ERR_INVALID, "output capacity below the particle count");
       std::memcpy(positions_out, t.result.data(), 12 * (size_t)t.n);
     }
+  });
+}
+
+int mpm_blake3(const void* data, size_t len, uint8_t* out32) {
+  return guard([&] {
+    REQUIRE((data || len == 0) && out32, MPM_ERR_INVALID, "null argument");
+    mpm::Blake3 h;
+    h.update(static_cast<const uint8_t*>(data), len);
+    h.finalize(out32);
+  });
+}
+
+int mpm_checkpoint_reencode(const uint8_t* bytes, size_t len, uint32_t max_particles, uint8_t* out, size_t cap,
+                            size_t* size_out, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(bytes || len == 0, MPM_ERR_INVALID, "null argument");
+    const mpm::SoilCheckpoint k = mpm::decode_checkpoint(bytes, len, max_particles);
+    if (count_out) *count_out = k.count;
+    if (!out) {
+      if (size_out) *size_out = mpm::checkpoint_bytes(k.window[0] || k.window[1] || k.window[2],
+                                                      (uint32_t)k.materials.size(), k.count);
+      return;
+    }
+    const std::vector<uint8_t> enc = mpm::encode_checkpoint(k);
+    if (size_out) *size_out = enc.size();
+    REQUIRE(cap >= enc.size(), MPM_ERR_INVALID, "checkpoint buffer too small");
+    std::memcpy(out, enc.data(), enc.size());
+  });
+}
+
+int mpm_checkpoint_save(mpm_sim* sim, uint8_t* out, size_t cap, size_t* size_out) {
+  return guard([&] {
+    REQUIRE(sim && size_out, MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    const mpm_config& c = sim->cfg;
+    const bool lattice = c.grid_window_cells[0] || c.grid_window_cells[1] || c.grid_window_cells[2];
+    const size_t need = mpm::checkpoint_bytes(lattice, (uint32_t)sim->rows.size(), sim->count);
+    *size_out = need;
+    if (!out) return;
+    REQUIRE(cap >= need, MPM_ERR_INVALID, "checkpoint buffer too small");
+    REQUIRE(c.time_step == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED, "only explicit simulations are archived");
+    bool ext = c.rheology.youngs != 0.f || c.rheology.poisson != 0.f;
+    for (const mpm_rheology& r : sim->rows) ext = ext || r.youngs != 0.f || r.poisson != 0.f;
+    REQUIRE(!ext, MPM_ERR_UNSUPPORTED,
+            "MPM soil checkpoint: the format holds one Young's modulus and Poisson ratio; per-material values "
+            "cannot be archived");
+    if (sim->group && sim->sid != 0xffffffffu) {
+      mpm_status_info st{};
+      sim->group->status(sim->sid, &st, sim->eng->stream);
+      REQUIRE(st.fault_bits == 0, MPM_ERR_FAULT,
+              "MPM soil checkpoint: latched grid fault; incomplete state cannot be archived");
+    }
+    mpm::SoilCheckpoint k;
+    k.cfg = c;
+    for (int a = 0; a < 3; ++a) k.window[a] = c.grid_window_cells[a];
+    k.materials = sim->rows;
+    k.count = sim->count;
+    const size_t n = sim->count;
+    k.words.assign(n * mpm::kCheckpointWordsPerParticle, 0u);
+    if (n) {
+      std::vector<float> x(3 * n), v(3 * n), C(9 * n), F(9 * n), vol(n), mass(n), jp(n);
+      cudaStream_t s = sim->eng->stream;
+      sim->group->read_rows(sim->sid, mpm::PX, 3, x.data(), s);
+      sim->group->read_rows(sim->sid, mpm::VX, 3, v.data(), s);
+      sim->group->read_rows(sim->sid, mpm::C0, 9, C.data(), s);
+      sim->group->read_rows(sim->sid, mpm::F0, 9, F.data(), s);
+      sim->group->read_rows(sim->sid, mpm::VOL, 1, vol.data(), s);
+      sim->group->read_rows(sim->sid, mpm::MASS, 1, mass.data(), s);
+      sim->group->read_rows(sim->sid, mpm::JP, 1, jp.data(), s);
+      auto bits = [](float f) {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        return u;
+      };
+      uint32_t* w = k.words.data();
+      for (size_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) w[4 * i + a] = bits(x[3 * i + a]);
+      w += 4 * n;
+      for (size_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) w[4 * i + a] = bits(v[3 * i + a]);
+      w += 4 * n;
+      for (size_t i = 0; i < n; ++i)
+        for (int col = 0; col < 3; ++col)
+          for (int r = 0; r < 3; ++r) w[12 * i + 4 * col + r] = bits(C[9 * i + 3 * col + r]);
+      w += 12 * n;
+      for (size_t i = 0; i < n; ++i)
+        for (int col = 0; col < 3; ++col)
+          for (int r = 0; r < 3; ++r) w[12 * i + 4 * col + r] = bits(F[9 * i + 3 * col + r]);
+      w += 12 * n;
+      for (size_t i = 0; i < n; ++i) w[i] = bits(vol[i]);
+      w += n;
+      for (size_t i = 0; i < n; ++i) w[i] = bits(mass[i]);
+      w += n;
+      for (size_t i = 0; i < n; ++i) w[i] = bits(jp[i]);
+      w += n;
+      for (size_t i = 0; i < n; ++i) w[i] = sim->ids.size() == n ? sim->ids[i] : 0u;
+      // tire compaction (4 words per particle): no tire coupling here, zeros
+    }
+    mpm::validate_checkpoint(k);
+    const std::vector<uint8_t> enc = mpm::encode_checkpoint(k);
+    std::memcpy(out, enc.data(), enc.size());
+    *size_out = enc.size();
+  });
+}
+
+namespace {
+void must(int rc) {
+  if (rc != MPM_OK) throw mpm::Error(rc, g_last_error);
+}
+}  // namespace
+
+int mpm_checkpoint_load(mpm_sim* sim, const uint8_t* bytes, size_t len) {
+  return guard([&] {
+    REQUIRE(sim && (bytes || len == 0), MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    const mpm::SoilCheckpoint k = mpm::decode_checkpoint(bytes, len, sim->cfg.max_particles);
+    const int32_t* w0 = sim->cfg.grid_window_cells;
+    REQUIRE(mpm::checkpoint_config_compatible(k.cfg, sim->cfg) && k.window[0] == w0[0] && k.window[1] == w0[1] &&
+                k.window[2] == w0[2] && k.count <= sim->cfg.max_particles,
+            MPM_ERR_INVALID, "MPM soil checkpoint: incompatible configuration or capacity");
+    const size_t n = k.count;
+    std::vector<float> x(3 * n), v(3 * n), C(9 * n), F(9 * n), vol(n), mass(n), jp(n);
+    std::vector<uint32_t> ids(n);
+    auto flt = [](uint32_t u) {
+      float f;
+      std::memcpy(&f, &u, 4);
+      return f;
+    };
+    const uint32_t* w = k.words.data();
+    for (size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) x[3 * i + a] = flt(w[4 * i + a]);
+    w += 4 * n;
+    for (size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) v[3 * i + a] = flt(w[4 * i + a]);
+    w += 4 * n;
+    for (size_t i = 0; i < n; ++i)
+      for (int col = 0; col < 3; ++col)
+        for (int r = 0; r < 3; ++r) C[9 * i + 3 * col + r] = flt(w[12 * i + 4 * col + r]);
+    w += 12 * n;
+    for (size_t i = 0; i < n; ++i)
+      for (int col = 0; col < 3; ++col)
+        for (int r = 0; r < 3; ++r) F[9 * i + 3 * col + r] = flt(w[12 * i + 4 * col + r]);
+    w += 12 * n;
+    for (size_t i = 0; i < n; ++i) vol[i] = flt(w[i]);
+    w += n;
+    for (size_t i = 0; i < n; ++i) mass[i] = flt(w[i]);
+    w += n;
+    for (size_t i = 0; i < n; ++i) jp[i] = flt(w[i]);
+    w += n;
+    for (size_t i = 0; i < n; ++i) ids[i] = w[i];
+    const uint32_t un = (uint32_t)n;
+    must(mpm_set_particles(sim, n ? x.data() : nullptr, n ? v.data() : nullptr, un));
+    if (!k.materials.empty())
+      must(mpm_set_materials(sim, k.materials.data(), (uint32_t)k.materials.size(), ids.data(), un));
+    else
+      must(mpm_set_materials(sim, &sim->cfg.rheology, 1, ids.data(), un));
+    if (n) {
+      must(mpm_set_particle_mass_volume(sim, mass.data(), vol.data(), un));
+      must(mpm_write_particle_state(sim, C.data(), F.data(), jp.data(), un));
+    }
+    if (k.materials.empty()) sim->rows.clear();
+    sim->invalidate();
   });
 }
 

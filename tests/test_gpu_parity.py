@@ -336,6 +336,64 @@ def test_all_fp64_gpu_matches_fp64_oracle(engine, preset):
     assert abs(mass - cfg.particle_mass * len(pts)) / (cfg.particle_mass * len(pts)) < 1e-12
 
 
+def test_soil_checkpoint_round_trip_and_continuation(engine):
+    """archive_drop_reload_preserves_all_history (mpm_checkpoint_tests.rs:176-257):
+    a checkpoint of an evolved state restores bit for bit into a fresh
+    simulation, re-encodes identically, and both continue alike."""
+    cfg = m.MpmConfig.sand()
+    cfg.max_particles = 4096
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 10, 5)
+    rows = [m.MpmRheology.Sand(0.5), m.MpmRheology.Snow(), m.MpmRheology.Viscous(3.0, 5.0)]
+    ids = (np.arange(len(pts)) % 3).astype(np.uint32)
+    a = m.MpmSimulation.new(engine, cfg)
+    a.set_particles(pts)
+    a.set_materials(rows, ids)
+    a.step_n(1.0 / 480, 20)
+    data = a.checkpoint_soil()
+    assert len(data) == 44 + 4 * (21 + 1 + 12 + 1) + 160 * len(pts)
+    assert m.checkpoint_reencode(data, cfg.max_particles) == (data, len(pts))
+    b = m.MpmSimulation.new(engine, cfg)
+    b.restore_soil(data)
+    for f in ("read_positions", "read_velocities"):
+        assert np.array_equal(getattr(a, f)(), getattr(b, f)())
+    sa, sb = a.read_particle_state(), b.read_particle_state()
+    for x, y in zip(sa, sb):
+        assert np.array_equal(x, y)
+    assert b.checkpoint_soil() == data
+    a.step_n(1.0 / 480, 10)
+    b.step_n(1.0 / 480, 10)
+    assert np.abs(a.read_positions() - b.read_positions()).max() < 1e-5
+
+
+def test_soil_checkpoint_rejects_incompatible_or_faulted_state(engine):
+    cfg = m.MpmConfig.sand()
+    cfg.max_particles = 256
+    pts = scenes.fill_box_lcg([-0.1, 0.3, -0.1], [0.1, 0.5, 0.1], 4, 1)
+    a = m.MpmSimulation.new(engine, cfg)
+    a.set_particles(pts)
+    a.step_n(1.0 / 480, 2)
+    data = a.checkpoint_soil()
+    other = m.MpmConfig.sand()
+    other.max_particles = 256
+    other.youngs = cfg.youngs * 2
+    b = m.MpmSimulation.new(engine, other)
+    with pytest.raises(m.MollaError):
+        b.restore_soil(data)
+    small = m.MpmConfig.sand()
+    small.max_particles = len(pts) - 1
+    c = m.MpmSimulation.new(engine, small)
+    with pytest.raises(m.MollaError):
+        c.restore_soil(data)
+    # a latched numerical fault cannot be archived
+    pos = a.read_positions()
+    pos[0, 0] = np.nan
+    a.set_particles(pos)
+    a.step_n(1.0 / 480, 1)
+    assert a.read_active_grid_status().numerical_fault
+    with pytest.raises(m.MollaError):
+        a.checkpoint_soil()
+
+
 # ---- fault latch (mpm_numerical_fault_tests.rs:19-100) -----------------------------
 
 @pytest.mark.parametrize("bits", [np.nan, np.inf, -np.inf])
