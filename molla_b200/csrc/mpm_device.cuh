@@ -159,8 +159,11 @@ __device__ __forceinline__ T det3(const T* a) {
 // sigma_i are FP64.  Double division and square roots are replaced by
 // Newton-Raphson refinement of single-precision seeds (two steps each,
 // quadratic convergence from 2^-22 to below 2^-52).
+// U is held in FP32 in both forms: its consumers (the stress record and
+// the rebuilt F) are FP32, while sigma and V carry the form's precision.
 template <class T> struct SvdOut {
-  T u[9], s[3], v[9];
+  float u[9];
+  T s[3], v[9];
 };
 
 // Newton-Raphson reciprocal: y <- y (2 - x y), seeded from the correctly
@@ -292,7 +295,6 @@ __device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sw
     const T y = f[1] * v[3 * i] + f[4] * v[3 * i + 1] + f[7] * v[3 * i + 2];
     const T z = f[2] * v[3 * i] + f[5] * v[3 * i + 1] + f[8] * v[3 * i + 2];
     T s;
-    T inv;
     if constexpr (sizeof(T) == 4) {
       s = sqrtf(x * x + y * y + z * z);
     } else {
@@ -306,18 +308,18 @@ __device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sw
         o.u[3 * i + 1] = y / s;
         o.u[3 * i + 2] = z / s;
       } else {
-        inv = nr_rcp(s);
-        o.u[3 * i] = x * inv;
-        o.u[3 * i + 1] = y * inv;
-        o.u[3 * i + 2] = z * inv;
+        const float inv = 1.0f / (float)s;
+        o.u[3 * i] = (float)x * inv;
+        o.u[3 * i + 1] = (float)y * inv;
+        o.u[3 * i + 2] = (float)z * inv;
       }
     } else {
-      o.u[3 * i] = i == 0 ? T(1) : T(0);
-      o.u[3 * i + 1] = i == 1 ? T(1) : T(0);
-      o.u[3 * i + 2] = i == 2 ? T(1) : T(0);
+      o.u[3 * i] = i == 0 ? 1.0f : 0.0f;
+      o.u[3 * i + 1] = i == 1 ? 1.0f : 0.0f;
+      o.u[3 * i + 2] = i == 2 ? 1.0f : 0.0f;
     }
   }
-  if (det3(o.u) < T(0)) {
+  if (det3(o.u) < 0.0f) {
     // flip the column of U with the smallest (signed) sigma
     const bool m1 = o.s[1] < o.s[0];
     const T s01 = m1 ? o.s[1] : o.s[0];
@@ -393,7 +395,7 @@ __device__ __forceinline__ void p2g_affine_principal(const SvdOut<double>& svd, 
   for (int i = 0; i < 3; ++i) tau[i] = k1 * (float)(scd[i] - 1.0) * (float)scd[i] + kv;
   float u[9];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) u[i] = (float)svd.u[i];
+  for (int i = 0; i < 9; ++i) u[i] = svd.u[i];
   const float k = -dt * vol * 4.0f * inv_dx * inv_dx;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -415,7 +417,7 @@ __device__ __forceinline__ void p2g_affine(const SvdOut<T>& svd, const MatDev& m
     float u[9], v[9], sc[3];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      u[i] = (float)svd.u[i];
+      u[i] = svd.u[i];
       v[i] = (float)svd.v[i];
     }
 #pragma unroll
@@ -466,7 +468,7 @@ __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev&
   if (!finitef(s[0]) || !finitef(s[1]) || !finitef(s[2])) return false;
 #pragma unroll
   for (int i = 0; i < 9; ++i)
-    if (!finitef((float)svd.u[i]) || !finitef((float)svd.v[i])) return false;
+    if (!finitef(svd.u[i]) || !finitef((float)svd.v[i])) return false;
   T ns[3] = {svd.s[0], svd.s[1], svd.s[2]};
   float dq = 0.0f;
   bool jp_replace = false;

@@ -35,6 +35,7 @@ namespace {
 
 struct SharedGather {
   float4 vel[kRegionNodes];
+  float fallback[kGatherThreads][13];  // per-thread result slot of gather_global
 };
 
 __device__ __forceinline__ int region_index(int lx, int ly, int lz) { return lx + kRsy * ly + kRsz * lz; }
@@ -58,11 +59,24 @@ __device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base
 // Gather for a particle whose stencil is not inside the staged 8^3 block
 // (it left its tile since the last regrouping): 27 global reads with the
 // reference's out-of-grid skip.  Kept out of line and rolled so that the
-// unrolled shared-memory path stays small.
-__device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int n, const int* base,
-                                           const float (*w)[3], const float (*d)[3], float* vs, float* G) {
-  for (int i = 0; i < 3; ++i) vs[i] = 0.f;
-  for (int i = 0; i < 9; ++i) G[i] = 0.f;
+// unrolled shared-memory path stays small; it takes scalars and writes
+// v (3) and G = sum w gv d^T (9) to the caller's shared-memory slot, so the
+// call needs no local memory.
+__device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int n, float xp0, float xp1, float xp2,
+                                           int wx, int wy, int wz, float dx, float* out) {
+  const float xp[3] = {xp0, xp1, xp2};
+  const int win[3] = {wx, wy, wz};
+  float w[3][3], d[3][3];
+  int base[3];
+  for (int a = 0; a < 3; ++a) {
+    const float bf = floorf(xp[a] - 0.5f);
+    base[a] = (int)bf - win[a];
+    const float fx = xp[a] - bf;
+    quad_weights(fx, w[a]);
+    for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * dx;
+  }
+  float acc[12];
+  for (int i = 0; i < 12; ++i) acc[i] = 0.f;
   for (int q = 0; q < 27; ++q) {
     const int i = q / 9, j = (q / 3) % 3, k = q % 3;
     const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
@@ -71,12 +85,13 @@ __device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int 
     const float wt = w[0][i] * w[1][j] * w[2][k];
     const float gv[3] = {wt * g.x, wt * g.y, wt * g.z};
     for (int r = 0; r < 3; ++r) {
-      vs[r] += gv[r];
-      G[r] += gv[r] * d[0][i];
-      G[3 + r] += gv[r] * d[1][j];
-      G[6 + r] += gv[r] * d[2][k];
+      acc[r] += gv[r];
+      acc[3 + r] += gv[r] * d[0][i];
+      acc[6 + r] += gv[r] * d[1][j];
+      acc[9 + r] += gv[r] * d[2][k];
     }
   }
+  for (int i = 0; i < 12; ++i) out[i] = acc[i];
 }
 
 // mbarrier + bulk-copy (TMA engine) helpers for the scatter's record stage.
@@ -257,7 +272,12 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
                 }
               }
             } else {
-              gather_global(p.vel + sc.grid_off, n, base, w, d, vs, G);
+              float* slot = s_gath.fallback[threadIdx.x];
+              gather_global(p.vel + sc.grid_off, n, xp[0], xp[1], xp[2], win[0], win[1], win[2], sc.dx, slot);
+#pragma unroll
+              for (int r = 0; r < 3; ++r) vs[r] = slot[r];
+#pragma unroll
+              for (int r = 0; r < 9; ++r) G[r] = slot[3 + r];
             }
             const float four_inv_dx2 = 4.0f * sc.inv_dx * sc.inv_dx;
 #pragma unroll
@@ -319,7 +339,16 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
                   // the return mapping left every singular value unchanged.
                   SR Fr[9];
                   const bool rebuild = sizeof(SR) == 4 || changed;
-                  if (rebuild) sandwich(svd.u, svd.s, svd.v, Fr);
+                  if (rebuild) {
+                    // F = U diag(s) V^T in the form's precision (U is FP32)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                      for (int r = 0; r < 3; ++r)
+                        Fr[3 * c + r] = ((SR)svd.u[r] * svd.s[0]) * svd.v[c] +
+                                        ((SR)svd.u[3 + r] * svd.s[1]) * svd.v[3 + c] +
+                                        ((SR)svd.u[6 + r] * svd.s[2]) * svd.v[6 + c];
+                  }
                   bool fin4 = true;
 #pragma unroll
                   for (int i = 0; i < 9; ++i) fin4 = fin4 && (!rebuild || finitef((float)Fr[i]));
