@@ -74,9 +74,10 @@ typedef struct mpm_rheology {
   float poisson;
 } mpm_rheology;
 
-/* Time-step selector, MpmTimeStep (mpm.rs:372-398). Only the explicit step is
- * built; the semi-implicit Jacobi relaxation is rejected with
- * MPM_ERR_UNSUPPORTED. */
+/* Time-step selector, MpmTimeStep (mpm.rs:372-398).  IMPLICIT adds
+ * `jacobi_iters` semi-implicit Jacobi sweeps on the grid velocity after the
+ * grid update (mpm_implicit_apply, mpm.wgsl:1060-1164); rigid-body coupling
+ * is not part of this path. */
 typedef enum mpm_time_step_kind { MPM_TIME_STEP_EXPLICIT = 0, MPM_TIME_STEP_IMPLICIT = 1 } mpm_time_step_kind;
 
 /* Precision of the per-particle SVD/polar decomposition.  The particle and

@@ -54,8 +54,7 @@ void validate_config(const mpm_config& c) {
   REQUIRE(std::isfinite(c.cell_size) && c.cell_size > 0.f && finite3(c.grid_origin), MPM_ERR_INVALID,
           "MPM grid exceeds device capacity or has invalid spacing/origin");
   REQUIRE(c.rheology.kind <= MPM_RHEOLOGY_VISCOUS, MPM_ERR_INVALID, "unknown MPM rheology");
-  REQUIRE(c.time_step == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED,
-          "semi-implicit Jacobi MPM is not part of this build; use the explicit time step");
+  REQUIRE(c.time_step <= MPM_TIME_STEP_IMPLICIT, MPM_ERR_INVALID, "unknown MPM time step");
   REQUIRE(c.walls <= MPM_WALLS_STICKY, MPM_ERR_INVALID, "unknown MPM wall model");
   REQUIRE(c.svd_precision <= MPM_SVD_FP64, MPM_ERR_INVALID, "unknown MPM SVD precision");
   REQUIRE(c.boundary_pad == 0 || c.boundary_pad * 2 < c.grid_size, MPM_ERR_INVALID, "MPM boundary pad too wide");
@@ -460,10 +459,10 @@ int mpm_set_material(mpm_sim* sim, float youngs, float friction_angle) {
 int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters) {
   return guard([&] {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
-    REQUIRE(kind == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED,
-            "semi-implicit Jacobi MPM is not part of this build; use the explicit time step");
+    REQUIRE(kind <= MPM_TIME_STEP_IMPLICIT, MPM_ERR_INVALID, "unknown MPM time step");
     sim->cfg.time_step = kind;
-    sim->cfg.jacobi_iters = jacobi_iters;
+    sim->cfg.jacobi_iters = kind == MPM_TIME_STEP_IMPLICIT ? jacobi_iters : 0u;
+    if (sim->sid != 0xffffffffu) sim->group->set_scene_cfg(sim->sid, sim->cfg);
     sim->invalidate();
   });
 }
@@ -1173,7 +1172,6 @@ int mpm_checkpoint_save(mpm_sim* sim, uint8_t* out, size_t cap, size_t* size_out
     *size_out = need;
     if (!out) return;
     REQUIRE(cap >= need, MPM_ERR_INVALID, "checkpoint buffer too small");
-    REQUIRE(c.time_step == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED, "only explicit simulations are archived");
     bool ext = c.rheology.youngs != 0.f || c.rheology.poisson != 0.f;
     for (const mpm_rheology& r : sim->rows) ext = ext || r.youngs != 0.f || r.poisson != 0.f;
     REQUIRE(!ext, MPM_ERR_UNSUPPORTED,
@@ -1302,6 +1300,8 @@ int mpm_sim64_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim64** out)
   return guard([&] {
     REQUIRE(engine && engine->e && cfg && out, MPM_ERR_INVALID, "null argument");
     validate_config(*cfg);
+    REQUIRE(cfg->time_step == MPM_TIME_STEP_EXPLICIT, MPM_ERR_UNSUPPORTED,
+            "the all-FP64 simulation runs the explicit step only");
     engine->e->check();
     auto s = std::make_unique<mpm_sim64>();
     s->eng = engine->e.get();

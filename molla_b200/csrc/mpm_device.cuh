@@ -76,6 +76,8 @@ struct SceneDev {
   uint32_t id_base;    // first identity of this scene
   uint32_t n_particles;
   uint32_t live;       // 0 once the scene was removed (its particles leave at the next regroup)
+  uint32_t jacobi_iters;  // semi-implicit sweeps per substep (MpmTimeStep::Implicit), 0 explicit
+  float youngs;           // the configuration's Young's modulus (implicit stiffness estimate)
   MatDev mat[kMaxMaterials];
 };
 

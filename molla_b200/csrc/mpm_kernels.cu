@@ -91,6 +91,80 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
   p.vel[g] = make_float4(v[0], v[1], v[2], m);
 }
 
+// One semi-implicit Jacobi sweep on the grid velocity (mpm_implicit_apply,
+// mpm.wgsl:1060-1164), src -> dst, over the blocks the last scatter touched:
+// a node with mass m blends its velocity with the mean velocity of its
+// face neighbours that carry mass, v = (m v + a v_avg) / (m + a), with
+// a = dt^2 m c^2 / dx^2 and c^2 = E / 1500 (the reference's wave-speed
+// stiffness estimate); massless nodes and scenes whose sweeps are done copy.
+__global__ void __launch_bounds__(kCellThreads) k_grid_jacobi(PoolDev p, const uint32_t* __restrict__ block_scene,
+                                                              uint64_t total_cells, int acc_in,
+                                                              const float4* __restrict__ src, float4* __restrict__ dst,
+                                                              uint32_t sweep) {
+  const uint64_t blk = blockIdx.x;
+  if (blk * kCellThreads >= total_cells) return;
+  const uint32_t sid = block_scene[blk];
+  if (sid == 0xffffffffu || !p.touched[acc_in][blk]) return;
+  const uint64_t g = blk * kCellThreads + threadIdx.x;
+  const SceneDev& sc = p.scenes[sid];
+  const uint64_t local64 = g - sc.grid_off;
+  const uint32_t n = sc.n;
+  if (local64 >= (uint64_t)n * n * n) return;
+  const float4 cur = src[g];
+  const float m = p.acc[acc_in][g].x;
+  if (sweep >= sc.jacobi_iters || m <= 1.0e-9f || !(m == m)) {
+    dst[g] = cur;
+    return;
+  }
+  const uint32_t local = (uint32_t)local64;
+  const uint32_t q = local / n;
+  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
+  const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  float ax = 0.f, ay = 0.f, az = 0.f, count = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int nx = ix + off[k][0], ny = iy + off[k][1], nz = iz + off[k][2];
+    if ((unsigned)nx >= n || (unsigned)ny >= n || (unsigned)nz >= n) continue;
+    const uint64_t ng = sc.grid_off + (uint64_t)nx + (uint64_t)n * ((uint64_t)ny + (uint64_t)n * (uint64_t)nz);
+    const float nm = p.acc[acc_in][ng].x;
+    if (nm <= 1.0e-9f || !(nm == nm)) continue;
+    const float4 nv = src[ng];
+    ax = ax + nv.x;
+    ay = ay + nv.y;
+    az = az + nv.z;
+    count = count + 1.0f;
+  }
+  if (count > 0.f) {
+    ax = ax / count;
+    ay = ay / count;
+    az = az / count;
+  } else {
+    ax = cur.x;
+    ay = cur.y;
+    az = cur.z;
+  }
+  const float c2 = sc.youngs / 1500.0f;
+  const float alpha = sc.dt * sc.dt * m * c2 * sc.inv_dx * sc.inv_dx;
+  const float denom = m + alpha;
+  const float vx = (m * cur.x + alpha * ax) / denom, vy = (m * cur.y + alpha * ay) / denom,
+              vz = (m * cur.z + alpha * az) / denom;
+  const bool nan = !(vx == vx) || !(vy == vy) || !(vz == vz);
+  dst[g] = nan ? make_float4(cur.x, cur.y, cur.z, m) : make_float4(vx, vy, vz, m);
+}
+
+// dst <- src over the touched blocks (the last Jacobi sweep's result back into
+// the velocity buffer the gather reads).
+__global__ void __launch_bounds__(kCellThreads) k_vel_copy(const uint8_t* __restrict__ touched,
+                                                           const uint32_t* __restrict__ block_scene,
+                                                           uint64_t total_cells, const float4* __restrict__ src,
+                                                           float4* __restrict__ dst) {
+  const uint64_t blk = blockIdx.x;
+  if (blk * kCellThreads >= total_cells) return;
+  if (block_scene[blk] == 0xffffffffu || !touched[blk]) return;
+  const uint64_t g = blk * kCellThreads + threadIdx.x;
+  dst[g] = src[g];
+}
+
 // Sort keys of the live slots (tile_keys, mpm_particle_order.wgsl:11-25)
 // written at the particle's identity.
 __global__ void k_keys(PoolDev p, uint32_t n_slots) {
@@ -338,6 +412,22 @@ cudaError_t launch_grid_update(const PoolDev& p, const uint32_t* block_scene, ui
   const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
   if (blocks == 0) return cudaSuccess;
   k_grid_update<<<(unsigned)blocks, kCellThreads, 0, st>>>(p, block_scene, total_cells, acc_in, count_substep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_jacobi(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
+                               const float4* src, float4* dst, uint32_t sweep, cudaStream_t st) {
+  const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
+  if (blocks == 0) return cudaSuccess;
+  k_grid_jacobi<<<(unsigned)blocks, kCellThreads, 0, st>>>(p, block_scene, total_cells, acc_in, src, dst, sweep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene, uint64_t total_cells,
+                            const float4* src, float4* dst, cudaStream_t st) {
+  const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
+  if (blocks == 0) return cudaSuccess;
+  k_vel_copy<<<(unsigned)blocks, kCellThreads, 0, st>>>(touched, block_scene, total_cells, src, dst);
   return cudaGetLastError();
 }
 

@@ -187,6 +187,8 @@ SceneDev make_scene_dev(const mpm_config& cfg, const std::vector<mpm_rheology>& 
   }
   d.n_mat = (uint32_t)rows.size();
   d.live = 1;
+  d.jacobi_iters = cfg.time_step == MPM_TIME_STEP_IMPLICIT ? cfg.jacobi_iters : 0u;
+  d.youngs = cfg.youngs;
   for (size_t i = 0; i < rows.size() && i < (size_t)kMaxMaterials; ++i) {
     const mpm_rheology& r = rows[i];
     MatDev& m = d.mat[i];
@@ -362,6 +364,7 @@ void Group::rebuild_layout() {
   scenes_dirty = true;
   need_regroup = true;
   invalidate_graphs();
+  if (max_jacobi_iters() && vel2.count < cell_cap) vel2.alloc(cell_cap);
 }
 
 void Group::sync_scenes(cudaStream_t st) {
@@ -493,6 +496,7 @@ void Group::set_scene_dt(uint32_t sid, float dt) {
   d.n_particles = s.n;
   scenes_h[sid] = d;
   scenes_dirty = true;
+  if (d.jacobi_iters && vel2.count < cell_cap) vel2.alloc(cell_cap);
 }
 
 void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) {
@@ -506,6 +510,7 @@ void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) 
 void Group::set_scene_cfg(uint32_t sid, const mpm_config& cfg) {
   SceneHost& s = scenes.at(sid);
   s.cfg = cfg;
+  invalidate_graphs();
   const float dt = s.dt;
   s.dt = -1.f;
   set_scene_dt(sid, dt);
@@ -707,19 +712,43 @@ void Group::set_deterministic(bool on) {
 // update, the gather (which also records B for the next substep unless it is
 // the last) and the next scatter.  Regrouping happens after a scatter, every
 // `sort_interval` substeps.
+uint32_t Group::max_jacobi_iters() const {
+  uint32_t mj = 0;
+  for (size_t i = 0; i < scenes.size(); ++i)
+    if (scenes[i].live) mj = std::max(mj, scenes_h[i].jacobi_iters);
+  return mj;
+}
+
+void Group::grid_pass(int a, uint32_t max_jacobi, cudaStream_t st) {
+  const uint64_t total_cells = cells.high_water();
+  MPM_CK(launch_grid_update(pool(), block_scene.ptr, total_cells, a, 1, st));
+  eng->launches += 1;
+  if (!max_jacobi) return;
+  float4* bufs[2] = {vel.ptr, vel2.ptr};
+  int cur = 0;
+  for (uint32_t k = 0; k < max_jacobi; ++k) {
+    MPM_CK(launch_grid_jacobi(pool(), block_scene.ptr, total_cells, a, bufs[cur], bufs[cur ^ 1], k, st));
+    eng->launches += 1;
+    cur ^= 1;
+  }
+  if (cur) {
+    MPM_CK(launch_vel_copy(touched[a].ptr, block_scene.ptr, total_cells, bufs[1], bufs[0], st));
+    eng->launches += 1;
+  }
+}
+
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   if (need_regroup || deterministic) regroup(true, st);
+  const uint32_t max_jacobi = max_jacobi_iters();
   launch_gather_pass(kRecord, false, st);
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
-  const uint64_t total_cells = cells.high_water();
   uint32_t since = 0;
   for (uint32_t s = 0; s < substeps; ++s) {
     ProfRec pr;
     eng->prof_begin(kStageGrid, st, &pr);
-    MPM_CK(launch_grid_update(pool(), block_scene.ptr, total_cells, a, 1, st));
+    grid_pass(a, max_jacobi, st);
     eng->prof_end(&pr, st);
-    eng->launches += 1;
     const bool last = s + 1 == substeps;
     const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
     launch_gather_pass(last ? kG2P : kG2PRecord, due, st);

@@ -163,6 +163,7 @@ class Group {
   DevBuf<uint32_t> slot_of, keys_by_id, slot_key, ks[2], vs[2], hist;
   // grid pool
   DevBuf<float4> acc[2], vel;
+  DevBuf<float4> vel2;  // semi-implicit Jacobi ping-pong (allocated when a scene needs it)
   DevBuf<uint8_t> touched[2];  // per 256-cell block: acc[i] is nonzero there
   DevBuf<uint32_t> block_scene;
   // scenes
@@ -221,6 +222,10 @@ class Group {
   // Same through a cached CUDA graph.
   void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st);
   void regroup(bool compute_keys, cudaStream_t st, bool move_records = false);
+  // Grid update of accumulator a, then the semi-implicit Jacobi sweeps of
+  // the scenes that ask for them.
+  void grid_pass(int a, uint32_t max_jacobi, cudaStream_t st);
+  uint32_t max_jacobi_iters() const;
   // one item per occupied tile, plus one per kStageMax particles of a tile
   size_t max_item_count() const { return (size_t)key_space + cap / kStageMax + 2; }
   void sync_scenes(cudaStream_t st);

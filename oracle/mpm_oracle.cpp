@@ -243,6 +243,7 @@ typedef struct orc_scene {
   orc_material materials[8];
   double svd_tol;        // 1e-7 in the reference
   uint32_t svd_sweeps;   // 16 in the reference
+  uint32_t jacobi_iters; // MpmTimeStep::Implicit sweeps per substep (0: explicit)
 } orc_scene;
 
 }  // extern "C"
@@ -495,6 +496,56 @@ template <class R> static void grid_update(const Params<R>& p, Grid<R>& g, int n
       }
 }
 
+// mpm_implicit_apply + mpm_implicit_swap (mpm.wgsl:1060-1173): jacobi_iters
+// sweeps on the grid velocity; a node with mass blends with the mean of its
+// face neighbours that carry mass, at the rate a = dt^2 m (E / 1500) / dx^2.
+template <class R> static void implicit_sweeps(const orc_scene& sc, const Params<R>& p, Grid<R>& g, int nthreads) {
+  const int n = p.n;
+  const size_t n3 = (size_t)n * n * n;
+  std::vector<R> next(3 * n3);
+  const R c2 = p.youngs / R(1500);
+  for (uint32_t it = 0; it < sc.jacobi_iters; ++it) {
+#pragma omp parallel for num_threads(nthreads > 1 ? nthreads : 1) schedule(static) if (nthreads > 1)
+    for (int iz = 0; iz < n; ++iz)
+      for (int iy = 0; iy < n; ++iy)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t c = (size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz);
+          const R m = g.mass[c];
+          const R* v = &g.vel[3 * c];
+          R* o = &next[3 * c];
+          if (m <= R(1.0e-9) || !(m == m)) {
+            o[0] = v[0];
+            o[1] = v[1];
+            o[2] = v[2];
+            continue;
+          }
+          const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+          R avg[3] = {R(0), R(0), R(0)};
+          R count = R(0);
+          for (int k = 0; k < 6; ++k) {
+            const int nx = ix + off[k][0], ny = iy + off[k][1], nz = iz + off[k][2];
+            if (nx < 0 || ny < 0 || nz < 0 || nx >= n || ny >= n || nz >= n) continue;
+            const size_t nc = (size_t)nx + (size_t)n * ((size_t)ny + (size_t)n * (size_t)nz);
+            const R nm = g.mass[nc];
+            if (nm <= R(1.0e-9) || !(nm == nm)) continue;
+            for (int a = 0; a < 3; ++a) avg[a] = avg[a] + g.vel[3 * nc + a];
+            count = count + R(1);
+          }
+          for (int a = 0; a < 3; ++a) avg[a] = count > R(0) ? avg[a] / count : v[a];
+          const R alpha = p.dt * p.dt * m * c2 * p.inv_dx * p.inv_dx;
+          const R denom = m + alpha;
+          R vn[3];
+          bool nan = false;
+          for (int a = 0; a < 3; ++a) {
+            vn[a] = (m * v[a] + alpha * avg[a]) / denom;
+            nan = nan || !(vn[a] == vn[a]);
+          }
+          for (int a = 0; a < 3; ++a) o[a] = nan ? v[a] : vn[a];
+        }
+    g.vel.swap(next);
+  }
+}
+
 template <class R> static inline bool finite_vec(const R* v) {
   return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
 }
@@ -699,6 +750,7 @@ static void step(const orc_scene& sc, State<R>& st, R* out_mass, R* out_mom, uin
       }
     }
     grid_update(p, g, nthreads);
+    if (sc.jacobi_iters) implicit_sweeps(sc, p, g, nthreads);
     status[1] += 1;
     bool fault = false;
     if (nthreads <= 1) {

@@ -52,6 +52,7 @@ class orc_scene(C.Structure):
         ("materials", orc_material * 8),
         ("svd_tol", C.c_double),
         ("svd_sweeps", C.c_uint32),
+        ("jacobi_iters", C.c_uint32),
     ]
 
 
@@ -148,6 +149,7 @@ def make_scene(cfg, rows, dt: float, svd_tol: float = 1e-7, svd_sweeps: int = 16
         m.poisson = float(_get(r, "poisson"))
     s.svd_tol = svd_tol
     s.svd_sweeps = svd_sweeps
+    s.jacobi_iters = int(_get(cfg, "jacobi_iters", 0)) if int(_get(cfg, "time_step", 0)) == 1 else 0
     return s
 
 

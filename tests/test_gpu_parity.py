@@ -336,6 +336,28 @@ def test_all_fp64_gpu_matches_fp64_oracle(engine, preset):
     assert abs(mass - cfg.particle_mass * len(pts)) / (cfg.particle_mass * len(pts)) < 1e-12
 
 
+def test_semi_implicit_preset_matches_oracle(engine):
+    """MpmConfig::sand_calibrated (Implicit { jacobi_iters: 3 }) against the
+    oracle's semi-implicit sweeps (mpm.wgsl:1060-1173); and switching an
+    existing simulation to an even sweep count through set_time_step."""
+    cfg = m.MpmConfig.sand_calibrated()
+    assert cfg.time_step == 1 and cfg.jacobi_iters == 3
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.7, 0.2], 10, 9)
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 480, 30)
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 2e-5
+    assert np.abs(gpu["vel"] - st["vel"]).max() < 2e-3
+    sim = m.MpmSimulation.new(engine, m.MpmConfig.sand())
+    sim.set_particles(pts)
+    sim.set_time_step(1, 2)
+    sim.step_n(1.0 / 480, 30)
+    c2 = m.MpmConfig.sand()
+    c2.time_step, c2.jacobi_iters = 1, 2
+    sc = O.make_scene(c2, [c2.rheology], 1.0 / 480)
+    st2 = O.init_state(pts, mass=c2.particle_mass, volume=c2.particle_volume)
+    O.step(sc, st2, 30)
+    assert np.abs(sim.read_positions() - st2["pos"]).max() < 2e-5
+
+
 def test_soil_checkpoint_round_trip_and_continuation(engine):
     """archive_drop_reload_preserves_all_history (mpm_checkpoint_tests.rs:176-257):
     a checkpoint of an evolved state restores bit for bit into a fresh

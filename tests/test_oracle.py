@@ -305,3 +305,43 @@ def test_fault_latches_and_freezes_state():
     O.step(sc, st, 3)
     for k in ("pos", "vel", "C", "jp"):
         assert np.array_equal(before[k], st[k], equal_nan=True)
+
+
+# ---- semi-implicit Jacobi relaxation (mpm.wgsl:1060-1173) ----
+
+def test_implicit_sweeps_keep_a_uniform_velocity_field():
+    """Every node of a block in uniform translation has the same velocity,
+    so the neighbour mean equals it and the relaxation changes nothing."""
+    cfg = m.MpmConfig.sand()
+    cfg.gravity_y = 0.0
+    pts = scenes.fill_box_lcg([-0.15, 0.3, -0.15], [0.15, 0.6, 0.15], 8, 4)
+    vel = np.tile(np.array([[0.3, -0.2, 0.1]], np.float32), (len(pts), 1))
+    runs = []
+    for kind, iters in ((0, 0), (1, 3)):
+        cfg.time_step, cfg.jacobi_iters = kind, iters
+        sc = O.make_scene(cfg, [cfg.rheology], 1.0 / 480)
+        st = O.cast_state(O.init_state(pts, vel, mass=cfg.particle_mass, volume=cfg.particle_volume), np.float64)
+        O.step(sc, st, 1, precision="f64")
+        runs.append(st)
+    assert np.abs(runs[0]["vel"] - runs[1]["vel"]).max() < 1e-12
+    assert np.abs(runs[0]["pos"] - runs[1]["pos"]).max() < 1e-14
+
+
+def test_implicit_sweeps_relax_a_velocity_jump():
+    """Two halves sliding past each other: the semi-implicit sweeps pull the
+    grid velocities toward their neighbour means, so the particle velocity
+    jump across the interface after one substep is smaller than explicit."""
+    cfg = m.MpmConfig.sand_calibrated()
+    cfg.gravity_y = 0.0
+    pts = scenes.fill_box_lcg([-0.15, 0.3, -0.15], [0.15, 0.6, 0.15], 10, 6)
+    vel = np.zeros_like(pts)
+    vel[:, 0] = np.where(pts[:, 1] > 0.45, 1.0, -1.0)
+    jumps = {}
+    for kind, iters in ((0, 0), (1, 3)):
+        cfg.time_step, cfg.jacobi_iters = kind, iters
+        sc = O.make_scene(cfg, [cfg.rheology], 1.0 / 480)
+        st = O.init_state(pts, vel, mass=cfg.particle_mass, volume=cfg.particle_volume)
+        O.step(sc, st, 1)
+        v = st["vel"][:, 0]
+        jumps[iters] = v[pts[:, 1] > 0.45].mean() - v[pts[:, 1] <= 0.45].mean()
+    assert 0.0 < jumps[3] < jumps[0]
