@@ -1,7 +1,10 @@
 // mpm_kernels.cuh — host launchers of the substep kernels.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <string>
 
 #include "mpm_device.cuh"
 
@@ -16,7 +19,11 @@ enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
 
 cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
                           int reuse, int grid, cudaStream_t st);
-cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st);
+// The scatter stages its records with TMA through `rec_map`, a 2-D tensor
+// map of the record buffer (16 floats x cap, 64-byte swizzle) built by
+// make_record_map.
+cudaError_t launch_scatter(const PoolDev& p, const CUtensorMap& rec_map, int acc_out, int grid, cudaStream_t st);
+bool make_record_map(CUtensorMap* out, const float* rec, uint32_t cap, std::string* err);
 // Deterministic (fixed-order) scatter: per-tile blocks, then a combine pass.
 cudaError_t launch_scatter_det(const PoolDev& p, float4* blocks, int acc_out, int grid, cudaStream_t st);
 cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uint32_t* tile_item, uint32_t max_items,
@@ -24,7 +31,8 @@ cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uin
 constexpr int kTileNodes = 216;  // 6^3 node footprint of a 4^3-cell tile of base cells
 constexpr uint32_t kFaultNondeterministic = 4u;  // a deposit left the fixed-order path
 constexpr uint32_t kFaultDeviceWait = 8u;        // a bounded device-side wait gave up (or an item was malformed)
-constexpr int kStageMax = 1008;                  // particles per scatter item (records staged in shared memory)
+constexpr int kStageMax = 960;                   // particles per scatter item (records staged in shared memory)
+constexpr int kStageBoxRows = 64;                // records per TMA box of the scatter stage
 // Persistent grid sizes (SMs x resident CTAs).
 int gather_grid_size(bool svd_fp64);
 int scatter_grid_size();

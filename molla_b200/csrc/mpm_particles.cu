@@ -107,15 +107,14 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
-// 16-byte aligned) completing on `bar`, which expects those bytes.
-__device__ __forceinline__ void bulk_load_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
+// 2-D TMA tile load (box of kStageBoxRows records) at coordinates (0, row)
+// of the record tensor map, completing on `bar`.
+__device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int row, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(smem_addr(bar))
+      : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t done;
@@ -451,8 +450,11 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 // Persistent CTAs over items (a tile's particles from the last regrouping,
 // at most kStageMax), 192 threads.  Per item:
 //  1. stage: the item's 64-byte records (contiguous slots) arrive in shared
-//     memory by one bulk copy (the TMA engine: cp.async.bulk completing on
-//     an mbarrier), issued while the previous item's block was flushed;
+//     memory as 2-D TMA tiles of 64 records (cp.async.bulk.tensor completing
+//     on an mbarrier), issued while the previous item's block was flushed.
+//     The tiles use the 64-byte swizzle: 16-byte chunk k of record j sits at
+//     chunk k ^ ((j >> 1) & 3), which spreads the lanes' reads of one chunk
+//     of different records over all shared-memory banks;
 //  2. bin: every particle is binned by its current base cell among the 6^3
 //     cells whose stencils fit the tile's 8^3-node block (a counting sort in
 //     shared memory with warp-aggregated counters), so particles that moved
@@ -471,10 +473,10 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 // Every wait on the stage is bounded (about one second); a wait that gives
 // up sets kFaultDeviceWait in the scene's status word and ends the CTA after
 // a second bounded wait for its copy in flight.
-__device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4* __restrict__ acc,
+__device__ __noinline__ void deposit_global(float4 r0, float4 r1, float4 r2, float4 r3, float4* __restrict__ acc,
                                             uint8_t* __restrict__ touched, uint64_t grid_off, int n, float ox,
-                                            float oy, float oz, float inv_dx, float dx, const int* win) {
-  const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+                                            float oy, float oz, float inv_dx, float dx, int wx, int wy, int wz) {
+  const int win[3] = {wx, wy, wz};
   const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
   const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
   float wgt[3][3], fx[3];
@@ -503,8 +505,17 @@ __device__ __noinline__ void deposit_global(const float4* __restrict__ r, float4
 constexpr int kLocalCells = 216;  // 6^3 base cells whose stencils fit the 8^3 block
 constexpr int kBinRounds = (kStageMax + kScatterThreads - 1) / kScatterThreads;
 
-__global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_out) {
-  extern __shared__ __align__(128) float4 s_stage[];  // [kStageMax * 4]
+// 16-byte chunk k of staged record j under the 64-byte swizzle.
+__device__ __forceinline__ float4 stage_chunk(const float4* stage, uint32_t j, uint32_t k) {
+  return stage[4 * j + (k ^ ((j >> 1) & 3u))];
+}
+
+__global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __grid_constant__ CUtensorMap rec_map,
+                                                            int acc_out) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  // the swizzle pattern repeats every 512 bytes: align the stage to 1 KiB
+  float4* s_stage =
+      reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~static_cast<uintptr_t>(1023u));
   __shared__ float s_acc[4][kRegionFloats];
   __shared__ uint32_t s_cell[kLocalCells];  // counts, then exclusive starts
   __shared__ uint16_t s_idx[kStageMax];     // item particles sorted by local cell
@@ -512,7 +523,6 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
   __shared__ __align__(8) uint64_t s_bar;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
-  const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
   const uint32_t n_items = *p.n_items;
   const int slab = threadIdx.x >> 6;
   const uint32_t lane64 = threadIdx.x & 63u;
@@ -524,12 +534,18 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
     fence_mbar_init();
   }
   __syncthreads();
-  // Thread 0 stages item `it` (items of 1..kStageMax particles).
+  // Thread 0 stages item `it` (items of 1..kStageMax particles) as
+  // ceil(count / 64) tiles; rows past the item are loaded but not read.
   auto stage = [&](uint32_t it) {
     const Item nx = p.items[it];
     if (nx.count - 1u < (uint32_t)kStageMax) {
+      const uint32_t boxes = (nx.count + kStageBoxRows - 1) / kStageBoxRows;
       fence_proxy_async_smem();
-      bulk_load_g2s(s_stage, rec + 4 * (size_t)nx.start, nx.count * 64u, &s_bar);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&s_bar)),
+                   "r"(boxes * kStageBoxRows * 64u)
+                   : "memory");
+      for (uint32_t b = 0; b < boxes; ++b)
+        tma_load_rows(s_stage + (size_t)b * kStageBoxRows * 4, &rec_map, (int)(nx.start + b * kStageBoxRows), &s_bar);
     }
   };
   if (threadIdx.x == 0 && blockIdx.x < n_items) stage(blockIdx.x);
@@ -563,7 +579,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
       const uint32_t j = threadIdx.x + q * kScatterThreads;
       uint32_t lc = 0xffffu;
       if (live && j < item.count) {
-        const float4 r0 = s_stage[4 * j];
+        const float4 r0 = stage_chunk(s_stage, j, 0);
         if (r0.w != 0.f) {
           const int lx = (int)floorf((r0.x - ox) * inv_dx - 0.5f) - win[0] - rx;
           const int ly = (int)floorf((r0.y - oy) * inv_dx - 0.5f) - win[1] - ry;
@@ -571,7 +587,8 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
           if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
             lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
           } else {
-            deposit_global(s_stage + 4 * j, acc, touched, grid_off, n, ox, oy, oz, inv_dx, dx, win);
+            deposit_global(r0, stage_chunk(s_stage, j, 1), stage_chunk(s_stage, j, 2), stage_chunk(s_stage, j, 3), acc,
+                           touched, grid_off, n, ox, oy, oz, inv_dx, dx, win[0], win[1], win[2]);
           }
         }
       }
@@ -628,8 +645,9 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, int acc_o
         for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
         const uint32_t first = s_cell[lc], end = lc == kLocalCells - 1 ? total : s_cell[lc + 1];
         for (uint32_t t = first; t < end; ++t) {
-          const float4* __restrict__ rp = s_stage + 4 * (uint32_t)s_idx[t];
-          const float4 r0 = rp[0], r1 = rp[1], r2 = rp[2], r3 = rp[3];
+          const uint32_t j = s_idx[t];
+          const float4 r0 = stage_chunk(s_stage, j, 0), r1 = stage_chunk(s_stage, j, 1),
+                       r2 = stage_chunk(s_stage, j, 2), r3 = stage_chunk(s_stage, j, 3);
           const float mass = r0.w;
           const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
           const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
@@ -940,10 +958,42 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
   return cudaErrorInvalidValue;
 }
 
-constexpr size_t kStageBytes = (size_t)kStageMax * 64;
+// stage tiles plus 1 KiB for the alignment of the swizzled stage
+constexpr size_t kStageBytes = (size_t)kStageMax * 64 + 1024;
+static_assert(kStageMax % kStageBoxRows == 0, "the stage holds whole TMA tiles");
 
-cudaError_t launch_scatter(const PoolDev& p, int acc_out, int grid, cudaStream_t st) {
-  k_p2g<<<grid, kScatterThreads, kStageBytes, st>>>(p, acc_out);
+bool make_record_map(CUtensorMap* out, const float* rec, uint32_t cap, std::string* err) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      if (err) *err = "cuTensorMapEncodeTiled is not available from the driver";
+      return false;
+    }
+    encode = reinterpret_cast<EncodeFn>(fn);
+  }
+  // records: rows of 16 floats (64 bytes), cap rows; tiles of 64 rows
+  const cuuint64_t dims[2] = {16, cap ? cap : 1};
+  const cuuint64_t strides[1] = {64};
+  const cuuint32_t box[2] = {16, (cuuint32_t)kStageBoxRows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(rec), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    if (err) *err = "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r);
+    return false;
+  }
+  return true;
+}
+
+cudaError_t launch_scatter(const PoolDev& p, const CUtensorMap& rec_map, int acc_out, int grid, cudaStream_t st) {
+  k_p2g<<<grid, kScatterThreads, kStageBytes, st>>>(p, rec_map, acc_out);
   return cudaGetLastError();
 }
 

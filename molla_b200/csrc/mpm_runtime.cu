@@ -229,6 +229,10 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   planes[0].alloc((size_t)kPlanes * cap);
   planes[1].alloc((size_t)kPlanes * cap);
   rec[0].alloc((size_t)16 * cap);
+  {
+    std::string err;
+    if (!make_record_map(&rec_map[0], rec[0].ptr, cap, &err)) throw Error(MPM_ERR_GPU, "MPM scatter stage: " + err);
+  }
   for (int i = 0; i < 2; ++i) {
     meta[i].alloc(cap);
     orig[i].alloc(cap);
@@ -593,7 +597,7 @@ void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
     MPM_CK(launch_combine_det(pool(), det_blocks.ptr, tile_item.ptr, key_space, acc_out, st));
     eng->launches += 1;
   } else {
-    MPM_CK(launch_scatter(pool(), acc_out, grid_scatter, st));
+    MPM_CK(launch_scatter(pool(), rec_map[rec_cur], acc_out, grid_scatter, st));
   }
   eng->prof_end(&pr, st);
   eng->launches += 1;
@@ -699,7 +703,11 @@ void Group::set_deterministic(bool on) {
   if (on == deterministic) return;
   deterministic = on;
   if (on) {
-    if (rec[1].count < (size_t)16 * cap) rec[1].alloc((size_t)16 * cap);
+    if (rec[1].count < (size_t)16 * cap) {
+      rec[1].alloc((size_t)16 * cap);
+      std::string err;
+      if (!make_record_map(&rec_map[1], rec[1].ptr, cap, &err)) throw Error(MPM_ERR_GPU, "MPM scatter stage: " + err);
+    }
     const size_t max_items = (size_t)key_space + 2;
     if (tile_item.count < max_items) tile_item.alloc(max_items);
     if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);

@@ -158,6 +158,7 @@ class Group {
   // particle pool (double-buffered for the regroup)
   DevBuf<float> planes[2];
   DevBuf<float> rec[2];  // per-slot scatter record, 16 floats (64 B) per slot (rec[1]: deterministic mode)
+  CUtensorMap rec_map[2];  // TMA maps of rec[0], rec[1] for the scatter stage
   int rec_cur = 0;
   DevBuf<uint32_t> meta[2], orig[2];
   DevBuf<uint32_t> slot_of, keys_by_id, slot_key, ks[2], vs[2], hist;
