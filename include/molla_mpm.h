@@ -228,6 +228,16 @@ MPM_API int mpm_batch_encode_step(mpm_batch* batch, const mpm_prepared* prepared
 MPM_API int mpm_batch_submit(mpm_batch* batch);
 MPM_API int mpm_batch_cancel(mpm_batch* batch);
 
+/* set_rigid_spheres (mpm.rs:1521-1565): n <= max_rigid (and <= 8) spheres
+ * of 7 floats each (center xyz, radius, velocity xyz), replacing the
+ * previous set; kept across set_particles.  Each substep, grid nodes inside
+ * a sphere take its velocity with the heavy-cell mass 1e6 (rigid_imprint,
+ * mpm.wgsl:939-1003) and sand nodes within radius + dx react on it
+ * (mpm_rigid_force_integrate, :1175-1228). */
+MPM_API int mpm_set_rigid_spheres(mpm_sim* sim, const float* spheres, uint32_t n);
+/* read_rigid_wrenches (mpm.rs:2809, 2908-2956): blocking; out[6 * i] =
+ * force xyz, torque xyz on sphere i during the last substep. */
+MPM_API int mpm_read_rigid_wrenches(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
 /* read_positions / read_velocities (mpm.rs:2718-2798): blocking; writes
  * min(count, cap) rows of 3 floats in the original particle order and
  * stores the particle count in *count_out. */

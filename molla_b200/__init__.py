@@ -460,6 +460,23 @@ class MpmSimulation:
         _check(_ffi.lib().mpm_read_grid_mass_momentum(self._h, _fp(m), _fp(p), n3))
         return m, p
 
+    def set_rigid_spheres(self, spheres):
+        """set_rigid_spheres (mpm.rs:1521-1565): [(center_xyz, radius, velocity_xyz)]."""
+        arr = np.zeros((max(len(spheres), 1), 7), np.float32)
+        for i, (c, r, v) in enumerate(spheres):
+            arr[i, 0:3] = c
+            arr[i, 3] = r
+            arr[i, 4:7] = v
+        _check(_ffi.lib().mpm_set_rigid_spheres(self._h, _fp(arr), len(spheres)))
+
+    def read_rigid_wrenches(self):
+        """read_rigid_wrenches (mpm.rs:2809): [(force_xyz, torque_xyz)] of the last substep."""
+        cap = 8
+        out = np.zeros((cap, 6), np.float32)
+        cnt = C.c_uint32()
+        _check(_ffi.lib().mpm_read_rigid_wrenches(self._h, _fp(out), cap, C.byref(cnt)))
+        return [(out[i, :3].copy(), out[i, 3:].copy()) for i in range(cnt.value)]
+
     def checkpoint_soil(self) -> bytes:
         """checkpoint_soil_with (mpm_checkpoint.rs:388-434): the particle state
         in molla's versioned soil-checkpoint bytes (BLAKE3 digest)."""

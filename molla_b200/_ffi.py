@@ -161,6 +161,8 @@ SIGNATURES = {
     "mpm_group_autotune": (I, [P, U32, U32P, U32, F32P, U32P]),
     "mpm_autotune": (I, [P, C.c_float, U32, U32P, U32, F32P, U32P]),
     "mpm_group_tune": (I, [P, U32, U32]),
+    "mpm_set_rigid_spheres": (I, [P, F32P, U32]),
+    "mpm_read_rigid_wrenches": (I, [P, F32P, U32, U32P]),
     "mpm_checkpoint_save": (I, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "mpm_checkpoint_load": (I, [P, P, C.c_size_t]),
     "mpm_checkpoint_reencode": (I, [P, C.c_size_t, U32, P, C.c_size_t, C.POINTER(C.c_size_t), U32P]),

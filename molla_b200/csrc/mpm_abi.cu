@@ -92,6 +92,7 @@ struct mpm_sim {
   bool det_prepared = false;
   bool det_enabled = false;
   uint32_t sort_interval = 0;
+  std::vector<float> spheres;  // rigid spheres, 7 floats each (kept across set_particles)
   uint64_t epoch = 1;
   float dt = 1.0e-4f;
 
@@ -379,6 +380,8 @@ static void sim_reseed(mpm_sim* s, const float* xyz, const float* vel, uint32_t 
   s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, n ? mat.data() : nullptr, n, s->dt);
   s->count = n;
   s->apply_group_settings();
+  if (!s->spheres.empty())
+    s->group->set_scene_rigid(s->sid, s->spheres.data(), (uint32_t)(s->spheres.size() / 7), s->eng->stream);
   s->invalidate();
 }
 
@@ -391,6 +394,35 @@ int mpm_set_particles(mpm_sim* sim, const float* xyz, const float* vel_or_null, 
     sim->mass.clear();
     sim->volume.clear();
     sim_reseed(sim, xyz, vel_or_null, n);
+  });
+}
+
+int mpm_set_rigid_spheres(mpm_sim* sim, const float* spheres, uint32_t n) {
+  return guard([&] {
+    REQUIRE(sim && (spheres || n == 0), MPM_ERR_INVALID, "null argument");
+    REQUIRE(n <= sim->cfg.max_rigid, MPM_ERR_GPU,
+            "set_rigid_spheres: n=" + std::to_string(n) + " > max_rigid=" + std::to_string(sim->cfg.max_rigid));
+    REQUIRE(n <= (uint32_t)mpm::kMaxRigid, MPM_ERR_UNSUPPORTED, "at most 8 rigid spheres per simulation");
+    sim->eng->check();
+    sim->spheres.assign(spheres, spheres + 7 * (size_t)n);
+    if (sim->sid != 0xffffffffu) sim->group->set_scene_rigid(sim->sid, spheres, n, sim->eng->stream);
+    sim->invalidate();
+  });
+}
+
+int mpm_read_rigid_wrenches(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim->eng->check();
+    const uint32_t n = (uint32_t)(sim->spheres.size() / 7);
+    if (count_out) *count_out = n;
+    if (!n) return;
+    REQUIRE(out && cap >= n, MPM_ERR_INVALID, "output capacity below the sphere count");
+    if (sim->sid == 0xffffffffu) {
+      std::fill(out, out + 6 * (size_t)n, 0.f);
+      return;
+    }
+    sim->group->read_scene_wrench(sim->sid, out, n, sim->eng->stream);
   });
 }
 
@@ -1247,6 +1279,8 @@ int mpm_checkpoint_load(mpm_sim* sim, const uint8_t* bytes, size_t len) {
     REQUIRE(sim && (bytes || len == 0), MPM_ERR_INVALID, "null argument");
     sim->eng->check();
     const mpm::SoilCheckpoint k = mpm::decode_checkpoint(bytes, len, sim->cfg.max_particles);
+    REQUIRE(sim->spheres.empty(), MPM_ERR_INVALID,
+            "MPM soil checkpoint: incompatible configuration, capacity or attached rigid bodies");
     const int32_t* w0 = sim->cfg.grid_window_cells;
     REQUIRE(mpm::checkpoint_config_compatible(k.cfg, sim->cfg) && k.window[0] == w0[0] && k.window[1] == w0[1] &&
                 k.window[2] == w0[2] && k.count <= sim->cfg.max_particles,

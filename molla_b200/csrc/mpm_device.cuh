@@ -78,7 +78,17 @@ struct SceneDev {
   uint32_t live;       // 0 once the scene was removed (its particles leave at the next regroup)
   uint32_t jacobi_iters;  // semi-implicit sweeps per substep (MpmTimeStep::Implicit), 0 explicit
   float youngs;           // the configuration's Young's modulus (implicit stiffness estimate)
+  uint32_t n_rigid;       // rigid spheres of this scene (slots scene * kMaxRigid ...)
+  uint32_t pad_rigid;
   MatDev mat[kMaxMaterials];
+};
+
+// A rigid sphere coupled to a scene (set_rigid_spheres, mpm.rs:1521-1565):
+// center, radius and linear velocity.
+constexpr int kMaxRigid = 8;
+struct RigidDev {
+  float cx, cy, cz, radius;
+  float vx, vy, vz, pad;
 };
 
 // A work item: `count` consecutive particle slots starting at `start`, all
@@ -96,6 +106,9 @@ struct PoolDev {
   uint32_t* keys_by_id; // sort key per identity (written when a regroup is due)
   float4* acc[2];       // grid accumulators (mass, momentum)
   uint8_t* touched[2];  // per 256-cell block of the grid pool: acc[i] holds deposits there
+  const uint8_t* rigid_blocks;  // per 256-cell block: a rigid sphere may reach it
+  const RigidDev* rigid;        // kMaxRigid per scene
+  float* wrench;                // 8 floats per sphere slot: force xyz, 0, torque xyz, 0
   float4* vel;          // grid velocity (vx, vy, vz, mass)
   float* rec;           // per slot 16 floats: (x, y, z, m), (m v, B0), (B1..B4), (B5..B8)
   const uint32_t* slot_key;  // regroup key of each slot: (tile << 6) | cell in tile

@@ -39,10 +39,15 @@ __device__ __forceinline__ uint32_t tile_key_of(const SceneDev& sc, float x, flo
 }  // namespace
 
 // grid_update (mpm.wgsl:1013-1058) over the grid pool, one block per
-// 256-cell block.  Only blocks the last scatter touched are converted; the
-// blocks touched by the scatter before it are cleared in the other
-// accumulator (ready for the next scatter) and unmarked.  Counts completed
-// substeps.
+// 256-cell block.  Only blocks the last scatter touched (or a rigid sphere
+// may reach) are converted; the blocks touched by the scatter before it are
+// cleared in the other accumulator (ready for the next scatter) and
+// unmarked.  Counts completed substeps.  The rigid-sphere imprint
+// (rigid_imprint, mpm.wgsl:939-1003) is fused in front of the conversion: a
+// node inside a sphere takes the sphere's velocity with the heavy-cell mass
+// 1e6, its sand mass and momentum give the reaction wrench, and the node is
+// marked rigid (negative w in the velocity buffer) so that gravity, walls
+// and the implicit sweeps leave it alone.
 __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
                                                               uint64_t total_cells, int acc_in, int count_substep) {
   static_assert(kCellThreads == kCellBlock, "one thread block per grid-pool block");
@@ -53,6 +58,7 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
   if (sid == 0xffffffffu) return;
   const bool in_a = p.touched[acc_in][blk] != 0;
   const bool in_b = p.touched[acc_in ^ 1][blk] != 0;
+  const bool rb = p.rigid_blocks[blk] != 0;
   if (in_b) p.acc[acc_in ^ 1][g] = make_float4(0.f, 0.f, 0.f, 0.f);
   const SceneDev& sc = p.scenes[sid];
   const uint64_t local64 = g - sc.grid_off;
@@ -63,18 +69,53 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
   }
   __syncthreads();  // every thread has read the marks
   if (threadIdx.x == 0 && in_b) p.touched[acc_in ^ 1][blk] = 0;
-  if (!in_a || local64 >= (uint64_t)n * n * n) return;
+  if ((!in_a && !rb) || local64 >= (uint64_t)n * n * n) return;
   const uint32_t local = (uint32_t)local64;  // grids hold fewer than 2^32 cells
-  const float4 a = p.acc[acc_in][g];
+  const uint32_t q = local / n;
+  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
+  float4 a = p.acc[acc_in][g];
+  bool rigid = false;
+  if (rb && sc.n_rigid) {
+    const float node[3] = {sc.ox + (float)(ix + sc.winx) * sc.dx, sc.oy + (float)(iy + sc.winy) * sc.dx,
+                           sc.oz + (float)(iz + sc.winz) * sc.dx};
+    for (uint32_t r = 0; r < sc.n_rigid; ++r) {
+      const RigidDev R = p.rigid[(size_t)sid * kMaxRigid + r];
+      const float arm[3] = {node[0] - R.cx, node[1] - R.cy, node[2] - R.cz};
+      if (!(sqrtf(arm[0] * arm[0] + arm[1] * arm[1] + arm[2] * arm[2]) < R.radius)) continue;
+      const float m_old = a.x;
+      const float mom_old[3] = {a.y, a.z, a.w};
+      const float stamp = 1.0e6f;
+      a = make_float4(stamp, stamp * R.vx, stamp * R.vy, stamp * R.vz);
+      p.acc[acc_in][g] = a;
+      if (!in_a) p.touched[acc_in][blk] = 1;
+      rigid = true;
+      if (m_old > 1.0e-9f) {
+        const float inv_dt = 1.0f / fmaxf(sc.dt, 1.0e-6f);
+        const float f[3] = {-(m_old * R.vx - mom_old[0]) * inv_dt, -(m_old * R.vy - mom_old[1]) * inv_dt,
+                            -(m_old * R.vz - mom_old[2]) * inv_dt};
+        const float t[3] = {arm[1] * f[2] - arm[2] * f[1], arm[2] * f[0] - arm[0] * f[2], arm[0] * f[1] - arm[1] * f[0]};
+        float* w = p.wrench + ((size_t)sid * kMaxRigid + r) * 8;
+        atomicAdd(w + 0, f[0]);
+        atomicAdd(w + 1, f[1]);
+        atomicAdd(w + 2, f[2]);
+        atomicAdd(w + 4, t[0]);
+        atomicAdd(w + 5, t[1]);
+        atomicAdd(w + 6, t[2]);
+      }
+      break;
+    }
+  }
   const float m = a.x;
   if (m <= 1.0e-9f || !(m == m)) {
     p.vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);
     return;
   }
   float v[3] = {a.y / m, a.z / m, a.w / m};
+  if (rigid) {
+    p.vel[g] = make_float4(v[0], v[1], v[2], -m);  // skip integration on rigid-imprinted nodes
+    return;
+  }
   v[1] = v[1] + sc.dt * sc.gy;
-  const uint32_t q = local / n;
-  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
   const int pad = sc.pad, nn = (int)n;
   const float f = sc.friction;
   if (sc.sticky) {
@@ -89,6 +130,51 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
     if (iz >= nn - pad) { v[2] = fminf(v[2], 0.f); v[0] *= f; v[1] *= f; }
   }
   p.vel[g] = make_float4(v[0], v[1], v[2], m);
+}
+
+// mpm_rigid_force_integrate (mpm.wgsl:1175-1228): every non-rigid node with
+// sand mass within radius + dx of a sphere adds the reaction
+// -(m w / dt) (v_sphere - v_node) (w tapered linearly over the outer cell)
+// and its torque to the sphere's wrench.
+__global__ void __launch_bounds__(kCellThreads) k_rigid_shell(PoolDev p, const uint32_t* __restrict__ block_scene,
+                                                              uint64_t total_cells, int acc_in) {
+  const uint64_t blk = blockIdx.x;
+  if (blk * kCellThreads >= total_cells) return;
+  const uint32_t sid = block_scene[blk];
+  if (sid == 0xffffffffu || !p.rigid_blocks[blk] || !p.touched[acc_in][blk]) return;
+  const SceneDev& sc = p.scenes[sid];
+  if (!sc.n_rigid) return;
+  const uint64_t g = blk * kCellThreads + threadIdx.x;
+  const uint64_t local64 = g - sc.grid_off;
+  const uint32_t n = sc.n;
+  if (local64 >= (uint64_t)n * n * n) return;
+  const float m = p.acc[acc_in][g].x;
+  if (m <= 1.0e-9f || !(m == m)) return;
+  const float4 vg = p.vel[g];
+  if (vg.w < 0.f) return;  // rigid-stamped node
+  const uint32_t local = (uint32_t)local64;
+  const uint32_t q = local / n;
+  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
+  const float node[3] = {sc.ox + (float)(ix + sc.winx) * sc.dx, sc.oy + (float)(iy + sc.winy) * sc.dx,
+                         sc.oz + (float)(iz + sc.winz) * sc.dx};
+  for (uint32_t r = 0; r < sc.n_rigid; ++r) {
+    const RigidDev R = p.rigid[(size_t)sid * kMaxRigid + r];
+    const float arm[3] = {node[0] - R.cx, node[1] - R.cy, node[2] - R.cz};
+    const float d = sqrtf(arm[0] * arm[0] + arm[1] * arm[1] + arm[2] * arm[2]);
+    if (d > R.radius + sc.dx) continue;
+    float w = 1.0f;
+    if (d > R.radius) w = fmaxf(0.0f, 1.0f - (d - R.radius) / sc.dx);
+    const float k = -(m * w / fmaxf(sc.dt, 1.0e-6f));
+    const float f[3] = {k * (R.vx - vg.x), k * (R.vy - vg.y), k * (R.vz - vg.z)};
+    const float t[3] = {arm[1] * f[2] - arm[2] * f[1], arm[2] * f[0] - arm[0] * f[2], arm[0] * f[1] - arm[1] * f[0]};
+    float* wr = p.wrench + ((size_t)sid * kMaxRigid + r) * 8;
+    atomicAdd(wr + 0, f[0]);
+    atomicAdd(wr + 1, f[1]);
+    atomicAdd(wr + 2, f[2]);
+    atomicAdd(wr + 4, t[0]);
+    atomicAdd(wr + 5, t[1]);
+    atomicAdd(wr + 6, t[2]);
+  }
 }
 
 // One semi-implicit Jacobi sweep on the grid velocity (mpm_implicit_apply,
@@ -112,7 +198,8 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_jacobi(PoolDev p, const u
   if (local64 >= (uint64_t)n * n * n) return;
   const float4 cur = src[g];
   const float m = p.acc[acc_in][g].x;
-  if (sweep >= sc.jacobi_iters || m <= 1.0e-9f || !(m == m)) {
+  // massless, rigid-stamped (negative w) or done: copy through
+  if (sweep >= sc.jacobi_iters || m <= 1.0e-9f || !(m == m) || cur.w < 0.f) {
     dst[g] = cur;
     return;
   }
@@ -420,6 +507,14 @@ cudaError_t launch_grid_jacobi(const PoolDev& p, const uint32_t* block_scene, ui
   const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
   if (blocks == 0) return cudaSuccess;
   k_grid_jacobi<<<(unsigned)blocks, kCellThreads, 0, st>>>(p, block_scene, total_cells, acc_in, src, dst, sweep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rigid_shell(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
+                               cudaStream_t st) {
+  const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
+  if (blocks == 0) return cudaSuccess;
+  k_rigid_shell<<<(unsigned)blocks, kCellThreads, 0, st>>>(p, block_scene, total_cells, acc_in);
   return cudaGetLastError();
 }
 

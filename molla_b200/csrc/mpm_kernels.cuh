@@ -57,6 +57,9 @@ cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, const 
 // Semi-implicit Jacobi sweep `sweep` (src -> dst) over the touched blocks.
 cudaError_t launch_grid_jacobi(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
                                const float4* src, float4* dst, uint32_t sweep, cudaStream_t st);
+// Rigid-sphere shell reaction over the touched blocks a sphere may reach.
+cudaError_t launch_rigid_shell(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
+                               cudaStream_t st);
 cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene, uint64_t total_cells,
                             const float4* src, float4* dst, cudaStream_t st);
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,

@@ -246,6 +246,9 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   hist.alloc(sort_hist_words(cap));
   vel.alloc(cell_cap);
   block_scene.alloc(cell_cap / kCellBlock);
+  rigid_blocks.alloc(cell_cap / kCellBlock);
+  rigid_d.alloc((size_t)max_scenes * kMaxRigid);
+  wrench_d.alloc((size_t)max_scenes * kMaxRigid * 8);
   touched[0].alloc(cell_cap / kCellBlock);
   touched[1].alloc(cell_cap / kCellBlock);
   scenes_d.alloc(max_scenes);
@@ -259,6 +262,8 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaMemsetAsync(acc[0].ptr, 0, acc[0].bytes(), stream));
   MPM_CK(cudaMemsetAsync(acc[1].ptr, 0, acc[1].bytes(), stream));
   MPM_CK(cudaMemsetAsync(vel.ptr, 0, vel.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(rigid_blocks.ptr, 0, rigid_blocks.bytes(), stream));
+  MPM_CK(cudaMemsetAsync(wrench_d.ptr, 0, wrench_d.bytes(), stream));
   MPM_CK(cudaMemsetAsync(touched[0].ptr, 0, touched[0].bytes(), stream));
   MPM_CK(cudaMemsetAsync(touched[1].ptr, 0, touched[1].bytes(), stream));
   MPM_CK(cudaMemsetAsync(keys_by_id.ptr, 0xff, keys_by_id.bytes(), stream));
@@ -298,6 +303,9 @@ PoolDev Group::pool() const {
   p.acc[1] = acc[1].ptr;
   p.touched[0] = touched[0].ptr;
   p.touched[1] = touched[1].ptr;
+  p.rigid_blocks = rigid_blocks.ptr;
+  p.rigid = rigid_d.ptr;
+  p.wrench = wrench_d.ptr;
   p.vel = vel.ptr;
   p.rec = rec[rec_cur].ptr;
   p.slot_key = slot_key.ptr;
@@ -354,6 +362,7 @@ void Group::rebuild_layout() {
     SceneHost& s = scenes[i];
     SceneDev d = s.live ? make_scene_dev(s.cfg, s.rows, s.dt) : scenes_h[i];
     if (s.live) {
+      d.n_rigid = s.n_rigid;
       d.key_off = s.key_off;
       d.status = i;
       d.grid_off = s.grid_off;
@@ -446,6 +455,7 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   MPM_CK(cudaMemsetAsync(acc[0].ptr + g0, 0, glen * sizeof(float4), stream));
   MPM_CK(cudaMemsetAsync(acc[1].ptr + g0, 0, glen * sizeof(float4), stream));
   MPM_CK(cudaMemsetAsync(vel.ptr + g0, 0, glen * sizeof(float4), stream));
+  MPM_CK(cudaMemsetAsync(rigid_blocks.ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   MPM_CK(cudaMemsetAsync(touched[0].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   MPM_CK(cudaMemsetAsync(touched[1].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   {
@@ -465,6 +475,7 @@ void Group::remove_scene(uint32_t sid) {
   SceneHost& s = scenes[sid];
   const uint32_t removed = s.n;
   s.live = false;
+  s.n_rigid = 0;
   rebuild_layout();  // marks the scene record dead, new key offsets
   // Compact: keys of every pooled particle (dead ones get 0xffffffff), sort,
   // keep the live prefix.
@@ -493,6 +504,7 @@ void Group::set_scene_dt(uint32_t sid, float dt) {
   if (s.dt == dt) return;
   s.dt = dt;
   SceneDev d = make_scene_dev(s.cfg, s.rows, dt);
+  d.n_rigid = s.n_rigid;
   d.key_off = s.key_off;
   d.status = sid;
   d.grid_off = s.grid_off;
@@ -501,6 +513,80 @@ void Group::set_scene_dt(uint32_t sid, float dt) {
   scenes_h[sid] = d;
   scenes_dirty = true;
   if (d.jacobi_iters && vel2.count < cell_cap) vel2.alloc(cell_cap);
+}
+
+bool Group::any_rigid() const {
+  for (const SceneHost& s : scenes)
+    if (s.live && s.n_rigid) return true;
+  return false;
+}
+
+void Group::set_scene_rigid(uint32_t sid, const float* sp, uint32_t n, cudaStream_t st) {
+  SceneHost& s = scenes.at(sid);
+  if (!s.live) throw Error(MPM_ERR_INVALID, "scene is not live");
+  if (n > (uint32_t)kMaxRigid) throw Error(MPM_ERR_INVALID, "at most 8 rigid spheres per scene");
+  std::vector<RigidDev> rd(n);
+  for (uint32_t r = 0; r < n; ++r) {
+    const float* q = sp + 7 * (size_t)r;
+    for (int k = 0; k < 7; ++k)
+      if (!std::isfinite(q[k])) throw Error(MPM_ERR_INVALID, "rigid sphere values must be finite");
+    rd[r] = RigidDev{q[0], q[1], q[2], q[3], q[4], q[5], q[6], 0.f};
+  }
+  if (n)
+    MPM_CK(cudaMemcpyAsync(rigid_d.ptr + (size_t)sid * kMaxRigid, rd.data(), n * sizeof(RigidDev),
+                           cudaMemcpyHostToDevice, st));
+  // Blocks a sphere may reach: every node within radius + dx of a center
+  // (the imprint needs radius, the shell reaction radius + dx), with a cell
+  // of margin for rounding.
+  const uint32_t nn = s.cfg.grid_size;
+  const uint64_t blocks = s.grid_len / kCellBlock;
+  std::vector<uint8_t> mark(blocks, 0);
+  const double dx = s.cfg.cell_size;
+  for (uint32_t r = 0; r < n; ++r) {
+    const RigidDev& R = rd[r];
+    const double c[3] = {R.cx, R.cy, R.cz};
+    int lo[3], hi[3];
+    bool empty = !(R.radius > 0.f);
+    for (int a = 0; a < 3; ++a) {
+      const double rel0 = (c[a] - R.radius - 2.0 * dx - s.cfg.grid_origin[a]) / dx - s.cfg.grid_window_cells[a];
+      const double rel1 = (c[a] + R.radius + 2.0 * dx - s.cfg.grid_origin[a]) / dx - s.cfg.grid_window_cells[a];
+      lo[a] = (int)std::max(0.0, std::floor(rel0));
+      hi[a] = (int)std::min((double)nn - 1, std::ceil(rel1));
+      empty = empty || hi[a] < lo[a];
+    }
+    if (empty) continue;
+    for (int z = lo[2]; z <= hi[2]; ++z)
+      for (int y = lo[1]; y <= hi[1]; ++y) {
+        const uint64_t row = (uint64_t)nn * ((uint64_t)y + (uint64_t)nn * z);
+        const uint64_t b0 = (row + lo[0]) / kCellBlock, b1 = (row + hi[0]) / kCellBlock;
+        for (uint64_t b = b0; b <= b1 && b < blocks; ++b) mark[b] = 1;
+      }
+  }
+  if (blocks)
+    MPM_CK(cudaMemcpyAsync(rigid_blocks.ptr + s.grid_off / kCellBlock, mark.data(), blocks, cudaMemcpyHostToDevice,
+                           st));
+  MPM_CK(cudaMemsetAsync(wrench_d.ptr + (size_t)sid * kMaxRigid * 8, 0, kMaxRigid * 8 * sizeof(float), st));
+  MPM_CK(cudaStreamSynchronize(st));
+  s.n_rigid = n;
+  const float dt = s.dt;
+  s.dt = -1.f;
+  set_scene_dt(sid, dt);
+  invalidate_graphs();
+}
+
+void Group::read_scene_wrench(uint32_t sid, float* out6, uint32_t n, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  n = std::min(n, s.n_rigid);
+  if (!n) return;
+  std::vector<float> w((size_t)n * 8);
+  MPM_CK(cudaMemcpyAsync(w.data(), wrench_d.ptr + (size_t)sid * kMaxRigid * 8, w.size() * sizeof(float),
+                         cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  for (uint32_t r = 0; r < n; ++r)
+    for (int k = 0; k < 3; ++k) {
+      out6[6 * r + k] = w[8 * r + k];
+      out6[6 * r + 3 + k] = w[8 * r + 4 + k];
+    }
 }
 
 void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) {
@@ -727,11 +813,20 @@ uint32_t Group::max_jacobi_iters() const {
   return mj;
 }
 
-void Group::grid_pass(int a, uint32_t max_jacobi, cudaStream_t st) {
+void Group::grid_pass(int a, uint32_t max_jacobi, bool rigid, cudaStream_t st) {
   const uint64_t total_cells = cells.high_water();
+  if (rigid) MPM_CK(cudaMemsetAsync(wrench_d.ptr, 0, wrench_d.bytes(), st));  // wrench of this substep only
   MPM_CK(launch_grid_update(pool(), block_scene.ptr, total_cells, a, 1, st));
   eng->launches += 1;
-  if (!max_jacobi) return;
+  if (max_jacobi) jacobi_pass(a, max_jacobi, st);
+  if (rigid) {
+    MPM_CK(launch_rigid_shell(pool(), block_scene.ptr, total_cells, a, st));
+    eng->launches += 1;
+  }
+}
+
+void Group::jacobi_pass(int a, uint32_t max_jacobi, cudaStream_t st) {
+  const uint64_t total_cells = cells.high_water();
   float4* bufs[2] = {vel.ptr, vel2.ptr};
   int cur = 0;
   for (uint32_t k = 0; k < max_jacobi; ++k) {
@@ -748,6 +843,7 @@ void Group::grid_pass(int a, uint32_t max_jacobi, cudaStream_t st) {
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   if (need_regroup || deterministic) regroup(true, st);
   const uint32_t max_jacobi = max_jacobi_iters();
+  const bool rigid = any_rigid();
   launch_gather_pass(kRecord, false, st);
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
@@ -755,7 +851,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   for (uint32_t s = 0; s < substeps; ++s) {
     ProfRec pr;
     eng->prof_begin(kStageGrid, st, &pr);
-    grid_pass(a, max_jacobi, st);
+    grid_pass(a, max_jacobi, rigid, st);
     eng->prof_end(&pr, st);
     const bool last = s + 1 == substeps;
     const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));

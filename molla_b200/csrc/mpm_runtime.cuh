@@ -116,6 +116,7 @@ struct SceneHost {
   uint64_t grid_len = 0;
   uint32_t key_off = 0;
   uint32_t tiles = 0;      // w^3
+  uint32_t n_rigid = 0;    // rigid spheres set on this scene
 };
 
 struct Range {
@@ -165,6 +166,9 @@ class Group {
   // grid pool
   DevBuf<float4> acc[2], vel;
   DevBuf<float4> vel2;  // semi-implicit Jacobi ping-pong (allocated when a scene needs it)
+  DevBuf<uint8_t> rigid_blocks;  // per 256-cell block: a rigid sphere may reach it
+  DevBuf<RigidDev> rigid_d;      // kMaxRigid per scene
+  DevBuf<float> wrench_d;        // 8 floats per sphere slot
   DevBuf<uint8_t> touched[2];  // per 256-cell block: acc[i] is nonzero there
   DevBuf<uint32_t> block_scene;
   // scenes
@@ -216,6 +220,13 @@ class Group {
   void set_scene_dt(uint32_t sid, float dt);
   void set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows);
   void set_scene_cfg(uint32_t sid, const mpm_config& cfg);
+  // set_rigid_spheres (mpm.rs:1521-1565): n spheres of 7 floats (center xyz,
+  // radius, velocity xyz) for scene sid; replaces the previous set.
+  void set_scene_rigid(uint32_t sid, const float* spheres, uint32_t n, cudaStream_t st);
+  // read_rigid_wrenches (mpm.rs:2908-2956): force xyz, torque xyz per sphere
+  // of the last substep.
+  void read_scene_wrench(uint32_t sid, float* out6, uint32_t n, cudaStream_t st);
+  bool any_rigid() const;
   void set_material_ids(uint32_t sid, const uint32_t* ids, uint32_t n);
 
   // Enqueue `substeps` substeps of every live scene on `st`.
@@ -225,7 +236,8 @@ class Group {
   void regroup(bool compute_keys, cudaStream_t st, bool move_records = false);
   // Grid update of accumulator a, then the semi-implicit Jacobi sweeps of
   // the scenes that ask for them.
-  void grid_pass(int a, uint32_t max_jacobi, cudaStream_t st);
+  void grid_pass(int a, uint32_t max_jacobi, bool rigid, cudaStream_t st);
+  void jacobi_pass(int a, uint32_t max_jacobi, cudaStream_t st);
   uint32_t max_jacobi_iters() const;
   // one item per occupied tile, plus one per kStageMax particles of a tile
   size_t max_item_count() const { return (size_t)key_space + cap / kStageMax + 2; }

@@ -244,6 +244,9 @@ typedef struct orc_scene {
   double svd_tol;        // 1e-7 in the reference
   uint32_t svd_sweeps;   // 16 in the reference
   uint32_t jacobi_iters; // MpmTimeStep::Implicit sweeps per substep (0: explicit)
+  uint32_t n_rigid;      // rigid spheres (set_rigid_spheres, mpm.rs:1521-1565)
+  float rigid[8][7];     // center xyz, radius, velocity xyz
+  double wrench[8][6];   // out: force xyz, torque xyz of the last substep
 } orc_scene;
 
 }  // extern "C"
@@ -363,6 +366,7 @@ template <class R> struct Grid {
   int n;
   std::vector<R> mass, mom;  // n^3, 3 n^3
   std::vector<R> vel;        // 3 n^3 (post grid_update)
+  std::vector<uint8_t> rigid;  // n^3: node stamped by a rigid sphere this substep
 };
 
 // The P2G body (mpm.wgsl:495-628 and :734-893): per-particle fixed-corotated
@@ -478,6 +482,7 @@ template <class R> static void grid_update(const Params<R>& p, Grid<R>& g, int n
         v[0] = g.mom[3 * c] / m;
         v[1] = g.mom[3 * c + 1] / m;
         v[2] = g.mom[3 * c + 2] / m;
+        if (!g.rigid.empty() && g.rigid[c]) continue;  // rigid-imprinted: no gravity, no walls
         v[1] = v[1] + p.dt * p.gy;
         const int pad = p.pad;
         const R f = p.friction;
@@ -493,6 +498,82 @@ template <class R> static void grid_update(const Params<R>& p, Grid<R>& g, int n
         if (iy >= n - pad) { v[1] = std::min(v[1], R(0)); v[0] = v[0] * f; v[2] = v[2] * f; }
         if (iz < pad) { v[2] = std::max(v[2], R(0)); v[0] = v[0] * f; v[1] = v[1] * f; }
         if (iz >= n - pad) { v[2] = std::min(v[2], R(0)); v[0] = v[0] * f; v[1] = v[1] * f; }
+      }
+}
+
+// rigid_imprint (mpm.wgsl:939-1003) for legacy spheres: a node inside the
+// first sphere that contains it takes the sphere velocity with the heavy
+// mass 1e6; its sand mass and momentum give the reaction -(m v - p) / dt
+// (dt floored at 1e-6) and its torque about the center.
+template <class R> static void rigid_imprint(orc_scene& sc, const Params<R>& p, Grid<R>& g) {
+  const int n = p.n;
+  const R o[3] = {p.ox, p.oy, p.oz};
+  const int win[3] = {p.wx, p.wy, p.wz};
+  for (int iz = 0; iz < n; ++iz)
+    for (int iy = 0; iy < n; ++iy)
+      for (int ix = 0; ix < n; ++ix) {
+        const size_t c = (size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz);
+        const int idx[3] = {ix, iy, iz};
+        R node[3];
+        for (int a = 0; a < 3; ++a) node[a] = o[a] + (R)(idx[a] + win[a]) * p.dx;
+        for (uint32_t r = 0; r < sc.n_rigid; ++r) {
+          const float* q = sc.rigid[r];
+          const R arm[3] = {node[0] - (R)q[0], node[1] - (R)q[1], node[2] - (R)q[2]};
+          if (!(std::sqrt(arm[0] * arm[0] + arm[1] * arm[1] + arm[2] * arm[2]) < (R)q[3])) continue;
+          const R m_old = g.mass[c];
+          const R mom_old[3] = {g.mom[3 * c], g.mom[3 * c + 1], g.mom[3 * c + 2]};
+          const R v[3] = {(R)q[4], (R)q[5], (R)q[6]};
+          const R stamp = R(1.0e6);
+          g.mass[c] = stamp;
+          for (int a = 0; a < 3; ++a) g.mom[3 * c + a] = stamp * v[a];
+          g.rigid[c] = 1;
+          if (m_old > R(1.0e-9)) {
+            const R inv_dt = R(1) / std::max(p.dt, R(1.0e-6));
+            R f[3];
+            for (int a = 0; a < 3; ++a) f[a] = -(m_old * v[a] - mom_old[a]) * inv_dt;
+            const R t[3] = {arm[1] * f[2] - arm[2] * f[1], arm[2] * f[0] - arm[0] * f[2], arm[0] * f[1] - arm[1] * f[0]};
+            for (int a = 0; a < 3; ++a) {
+              sc.wrench[r][a] += (double)f[a];
+              sc.wrench[r][3 + a] += (double)t[a];
+            }
+          }
+          break;
+        }
+      }
+}
+
+// mpm_rigid_force_integrate (mpm.wgsl:1175-1228): non-rigid nodes with sand
+// mass within radius + dx react with -(m w / dt) (v_sphere - v_node), w
+// tapered linearly over the outer cell.
+template <class R> static void rigid_shell(orc_scene& sc, const Params<R>& p, const Grid<R>& g) {
+  const int n = p.n;
+  const R o[3] = {p.ox, p.oy, p.oz};
+  const int win[3] = {p.wx, p.wy, p.wz};
+  for (int iz = 0; iz < n; ++iz)
+    for (int iy = 0; iy < n; ++iy)
+      for (int ix = 0; ix < n; ++ix) {
+        const size_t c = (size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz);
+        const R m = g.mass[c];
+        if (m <= R(1.0e-9) || !(m == m) || g.rigid[c]) continue;
+        const int idx[3] = {ix, iy, iz};
+        R node[3];
+        for (int a = 0; a < 3; ++a) node[a] = o[a] + (R)(idx[a] + win[a]) * p.dx;
+        for (uint32_t r = 0; r < sc.n_rigid; ++r) {
+          const float* q = sc.rigid[r];
+          const R arm[3] = {node[0] - (R)q[0], node[1] - (R)q[1], node[2] - (R)q[2]};
+          const R d = std::sqrt(arm[0] * arm[0] + arm[1] * arm[1] + arm[2] * arm[2]);
+          if (d > (R)q[3] + p.dx) continue;
+          R w = R(1);
+          if (d > (R)q[3]) w = std::max(R(0), R(1) - (d - (R)q[3]) / p.dx);
+          const R k = -(m * w / std::max(p.dt, R(1.0e-6)));
+          R f[3];
+          for (int a = 0; a < 3; ++a) f[a] = k * ((R)q[4 + a] - g.vel[3 * c + a]);
+          const R t[3] = {arm[1] * f[2] - arm[2] * f[1], arm[2] * f[0] - arm[0] * f[2], arm[0] * f[1] - arm[1] * f[0]};
+          for (int a = 0; a < 3; ++a) {
+            sc.wrench[r][a] += (double)f[a];
+            sc.wrench[r][3 + a] += (double)t[a];
+          }
+        }
       }
 }
 
@@ -513,7 +594,7 @@ template <class R> static void implicit_sweeps(const orc_scene& sc, const Params
           const R m = g.mass[c];
           const R* v = &g.vel[3 * c];
           R* o = &next[3 * c];
-          if (m <= R(1.0e-9) || !(m == m)) {
+          if (m <= R(1.0e-9) || !(m == m) || (!g.rigid.empty() && g.rigid[c])) {
             o[0] = v[0];
             o[1] = v[1];
             o[2] = v[2];
@@ -704,7 +785,7 @@ static bool plasticity_particle(const orc_scene& sc, const Params<R>& p, State<R
 // count (mpm.wgsl:1246).  Once the latch is set, later kernels are no-ops
 // (grid_valid(), mpm.wgsl:213-215).
 template <class R, class SR>
-static void step(const orc_scene& sc, State<R>& st, R* out_mass, R* out_mom, uint32_t* status, int substeps,
+static void step(orc_scene& sc, State<R>& st, R* out_mass, R* out_mom, uint32_t* status, int substeps,
                  int nthreads) {
   const Params<R> p = params_of<R>(sc);
   Grid<R> g;
@@ -713,8 +794,14 @@ static void step(const orc_scene& sc, State<R>& st, R* out_mass, R* out_mom, uin
   g.mass.assign(cells, R(0));
   g.mom.assign(3 * cells, R(0));
   g.vel.assign(3 * cells, R(0));
+  if (sc.n_rigid) g.rigid.assign(cells, 0);
   for (int s = 0; s < substeps; ++s) {
     if (status[0] != 0) break;
+    if (sc.n_rigid) {
+      std::fill(g.rigid.begin(), g.rigid.end(), (uint8_t)0);
+      for (uint32_t r = 0; r < sc.n_rigid; ++r)
+        for (int k = 0; k < 6; ++k) sc.wrench[r][k] = 0.0;
+    }
     {
       const long long nc = (long long)g.mass.size();
       R* gm = g.mass.data();
@@ -749,8 +836,10 @@ static void step(const orc_scene& sc, State<R>& st, R* out_mass, R* out_mom, uin
         });
       }
     }
+    if (sc.n_rigid) rigid_imprint(sc, p, g);
     grid_update(p, g, nthreads);
     if (sc.jacobi_iters) implicit_sweeps(sc, p, g, nthreads);
+    if (sc.n_rigid) rigid_shell(sc, p, g);
     status[1] += 1;
     bool fault = false;
     if (nthreads <= 1) {
@@ -794,7 +883,7 @@ extern "C" {
 // nthreads > 1 selects the OpenMP form (atomic accumulation; the timed CPU
 // baseline).  grid_mass/grid_mom (n^3 and 3 n^3) receive the last substep's
 // P2G result and may be null.
-int orc_step_f32(const orc_scene* sc, int n, float* pos, float* vel, float* C, float* F, float* mass,
+int orc_step_f32(orc_scene* sc, int n, float* pos, float* vel, float* C, float* F, float* mass,
                  float* vol, float* jp, const uint32_t* mat, float* grid_mass, float* grid_mom,
                  uint32_t* status, int substeps, int svd_fp64, int nthreads) {
   orc::State<float> st{n, pos, vel, C, F, mass, vol, jp, mat};
@@ -806,7 +895,7 @@ int orc_step_f32(const orc_scene* sc, int n, float* pos, float* vel, float* C, f
 }
 
 // FP64 everywhere (the accuracy reference).
-int orc_step_f64(const orc_scene* sc, int n, double* pos, double* vel, double* C, double* F, double* mass,
+int orc_step_f64(orc_scene* sc, int n, double* pos, double* vel, double* C, double* F, double* mass,
                  double* vol, double* jp, const uint32_t* mat, double* grid_mass, double* grid_mom,
                  uint32_t* status, int substeps, int nthreads) {
   orc::State<double> st{n, pos, vel, C, F, mass, vol, jp, mat};

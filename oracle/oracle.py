@@ -53,6 +53,9 @@ class orc_scene(C.Structure):
         ("svd_tol", C.c_double),
         ("svd_sweeps", C.c_uint32),
         ("jacobi_iters", C.c_uint32),
+        ("n_rigid", C.c_uint32),
+        ("rigid", (C.c_float * 7) * 8),
+        ("wrench", (C.c_double * 6) * 8),
     ]
 
 
@@ -201,6 +204,20 @@ def step(scene: orc_scene, st: dict, substeps: int, precision: str = "f32", nthr
     if want_grid:
         return gm, gp
     return None
+
+
+def set_rigid_spheres(scene: orc_scene, spheres):
+    """[(center_xyz, radius, velocity_xyz)] on the scene (at most 8)."""
+    scene.n_rigid = len(spheres)
+    for i, (c, r, v) in enumerate(spheres):
+        vals = [*c, r, *v]
+        for k in range(7):
+            scene.rigid[i][k] = float(vals[k])
+
+
+def rigid_wrenches(scene: orc_scene):
+    """[(force_xyz, torque_xyz)] of the last substep."""
+    return [(np.array(scene.wrench[i][:3]), np.array(scene.wrench[i][3:])) for i in range(scene.n_rigid)]
 
 
 def particle_order(scene: orc_scene, positions, count: int, capacity: int):

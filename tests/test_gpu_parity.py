@@ -358,6 +358,33 @@ def test_semi_implicit_preset_matches_oracle(engine):
     assert np.abs(sim.read_positions() - st2["pos"]).max() < 2e-5
 
 
+def test_rigid_spheres_match_oracle(engine):
+    """set_rigid_spheres / read_rigid_wrenches (mpm.rs:1521-1565, 2809) with
+    the imprint and shell reaction (mpm.wgsl:939-1003, 1175-1228) against the
+    oracle: positions and the last substep's wrench."""
+    cfg = m.MpmConfig.sand()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.5, 0.2], 10, 2)
+    spheres = [((0.0, 0.55, 0.0), 0.12, (0.0, -1.0, 0.0)), ((0.12, 0.42, 0.1), 0.06, (0.3, 0.0, -0.2))]
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_rigid_spheres(spheres)
+    sim.set_particles(pts)  # the spheres are kept across set_particles
+    sim.step_n(1.0 / 480, 10)
+    got = sim.read_rigid_wrenches()
+    sc = O.make_scene(cfg, [cfg.rheology], 1.0 / 480)
+    O.set_rigid_spheres(sc, spheres)
+    st = O.init_state(pts, mass=cfg.particle_mass, volume=cfg.particle_volume)
+    O.step(sc, st, 10)
+    ref = O.rigid_wrenches(sc)
+    assert np.abs(sim.read_positions() - st["pos"]).max() < 2e-5
+    assert len(got) == 2
+    for (gf, gt), (rf, rt) in zip(got, ref):
+        scale = max(np.abs(rf).max(), 1e-6)
+        assert np.abs(gf - rf).max() < 2e-3 * scale
+        assert np.abs(gt - rt).max() < 2e-3 * scale
+    with pytest.raises(m.MollaError):
+        sim.set_rigid_spheres([((0, 0, 0), 0.1, (0, 0, 0))] * (cfg.max_rigid + 1))
+
+
 def test_soil_checkpoint_round_trip_and_continuation(engine):
     """archive_drop_reload_preserves_all_history (mpm_checkpoint_tests.rs:176-257):
     a checkpoint of an evolved state restores bit for bit into a fresh

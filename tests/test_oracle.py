@@ -345,3 +345,39 @@ def test_implicit_sweeps_relax_a_velocity_jump():
         v = st["vel"][:, 0]
         jumps[iters] = v[pts[:, 1] > 0.45].mean() - v[pts[:, 1] <= 0.45].mean()
     assert 0.0 < jumps[3] < jumps[0]
+
+
+# ---- legacy rigid spheres (mpm.wgsl:939-1003, 1175-1228; mpm_oracle.rs:59-118) ----
+
+def test_rigid_imprint_wrench_of_a_particle_at_rest():
+    """rigid_cell_imprint_wrench: a sphere that covers the whole stencil of
+    a particle at rest takes its mass at the sphere velocity, so the force
+    on the sphere is -m v / dt and the particle leaves with v."""
+    cfg = m.MpmConfig.sand()
+    cfg.gravity_y = 0.0
+    dt = 1.0 / 480
+    sc = O.make_scene(cfg, [cfg.rheology], dt)
+    x = np.array([[0.013, 0.2, 0.017]], np.float32)
+    v = (0.4, -0.3, 0.2)
+    O.set_rigid_spheres(sc, [((0.013, 0.2, 0.017), 0.35, v)])
+    st = O.init_state(x, mass=cfg.particle_mass, volume=cfg.particle_volume)
+    O.step(sc, st, 1)
+    (force, torque), = O.rigid_wrenches(sc)
+    exp = -np.array(v) * np.float32(cfg.particle_mass) / np.float32(dt)
+    assert np.abs(force - exp).max() < 1e-4 * np.abs(exp).max()
+    assert np.abs(st["vel"][0] - np.array(v)).max() < 1e-5
+    # nodes symmetric about the particle within the sphere: torque small
+    assert np.abs(torque).max() < 0.05 * np.abs(exp).max()
+
+
+def test_rigid_sphere_pushes_sand_and_feels_it():
+    cfg = m.MpmConfig.sand()
+    pts = scenes.fill_box_lcg([-0.2, 0.3, -0.2], [0.2, 0.5, 0.2], 10, 2)
+    sc = O.make_scene(cfg, [cfg.rheology], 1.0 / 480)
+    O.set_rigid_spheres(sc, [((0.0, 0.55, 0.0), 0.12, (0.0, -1.0, 0.0))])
+    st = O.init_state(pts, mass=cfg.particle_mass, volume=cfg.particle_volume)
+    O.step(sc, st, 10)
+    (force, _), = O.rigid_wrenches(sc)
+    assert force[1] > 0.0  # sand resists the downward push
+    near = np.linalg.norm(st["pos"] - np.array([0.0, 0.55, 0.0]), axis=1) < 0.14
+    assert near.any() and st["vel"][near, 1].mean() < -0.1
