@@ -147,6 +147,9 @@ typedef struct mpm_server mpm_server;
 /* Engine::new_gpu (crates/molla-compute/src/engine.rs:140): binds a CUDA
  * device and creates the engine's stream.  `device` is the CUDA ordinal. */
 MPM_API int mpm_engine_create(int device, mpm_engine** out);
+/* Drops the caller's engine handle.  Simulations, groups and servers created
+ * from it keep the device stream alive until they are destroyed, so they may
+ * outlive the handle. */
 MPM_API int mpm_engine_destroy(mpm_engine* engine);
 /* Engine::check_device / DeviceHealth (engine.rs:70-119): MPM_ERR_GPU once a
  * device error was observed on this engine (sticky). */
@@ -242,6 +245,26 @@ MPM_API int mpm_read_rigid_wrenches(mpm_sim* sim, float* out, uint32_t cap, uint
  * min(count, cap) rows of 3 floats in the original particle order and
  * stores the particle count in *count_out. */
 MPM_API int mpm_read_positions(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
+/* particle_render_view (crates/molla-solvers/src/mpm_render_view.rs:20-44):
+ * live read-only rendering input on the simulation's device.  `positions`
+ * is a device buffer of float4 per particle (xyz in world metres, w = 0,
+ * 16-byte stride, original particle order); only the first `count` entries
+ * are live.  The buffer is the simulation's own and is re-packed on the
+ * engine's stream after every step, command batch and set_particles, so a
+ * draw queued on that stream after the physics sees that state.  The first
+ * call allocates capacity (max_particles) float4 and packs once; later calls
+ * allocate, launch and copy nothing.  `source` identifies the buffer
+ * (MpmParticleRenderSource): it stays the same across steps and reseeds of
+ * this simulation and differs between simulations.  Do not write to the
+ * buffer; it is freed with the simulation. */
+typedef struct mpm_render_view {
+  const void* positions;
+  uint32_t count;
+  uint32_t capacity;
+  uint64_t source;
+  uint64_t live_position_bytes;
+} mpm_render_view;
+MPM_API int mpm_particle_render_view(mpm_sim* sim, mpm_render_view* out);
 MPM_API int mpm_read_velocities(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
 /* Full particle state in original order: C[9n], F[9n] column-major, jp[n]
  * (any pointer may be NULL). */

@@ -27,7 +27,7 @@ from ._ffi import (MPM_ERR_BUSY, MPM_ERR_FAULT, MPM_ERR_GPU, MPM_ERR_INVALID, MP
 
 __all__ = [
     "Engine", "MpmConfig", "MpmRheology", "MpmTimeStep", "MpmSimulation", "PreparedMpmStep", "MpmCommandBatch",
-    "MpmActiveGridStats", "MpmGroup", "MpmServer", "MpmSimulation64", "MollaError", "SolverError", "GpuError",
+    "MpmActiveGridStats", "MpmParticleRenderView", "MpmParticleRenderSource", "MpmGroup", "MpmServer", "MpmSimulation64", "MollaError", "SolverError", "GpuError",
     "radix_sort_pairs", "blake3", "checkpoint_reencode",
     "MAX_MPM_MATERIALS", "library_path",
 ]
@@ -320,6 +320,67 @@ class MpmCommandBatch:
             pass
 
 
+class MpmParticleRenderSource:
+    """MpmParticleRenderSource (mpm_render_view.rs:14-16): binding identity
+    only; it does not freeze positions, count or physical time."""
+
+    def __init__(self, token: int):
+        self._token = int(token)
+
+    def __eq__(self, other):
+        return isinstance(other, MpmParticleRenderSource) and other._token == self._token
+
+    def __hash__(self):
+        return hash(self._token)
+
+    def __repr__(self):
+        return f"MpmParticleRenderSource({self._token})"
+
+
+class MpmParticleRenderView:
+    """MpmParticleRenderView (mpm_render_view.rs:3-36): live read-only
+    positions on the simulation's device, float4 per particle (xyz in world
+    metres, w = 0, 16-byte stride, original particle order); only the counted
+    prefix is live.  Queue reads on the engine's stream after the physics.
+    `__cuda_array_interface__` exposes the live prefix, so
+    `torch.as_tensor(view, device="cuda")` binds it without a copy.  The
+    interface's read-only flag is left clear because torch refuses it; the
+    buffer is read-only by contract (the next step overwrites it)."""
+
+    def __init__(self, raw: "_ffi.mpm_render_view", owner):
+        self._ptr = int(raw.positions or 0)
+        self._count = int(raw.count)
+        self._capacity = int(raw.capacity)
+        self._source = MpmParticleRenderSource(raw.source)
+        self._bytes = int(raw.live_position_bytes)
+        self._owner = owner  # keeps the simulation (and so the buffer) alive
+
+    def positions(self) -> int:
+        """Device address of the float4 position buffer."""
+        return self._ptr
+
+    def particle_count(self) -> int:
+        return self._count
+
+    @property
+    def capacity(self) -> int:
+        return self._capacity
+
+    def live_position_bytes(self) -> int:
+        return self._bytes
+
+    def source(self) -> MpmParticleRenderSource:
+        return self._source
+
+    def matches_source(self, source: MpmParticleRenderSource) -> bool:
+        return self._source == source
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self._count, 4), "typestr": "<f4", "data": (self._ptr if self._count else 0, False),
+                "version": 3, "strides": None, "stream": None}
+
+
 class MpmSimulation:
     """MpmSimulation (crates/molla-solvers/src/mpm.rs:695-2957) on the B200 path."""
 
@@ -432,6 +493,16 @@ class MpmSimulation:
 
     def read_positions(self) -> np.ndarray:
         return self._read3(_ffi.lib().mpm_read_positions)
+
+    def particle_render_view(self, engine=None) -> MpmParticleRenderView:
+        """particle_render_view (mpm_render_view.rs:38-56).  The first call
+        allocates the buffer and packs it once; later calls neither allocate
+        nor launch nor copy."""
+        if engine is not None and engine is not self.engine:
+            raise GpuError(MPM_ERR_INVALID, "particle render view requested on a foreign engine")
+        raw = _ffi.mpm_render_view()
+        _check(_ffi.lib().mpm_particle_render_view(self._h, C.byref(raw)))
+        return MpmParticleRenderView(raw, self)
 
     def read_velocities(self) -> np.ndarray:
         return self._read3(_ffi.lib().mpm_read_velocities)

@@ -85,6 +85,16 @@ class mpm_server_stats(C.Structure):
     ]
 
 
+class mpm_render_view(C.Structure):
+    _fields_ = [
+        ("positions", C.c_void_p),
+        ("count", C.c_uint32),
+        ("capacity", C.c_uint32),
+        ("source", C.c_uint64),
+        ("live_position_bytes", C.c_uint64),
+    ]
+
+
 class mpm_profile_stage(C.Structure):
     _fields_ = [("launches", C.c_uint64), ("total_ms", C.c_double)]
 
@@ -133,6 +143,7 @@ SIGNATURES = {
     "mpm_batch_submit": (I, [P]),
     "mpm_batch_cancel": (I, [P]),
     "mpm_read_positions": (I, [P, F32P, U32, U32P]),
+    "mpm_particle_render_view": (I, [P, C.POINTER(mpm_render_view)]),
     "mpm_read_velocities": (I, [P, F32P, U32, U32P]),
     "mpm_read_particle_state": (I, [P, F32P, F32P, F32P, U32, U32P]),
     "mpm_write_particle_state": (I, [P, F32P, F32P, F32P, U32]),

@@ -2,6 +2,7 @@
 // Each function maps library exceptions to status codes and records the
 // message for mpm_last_error on the calling thread.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -73,11 +74,15 @@ namespace mpm {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace mpm
 
+// The engine is shared by everything created from it: mpm_engine_destroy
+// drops the caller's reference, and the device stream goes away with the
+// last simulation, group or server that still uses it.
 struct mpm_engine {
-  std::unique_ptr<mpm::Engine> e;
+  std::shared_ptr<mpm::Engine> e;
 };
 
 struct mpm_sim {
+  std::shared_ptr<mpm::Engine> hold;  // first member: released after the group
   mpm::Engine* eng = nullptr;
   std::unique_ptr<mpm::Group> group;
   mpm_config cfg{};
@@ -93,6 +98,8 @@ struct mpm_sim {
   bool det_enabled = false;
   uint32_t sort_interval = 0;
   std::vector<float> spheres;  // rigid spheres, 7 floats each (kept across set_particles)
+  mpm::DevBuf<float4> render;  // render view positions (max_particles float4), allocated on first use
+  uint64_t render_source = 0;  // binding identity of `render`
   uint64_t epoch = 1;
   float dt = 1.0e-4f;
 
@@ -106,10 +113,16 @@ struct mpm_sim {
     group->sort_interval = interval;
   }
   void invalidate() { ++epoch; }
+  // Re-pack the render view after anything that moved particles, on the
+  // stream the physics ran on, so a draw queued after it sees this state.
+  void refresh_render(cudaStream_t st) {
+    if (render.ptr && sid != 0xffffffffu && count) group->pack_positions(sid, render.ptr, st);
+  }
 };
 
 // All-FP64 simulation (precision studies): FP64 state and grid.
 struct mpm_sim64 {
+  std::shared_ptr<mpm::Engine> hold;
   mpm::Engine* eng = nullptr;
   mpm_config cfg{};
   mpm::Scene64 sc{};
@@ -351,6 +364,7 @@ int mpm_sim_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim** out) {
     validate_config(*cfg);
     auto* s = new mpm_sim();
     try {
+      s->hold = engine->e;
       s->eng = engine->e.get();
       s->cfg = *cfg;
       const uint64_t n3 = (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
@@ -382,6 +396,7 @@ static void sim_reseed(mpm_sim* s, const float* xyz, const float* vel, uint32_t 
   s->apply_group_settings();
   if (!s->spheres.empty())
     s->group->set_scene_rigid(s->sid, s->spheres.data(), (uint32_t)(s->spheres.size() / 7), s->eng->stream);
+  s->refresh_render(s->eng->stream);
   s->invalidate();
 }
 
@@ -579,6 +594,7 @@ int mpm_step_n(mpm_sim* sim, float dt, uint32_t substeps) {
     sim->dt = dt;
     sim->group->set_scene_dt(sim->sid, dt);
     sim->group->step(substeps, sim->eng->stream);
+    sim->refresh_render(sim->eng->stream);
   });
 }
 
@@ -631,6 +647,7 @@ int mpm_batch_submit(mpm_batch* batch) {
       sim->group->set_scene_dt(sim->sid, w.first);
       sim->group->step_graph(w.second, 1, st);
     }
+    if (!batch->work.empty()) sim->refresh_render(st);
     if (ev) {
       MPM_CK(cudaEventRecord(ev, st));
       MPM_CK(cudaStreamWaitEvent(sim->eng->stream, ev, 0));
@@ -644,6 +661,24 @@ int mpm_batch_submit(mpm_batch* batch) {
 
 int mpm_batch_cancel(mpm_batch* batch) {
   return guard([&] { delete batch; });
+}
+
+int mpm_particle_render_view(mpm_sim* sim, mpm_render_view* out) {
+  static std::atomic<uint64_t> next_source{1};
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    sim->eng->check();
+    if (!sim->render.ptr) {
+      sim->render.alloc(std::max<uint32_t>(sim->cfg.max_particles, 1));
+      sim->render_source = next_source.fetch_add(1);
+      sim->refresh_render(sim->eng->stream);
+    }
+    out->positions = sim->render.ptr;
+    out->count = sim->count;
+    out->capacity = (uint32_t)sim->render.count;
+    out->source = sim->render_source;
+    out->live_position_bytes = 16ull * sim->count;
+  });
 }
 
 int mpm_read_positions(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out) {
@@ -823,6 +858,7 @@ int mpm_radix_sort_pairs_device(mpm_engine* engine, uint32_t* d_keys, uint32_t* 
 // ---- groups --------------------------------------------------------------------
 
 struct mpm_group {
+  std::shared_ptr<mpm::Engine> hold;
   mpm::Engine* eng;
   std::unique_ptr<mpm::Group> g;
 };
@@ -841,6 +877,7 @@ int mpm_group_create(mpm_engine* engine, uint32_t max_scenes, uint64_t max_parti
     engine->e->check();
     auto* h = new mpm_group();
     try {
+      h->hold = engine->e;
       h->eng = engine->e.get();
       h->g.reset(new mpm::Group(h->eng, max_scenes, max_particles_total, max_cells_total));
     } catch (...) {
@@ -1011,6 +1048,7 @@ double pct(std::vector<double> v, double q) {
 constexpr uint64_t kServerBytesPerParticle = 2ull * mpm::kPlanes * 4ull + 64ull + 44ull;
 
 struct mpm_server {
+  std::shared_ptr<mpm::Engine> hold;
   mpm::Engine* eng;
   std::unique_ptr<mpm::Group> g;
   uint64_t budget = 0;
@@ -1031,6 +1069,7 @@ int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t ma
     engine->e->check();
     auto* s = new mpm_server();
     try {
+      s->hold = engine->e;
       s->eng = engine->e.get();
       s->budget = hbm_budget_bytes;
       // Split the budget: particle pool 60% (two 27-plane buffers, the
@@ -1338,6 +1377,7 @@ int mpm_sim64_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim64** out)
             "the all-FP64 simulation runs the explicit step only");
     engine->e->check();
     auto s = std::make_unique<mpm_sim64>();
+    s->hold = engine->e;
     s->eng = engine->e.get();
     s->cfg = *cfg;
     mpm::Scene64& sc = s->sc;

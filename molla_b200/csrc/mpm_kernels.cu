@@ -441,6 +441,17 @@ __global__ void k_gather_xyz(PoolDev p, int first, const uint32_t* __restrict__ 
   out[3 * (size_t)i + 2] = plane(p, first + 2)[s];
 }
 
+// Render view (mpm_render_view.rs:20-44, position write mpm.wgsl:1349):
+// one scene's positions as float4 (xyz, w = 0) in identity order.  Coalesced
+// 16-byte stores; the plane reads follow slot_of.
+__global__ void k_pack_positions(PoolDev p, const uint32_t* __restrict__ slot_of, uint32_t id_base, uint32_t n,
+                                 float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = slot_of[id_base + i];
+  out[i] = make_float4(plane(p, PX)[s], plane(p, PX + 1)[s], plane(p, PX + 2)[s], 0.0f);
+}
+
 // Copy `count` planes starting at `first` into [n x count] rows in identity order.
 __global__ void k_gather_rows(PoolDev p, int first, int count, const uint32_t* __restrict__ slot_of,
                               uint32_t id_base, uint32_t n, float* __restrict__ out) {
@@ -588,6 +599,13 @@ cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_
                               float* out, cudaStream_t st) {
   if (!n) return cudaSuccess;
   k_gather_xyz<<<(n + 255) / 256, 256, 0, st>>>(p, first, slot_of, id_base, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_positions(const PoolDev& p, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
+                                  float4* out, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_pack_positions<<<(n + 255) / 256, 256, 0, st>>>(p, slot_of, id_base, n, out);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@ namespace mpm {
 constexpr int kParticleThreads = 256;
 constexpr int kGatherThreads = 128;
 constexpr int kScatterThreads = 192;  // 64 cells x 3 x-slabs of one tile
+constexpr int kFusedThreads = 256;    // fused gather + scatter: 2 CTAs of 128-register threads per SM
 constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 256-cell block
 
 enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
@@ -35,6 +36,11 @@ constexpr int kStageMax = 960;                   // particles per scatter item (
 constexpr int kStageBoxRows = 64;                // records per TMA box of the scatter stage
 // Persistent grid sizes (SMs x resident CTAs).
 int gather_grid_size(bool svd_fp64);
+// Fused gather + scatter of a non-final substep (k_g2p2g): gather with the B
+// record kept in shared memory, then the record deposit into acc[acc_out].
+cudaError_t launch_fused(bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps, int reuse,
+                         int acc_out, int grid, cudaStream_t st);
+int fused_grid_size(bool svd_fp64);
 int scatter_grid_size();
 cudaError_t launch_grid_update(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
                                int count_substep, cudaStream_t st);
@@ -65,6 +71,8 @@ cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene,
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
                          Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);
+cudaError_t launch_pack_positions(const PoolDev& p, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
+                                  float4* out, cudaStream_t st);
 cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
                               float* out, cudaStream_t st);
 cudaError_t launch_gather_rows(const PoolDev& p, int first, int count, const uint32_t* slot_of, uint32_t id_base,

@@ -16,10 +16,13 @@
 // around the tile in shared memory; the scatter stages the item's 64-byte
 // records with one bulk copy, bins them by their current base cell and
 // accumulates into an 8^3-node shared block that it flushes to HBM with one
-// float4 atomic per non-empty node.  They are separate kernels because the
-// gather (SVD, return mapping) needs ~128 registers per thread while the
-// scatter needs fewer: split, each runs at its own occupancy; the B record
-// costs HBM bandwidth the substep does not otherwise use.  The SVD computed
+// float4 atomic per non-empty node.  For large groups they are separate
+// kernels because the gather (SVD, return mapping) needs ~128 registers per
+// thread while the scatter needs fewer: split, each runs at its own
+// occupancy, and the B record's round trip through HBM is cheaper than the
+// fused kernel's lower occupancy.  For small groups (a few thousand items,
+// about one wave) the fused k_g2p2g keeps the records in shared memory and
+// saves a launch and a wave tail per substep.  The SVD computed
 // by the return mapping is reused for the next substep's stress; the first
 // substep of every step_n call runs a record-only gather that computes it
 // from F.
@@ -143,6 +146,264 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 }  // namespace
 
+// One particle of an item: G2P + F update + return mapping (MODE != kRecord)
+// and the scatter record (MODE != kG2P), returned in rec.  vblock is the
+// staged 8^3-node velocity block of the item's tile (origin node rx, ry, rz);
+// fallback is a 12-float shared-memory slot of this thread for gather_global.
+template <int MODE, bool WRITE_KEYS, class SR>
+__device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, uint32_t* status,
+                                              const float4* __restrict__ vblock, float* fallback, int rx, int ry,
+                                              int rz, int n, SR stol, int sweeps, int reuse_svd, float4 (&rec)[4]) {
+  constexpr bool kGather = MODE != kRecord;
+  constexpr bool kScatter = MODE != kG2P;
+  float x = plane(p, PX)[s], y = plane(p, PY)[s], z = plane(p, PZ)[s];
+  float F[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) F[i] = plane(p, F0 + i)[s];
+  float jp = plane(p, JP)[s];
+  const float mass = plane(p, MASS)[s];
+  const float vol = plane(p, VOL)[s];
+  const uint32_t mat = p.meta[s] & 7u;
+  float v[3], C[9];
+  bool ok = true;
+  SvdOut<SR> svd;
+  if constexpr (kGather) {
+    // ---- g2p (mpm.wgsl:1242-1353) ----
+    bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]);
+    const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+    fin = fin && finitef(xp[0]) && finitef(xp[1]) && finitef(xp[2]);
+    if (!fin) {
+      atomicOr(status, kFaultNumerical);
+      ok = false;
+    }
+    if (ok) {
+      float w[3][3], d[3][3];
+      int base[3];
+      const int win[3] = {sc.winx, sc.winy, sc.winz};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float bf = floorf(xp[a] - 0.5f);
+        base[a] = (int)bf - win[a];
+        const float fx = xp[a] - bf;
+        quad_weights(fx, w[a]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * sc.dx;
+      }
+      const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+      const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
+                          (unsigned)lz0 <= (unsigned)(kRegion - 3);
+      // Separable accumulation: v = sum w gv; G = sum (w gv) d^T.
+      float vs[3] = {0.f, 0.f, 0.f};
+      float G[9];
+      if (inside) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) G[i] = 0.f;
+        const float4* __restrict__ blk = &vblock[lx0 + 8 * ly0 + 64 * lz0];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          float si[3] = {0.f, 0.f, 0.f}, syi[3] = {0.f, 0.f, 0.f}, szi[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            float sj[3] = {0.f, 0.f, 0.f}, szj[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              const float4 g = blk[i + 8 * j + 64 * kk];
+              const float wk = w[2][kk];
+              sj[0] += wk * g.x;
+              sj[1] += wk * g.y;
+              sj[2] += wk * g.z;
+              const float wdk = wk * d[2][kk];
+              szj[0] += wdk * g.x;
+              szj[1] += wdk * g.y;
+              szj[2] += wdk * g.z;
+            }
+            const float wj = w[1][j];
+            const float wdj = wj * d[1][j];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              si[r] += wj * sj[r];
+              syi[r] += wdj * sj[r];
+              szi[r] += wj * szj[r];
+            }
+          }
+          const float wi = w[0][i];
+          const float wdi = wi * d[0][i];
+#pragma unroll
+          for (int r = 0; r < 3; ++r) {
+            vs[r] += wi * si[r];
+            G[r] += wdi * si[r];      // column x
+            G[3 + r] += wi * syi[r];  // column y
+            G[6 + r] += wi * szi[r];  // column z
+          }
+        }
+      } else {
+        float* slot = fallback;
+        gather_global(p.vel + sc.grid_off, n, xp[0], xp[1], xp[2], win[0], win[1], win[2], sc.dx, slot);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) vs[r] = slot[r];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) G[r] = slot[3 + r];
+      }
+      const float four_inv_dx2 = 4.0f * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) C[i] = four_inv_dx2 * G[i];
+      v[0] = vs[0];
+      v[1] = vs[1];
+      v[2] = vs[2];
+      const MatDev& md = sc.mat[mat];
+      if (md.rheo == 2) {
+        v[0] *= md.vfac;
+        v[1] *= md.vfac;
+        v[2] *= md.vfac;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) C[i] *= md.afac;
+      }
+      float np[3] = {x + sc.dt * v[0], y + sc.dt * v[1], z + sc.dt * v[2]};
+      bool fin2 = finitef(np[0]) && finitef(np[1]) && finitef(np[2]) && finitef(v[0]) && finitef(v[1]) &&
+                  finitef(v[2]);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) fin2 = fin2 && finitef(C[i]);
+      if (!fin2) {
+        atomicOr(status, kFaultNumerical);
+        ok = false;
+      }
+      if (ok) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          if (np[a] < sc.lo[a] || np[a] > sc.hi[a]) v[a] = 0.f;
+          np[a] = clampf(np[a], sc.lo[a], sc.hi[a]);
+        }
+        // F <- (I + dt C) F
+        float A[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) A[i] = sc.dt * C[i] + ((i % 4 == 0) ? 1.f : 0.f);
+        float Fn[9];
+        matmul(A, F, Fn);
+        bool fin3 = true;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) fin3 = fin3 && finitef(Fn[i]);
+        if (!fin3) {
+          atomicOr(status, kFaultNumerical);
+          ok = false;
+        } else {
+          x = np[0];
+          y = np[1];
+          z = np[2];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) F[i] = Fn[i];
+          // ---- plasticity (mpm.wgsl:1366-1479) on the updated F ----
+          SR Fs[9];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
+          svd3<SR>(Fs, svd, stol, sweeps);
+          float jp_new = jp;
+          bool changed = true;
+          if (plasticity_project<SR>(svd, md, jp_new, changed)) {
+            // FP32 mode rebuilds F = U s V^T every substep (the
+            // reference); the FP64-SVD mode keeps the trial F when
+            // the return mapping left every singular value unchanged.
+            SR Fr[9];
+            const bool rebuild = sizeof(SR) == 4 || changed;
+            if (rebuild) {
+              // F = U diag(s) V^T in the form's precision (U is FP32)
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                  Fr[3 * c + r] = ((SR)svd.u[r] * svd.s[0]) * svd.v[c] +
+                                  ((SR)svd.u[3 + r] * svd.s[1]) * svd.v[3 + c] +
+                                  ((SR)svd.u[6 + r] * svd.s[2]) * svd.v[6 + c];
+            }
+            bool fin4 = true;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) fin4 = fin4 && (!rebuild || finitef((float)Fr[i]));
+            if (fin4) {
+              if (rebuild) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
+              }
+              jp = jp_new;
+            } else {
+              atomicOr(status, kFaultNumerical);
+              ok = false;
+            }
+          } else {
+            atomicOr(status, kFaultNumerical);
+            ok = false;
+          }
+          // G2P results are published even when the return mapping
+          // faults (the reference's g2p and plasticity are separate
+          // dispatches); only the plasticity update is withheld.
+          plane(p, PX)[s] = x;
+          plane(p, PY)[s] = y;
+          plane(p, PZ)[s] = z;
+          plane(p, VX)[s] = v[0];
+          plane(p, VY)[s] = v[1];
+          plane(p, VZ)[s] = v[2];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) plane(p, C0 + i)[s] = C[i];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) plane(p, F0 + i)[s] = F[i];
+          plane(p, JP)[s] = jp;
+        }
+      }
+    }
+  } else {
+    // P2G-only: read v and C and validate the whole state (the
+    // reference's g2p checks, mpm.wgsl:1247-1255, moved to the first
+    // launch of the call so that a non-finite upload latches before
+    // anything moves).
+    v[0] = plane(p, VX)[s];
+    v[1] = plane(p, VY)[s];
+    v[2] = plane(p, VZ)[s];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) C[i] = plane(p, C0 + i)[s];
+    bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp) && finitef(v[0]) && finitef(v[1]) &&
+               finitef(v[2]) && finitef((x - sc.ox) * sc.inv_dx) && finitef((y - sc.oy) * sc.inv_dx) &&
+               finitef((z - sc.oz) * sc.inv_dx);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]) && finitef(C[i]);
+    if (!fin) {
+      atomicOr(status, kFaultNumerical);
+      ok = false;
+    }
+  }
+  if constexpr (kScatter) {
+    // B = m C + 4/dx^2 S for the next scatter (all-zero for a particle
+    // that faulted, which then deposits nothing).
+    float B[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) B[i] = 0.f;
+    if (ok) {
+      if (!kGather || !reuse_svd) {
+        SR Fs[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
+        svd3<SR>(Fs, svd, stol, sweeps);
+      }
+      p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
+    }
+    // Packed record (x, y, z, m), (m v, B0), (B1..B4), (B5..B8); a
+    // faulted particle gets m = 0 and deposits nothing.
+    const float mr = ok ? mass : 0.f;
+    const float vx = ok ? mass * v[0] : 0.f, vy = ok ? mass * v[1] : 0.f, vz = ok ? mass * v[2] : 0.f;
+    rec[0] = make_float4(x, y, z, mr);
+    rec[1] = make_float4(vx, vy, vz, B[0]);
+    rec[2] = make_float4(B[1], B[2], B[3], B[4]);
+    rec[3] = make_float4(B[5], B[6], B[7], B[8]);
+  }
+  if constexpr (WRITE_KEYS) {
+    const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+    const int win[3] = {sc.winx, sc.winy, sc.winz};
+    int nbase[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nbase[a] = (xp[a] == xp[a]) ? (int)floorf(xp[a] - 0.5f) - win[a] : 0;
+    p.keys_by_id[p.orig[s]] = base_key(sc, nbase);
+  }
+}
+
 // MODE: kRecord (no gather: validate the state and compute B from the SVD of
 // F — the first substep of a call), kG2P (gather + return mapping, the last
 // substep of a call), kG2PRecord (gather + return mapping + B for the next
@@ -188,252 +449,15 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
     if (!faulted) {
       for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
         const uint32_t s = item.start + k;
-        float x = plane(p, PX)[s], y = plane(p, PY)[s], z = plane(p, PZ)[s];
-        float F[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) F[i] = plane(p, F0 + i)[s];
-        float jp = plane(p, JP)[s];
-        const float mass = plane(p, MASS)[s];
-        const float vol = plane(p, VOL)[s];
-        const uint32_t mat = p.meta[s] & 7u;
-        float v[3], C[9];
-        bool ok = true;
-        SvdOut<SR> svd;
-        if constexpr (kGather) {
-          // ---- g2p (mpm.wgsl:1242-1353) ----
-          bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp);
-#pragma unroll
-          for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]);
-          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
-          fin = fin && finitef(xp[0]) && finitef(xp[1]) && finitef(xp[2]);
-          if (!fin) {
-            atomicOr(status, kFaultNumerical);
-            ok = false;
-          }
-          if (ok) {
-            float w[3][3], d[3][3];
-            int base[3];
-            const int win[3] = {sc.winx, sc.winy, sc.winz};
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              const float bf = floorf(xp[a] - 0.5f);
-              base[a] = (int)bf - win[a];
-              const float fx = xp[a] - bf;
-              quad_weights(fx, w[a]);
-#pragma unroll
-              for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * sc.dx;
-            }
-            const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
-            const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
-                                (unsigned)lz0 <= (unsigned)(kRegion - 3);
-            // Separable accumulation: v = sum w gv; G = sum (w gv) d^T.
-            float vs[3] = {0.f, 0.f, 0.f};
-            float G[9];
-            if (inside) {
-#pragma unroll
-              for (int i = 0; i < 9; ++i) G[i] = 0.f;
-              const float4* __restrict__ blk = &s_gath.vel[lx0 + 8 * ly0 + 64 * lz0];
-#pragma unroll
-              for (int i = 0; i < 3; ++i) {
-                float si[3] = {0.f, 0.f, 0.f}, syi[3] = {0.f, 0.f, 0.f}, szi[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                  float sj[3] = {0.f, 0.f, 0.f}, szj[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                  for (int kk = 0; kk < 3; ++kk) {
-                    const float4 g = blk[i + 8 * j + 64 * kk];
-                    const float wk = w[2][kk];
-                    sj[0] += wk * g.x;
-                    sj[1] += wk * g.y;
-                    sj[2] += wk * g.z;
-                    const float wdk = wk * d[2][kk];
-                    szj[0] += wdk * g.x;
-                    szj[1] += wdk * g.y;
-                    szj[2] += wdk * g.z;
-                  }
-                  const float wj = w[1][j];
-                  const float wdj = wj * d[1][j];
-#pragma unroll
-                  for (int r = 0; r < 3; ++r) {
-                    si[r] += wj * sj[r];
-                    syi[r] += wdj * sj[r];
-                    szi[r] += wj * szj[r];
-                  }
-                }
-                const float wi = w[0][i];
-                const float wdi = wi * d[0][i];
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                  vs[r] += wi * si[r];
-                  G[r] += wdi * si[r];      // column x
-                  G[3 + r] += wi * syi[r];  // column y
-                  G[6 + r] += wi * szi[r];  // column z
-                }
-              }
-            } else {
-              float* slot = s_gath.fallback[threadIdx.x];
-              gather_global(p.vel + sc.grid_off, n, xp[0], xp[1], xp[2], win[0], win[1], win[2], sc.dx, slot);
-#pragma unroll
-              for (int r = 0; r < 3; ++r) vs[r] = slot[r];
-#pragma unroll
-              for (int r = 0; r < 9; ++r) G[r] = slot[3 + r];
-            }
-            const float four_inv_dx2 = 4.0f * sc.inv_dx * sc.inv_dx;
-#pragma unroll
-            for (int i = 0; i < 9; ++i) C[i] = four_inv_dx2 * G[i];
-            v[0] = vs[0];
-            v[1] = vs[1];
-            v[2] = vs[2];
-            const MatDev& md = sc.mat[mat];
-            if (md.rheo == 2) {
-              v[0] *= md.vfac;
-              v[1] *= md.vfac;
-              v[2] *= md.vfac;
-#pragma unroll
-              for (int i = 0; i < 9; ++i) C[i] *= md.afac;
-            }
-            float np[3] = {x + sc.dt * v[0], y + sc.dt * v[1], z + sc.dt * v[2]};
-            bool fin2 = finitef(np[0]) && finitef(np[1]) && finitef(np[2]) && finitef(v[0]) && finitef(v[1]) &&
-                        finitef(v[2]);
-#pragma unroll
-            for (int i = 0; i < 9; ++i) fin2 = fin2 && finitef(C[i]);
-            if (!fin2) {
-              atomicOr(status, kFaultNumerical);
-              ok = false;
-            }
-            if (ok) {
-#pragma unroll
-              for (int a = 0; a < 3; ++a) {
-                if (np[a] < sc.lo[a] || np[a] > sc.hi[a]) v[a] = 0.f;
-                np[a] = clampf(np[a], sc.lo[a], sc.hi[a]);
-              }
-              // F <- (I + dt C) F
-              float A[9];
-#pragma unroll
-              for (int i = 0; i < 9; ++i) A[i] = sc.dt * C[i] + ((i % 4 == 0) ? 1.f : 0.f);
-              float Fn[9];
-              matmul(A, F, Fn);
-              bool fin3 = true;
-#pragma unroll
-              for (int i = 0; i < 9; ++i) fin3 = fin3 && finitef(Fn[i]);
-              if (!fin3) {
-                atomicOr(status, kFaultNumerical);
-                ok = false;
-              } else {
-                x = np[0];
-                y = np[1];
-                z = np[2];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) F[i] = Fn[i];
-                // ---- plasticity (mpm.wgsl:1366-1479) on the updated F ----
-                SR Fs[9];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
-                svd3<SR>(Fs, svd, stol, sweeps);
-                float jp_new = jp;
-                bool changed = true;
-                if (plasticity_project<SR>(svd, md, jp_new, changed)) {
-                  // FP32 mode rebuilds F = U s V^T every substep (the
-                  // reference); the FP64-SVD mode keeps the trial F when
-                  // the return mapping left every singular value unchanged.
-                  SR Fr[9];
-                  const bool rebuild = sizeof(SR) == 4 || changed;
-                  if (rebuild) {
-                    // F = U diag(s) V^T in the form's precision (U is FP32)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-#pragma unroll
-                      for (int r = 0; r < 3; ++r)
-                        Fr[3 * c + r] = ((SR)svd.u[r] * svd.s[0]) * svd.v[c] +
-                                        ((SR)svd.u[3 + r] * svd.s[1]) * svd.v[3 + c] +
-                                        ((SR)svd.u[6 + r] * svd.s[2]) * svd.v[6 + c];
-                  }
-                  bool fin4 = true;
-#pragma unroll
-                  for (int i = 0; i < 9; ++i) fin4 = fin4 && (!rebuild || finitef((float)Fr[i]));
-                  if (fin4) {
-                    if (rebuild) {
-#pragma unroll
-                      for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
-                    }
-                    jp = jp_new;
-                  } else {
-                    atomicOr(status, kFaultNumerical);
-                    ok = false;
-                  }
-                } else {
-                  atomicOr(status, kFaultNumerical);
-                  ok = false;
-                }
-                // G2P results are published even when the return mapping
-                // faults (the reference's g2p and plasticity are separate
-                // dispatches); only the plasticity update is withheld.
-                plane(p, PX)[s] = x;
-                plane(p, PY)[s] = y;
-                plane(p, PZ)[s] = z;
-                plane(p, VX)[s] = v[0];
-                plane(p, VY)[s] = v[1];
-                plane(p, VZ)[s] = v[2];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) plane(p, C0 + i)[s] = C[i];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) plane(p, F0 + i)[s] = F[i];
-                plane(p, JP)[s] = jp;
-              }
-            }
-          }
-        } else {
-          // P2G-only: read v and C and validate the whole state (the
-          // reference's g2p checks, mpm.wgsl:1247-1255, moved to the first
-          // launch of the call so that a non-finite upload latches before
-          // anything moves).
-          v[0] = plane(p, VX)[s];
-          v[1] = plane(p, VY)[s];
-          v[2] = plane(p, VZ)[s];
-#pragma unroll
-          for (int i = 0; i < 9; ++i) C[i] = plane(p, C0 + i)[s];
-          bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp) && finitef(v[0]) && finitef(v[1]) &&
-                     finitef(v[2]) && finitef((x - sc.ox) * sc.inv_dx) && finitef((y - sc.oy) * sc.inv_dx) &&
-                     finitef((z - sc.oz) * sc.inv_dx);
-#pragma unroll
-          for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]) && finitef(C[i]);
-          if (!fin) {
-            atomicOr(status, kFaultNumerical);
-            ok = false;
-          }
-        }
+        float4 rec[4];
+        particle_step<MODE, WRITE_KEYS, SR>(p, sc, s, status, s_gath.vel, s_gath.fallback[threadIdx.x], rx, ry, rz, n,
+                                            stol, sweeps, reuse_svd, rec);
         if constexpr (kScatter) {
-          // B = m C + 4/dx^2 S for the next scatter (all-zero for a particle
-          // that faulted, which then deposits nothing).
-          float B[9];
-#pragma unroll
-          for (int i = 0; i < 9; ++i) B[i] = 0.f;
-          if (ok) {
-            if (!kGather || !reuse_svd) {
-              SR Fs[9];
-#pragma unroll
-              for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
-              svd3<SR>(Fs, svd, stol, sweeps);
-            }
-            p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
-          }
-          // Packed record (x, y, z, m), (m v, B0), (B1..B4), (B5..B8); a
-          // faulted particle gets m = 0 and deposits nothing.
-          const float mr = ok ? mass : 0.f;
-          const float vx = ok ? mass * v[0] : 0.f, vy = ok ? mass * v[1] : 0.f, vz = ok ? mass * v[2] : 0.f;
           float4* r4 = reinterpret_cast<float4*>(p.rec) + 4 * (size_t)s;
-          r4[0] = make_float4(x, y, z, mr);
-          r4[1] = make_float4(vx, vy, vz, B[0]);
-          r4[2] = make_float4(B[1], B[2], B[3], B[4]);
-          r4[3] = make_float4(B[5], B[6], B[7], B[8]);
-        }
-        if constexpr (WRITE_KEYS) {
-          const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
-          const int win[3] = {sc.winx, sc.winy, sc.winz};
-          int nbase[3];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) nbase[a] = (xp[a] == xp[a]) ? (int)floorf(xp[a] - 0.5f) - win[a] : 0;
-          p.keys_by_id[p.orig[s]] = base_key(sc, nbase);
+          r4[0] = rec[0];
+          r4[1] = rec[1];
+          r4[2] = rec[2];
+          r4[3] = rec[3];
         }
       }
     }
@@ -503,11 +527,239 @@ __device__ __noinline__ void deposit_global(float4 r0, float4 r1, float4 r2, flo
 }
 
 constexpr int kLocalCells = 216;  // 6^3 base cells whose stencils fit the 8^3 block
-constexpr int kBinRounds = (kStageMax + kScatterThreads - 1) / kScatterThreads;
 
 // 16-byte chunk k of staged record j under the 64-byte swizzle.
 __device__ __forceinline__ float4 stage_chunk(const float4* stage, uint32_t j, uint32_t k) {
   return stage[4 * j + (k ^ ((j >> 1) & 3u))];
+}
+__device__ __forceinline__ void stage_store(float4* stage, uint32_t j, const float4 (&rec)[4]) {
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) stage[4 * j + (k ^ ((j >> 1) & 3u))] = rec[k];
+}
+
+// Where an item's scatter lands: its scene's lattice and grid block, and the
+// 8^3-node block origin (rx, ry, rz) of its tile.
+struct ItemFrame {
+  float ox, oy, oz, inv_dx, dx;
+  int wx, wy, wz, rx, ry, rz, n;
+  uint64_t grid_off;
+  float4* acc;
+  uint8_t* touched;
+};
+
+__device__ __forceinline__ ItemFrame item_frame(const SceneDev& sc, const Item& item, float4* acc, uint8_t* touched) {
+  ItemFrame f;
+  f.ox = sc.ox;
+  f.oy = sc.oy;
+  f.oz = sc.oz;
+  f.inv_dx = sc.inv_dx;
+  f.dx = sc.dx;
+  f.wx = sc.winx;
+  f.wy = sc.winy;
+  f.wz = sc.winz;
+  const uint32_t w = sc.w;
+  const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
+  f.rx = 4 * (int)tx - 1;
+  f.ry = 4 * (int)ty - 1;
+  f.rz = 4 * (int)tz - 1;
+  f.n = (int)sc.n;
+  f.grid_off = sc.grid_off;
+  f.acc = acc;
+  f.touched = touched;
+  return f;
+}
+
+// Shared-memory working set of one scatter item.
+struct ScatterShared {
+  float acc[4][kRegionFloats];  // the 8^3-node block: m, p.x, p.y, p.z
+  uint32_t cell[kLocalCells];   // counts, then exclusive starts
+  uint16_t idx[kStageMax];      // item records sorted by local cell
+  uint32_t total;
+};
+
+// Scatter step 2 (bin) for a CTA of T threads: every staged record is binned
+// by its current base cell among the 6^3 local cells (counting sort with
+// warp-aggregated counters); one whose stencil leaves the block deposits
+// straight to HBM.  Ends with a barrier after which cell[] holds exclusive
+// starts and idx[] the sorted record indices.
+template <int T>
+__device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bool live, const ItemFrame& f,
+                                         ScatterShared& ss) {
+  constexpr int kRounds = (kStageMax + T - 1) / T;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t bin[kRounds];  // local cell << 16 | rank, or 0xffffffff
+#pragma unroll
+  for (int q = 0; q < kRounds; ++q) {
+    const uint32_t j = threadIdx.x + q * T;
+    uint32_t lc = 0xffffu;
+    if (live && j < count) {
+      const float4 r0 = stage_chunk(stage, j, 0);
+      if (r0.w != 0.f) {
+        const int lx = (int)floorf((r0.x - f.ox) * f.inv_dx - 0.5f) - f.wx - f.rx;
+        const int ly = (int)floorf((r0.y - f.oy) * f.inv_dx - 0.5f) - f.wy - f.ry;
+        const int lz = (int)floorf((r0.z - f.oz) * f.inv_dx - 0.5f) - f.wz - f.rz;
+        if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
+          lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
+        } else {
+          deposit_global(r0, stage_chunk(stage, j, 1), stage_chunk(stage, j, 2), stage_chunk(stage, j, 3), f.acc,
+                         f.touched, f.grid_off, f.n, f.ox, f.oy, f.oz, f.inv_dx, f.dx, f.wx, f.wy, f.wz);
+        }
+      }
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, lc);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lc != 0xffffu && lane == leader) base = atomicAdd(&ss.cell[lc], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    bin[q] = lc == 0xffffu ? 0xffffffffu : (lc << 16) | (base + __popc(peers & ((1u << lane) - 1u)));
+  }
+  __syncthreads();
+  // exclusive scan of the 216 cell counts (warp 0, 7 cells per lane)
+  if (threadIdx.x < 32) {
+    uint32_t c[7], sum = 0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const int cell = (int)lane * 7 + k;
+      c[k] = cell < kLocalCells ? ss.cell[cell] : 0u;
+      sum += c[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const int cell = (int)lane * 7 + k;
+      if (cell < kLocalCells) ss.cell[cell] = run;
+      run += c[k];
+    }
+    if (lane == 31) ss.total = incl;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < kRounds; ++q) {
+    if (bin[q] != 0xffffffffu) ss.idx[ss.cell[bin[q] >> 16] + (bin[q] & 0xffffu)] = (uint16_t)(threadIdx.x + q * T);
+  }
+  __syncthreads();
+}
+
+// Scatter step 3 (deposit) for a CTA of T >= 192 threads.  Thread t < 192
+// takes x-slab t / 64 of the stencil and one of the tile's own 64 cells, in
+// the order of their particle counts at the regrouping (`order`), so that the
+// lanes of a warp walk lists of similar length; then all T threads share the
+// (margin cell, slab) pairs of the cells particles moved into.  A thread adds
+// the nine slab nodes of its cell's particles in registers and issues 9 x 4
+// shared-memory atomics for the whole cell; the lanes of a warp own
+// different cells, so those atomics do not collide.
+template <int T>
+__device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t* __restrict__ order, const ItemFrame& f,
+                                             ScatterShared& ss) {
+  static_assert(T >= 192, "the core cells take 3 x 64 threads");
+  const uint32_t total = ss.total;
+  float am[9], apx[9], apy[9], apz[9];
+  // Accumulates slab `slab` of the particles of local cell lc in registers;
+  // returns whether it had any.
+  auto accumulate = [&](int lc, int slab) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
+    const uint32_t first = ss.cell[lc], end = lc == kLocalCells - 1 ? total : ss.cell[lc + 1];
+    for (uint32_t t = first; t < end; ++t) {
+      const uint32_t j = ss.idx[t];
+      const float4 r0 = stage_chunk(stage, j, 0), r1 = stage_chunk(stage, j, 1), r2 = stage_chunk(stage, j, 2),
+                   r3 = stage_chunk(stage, j, 3);
+      const float mass = r0.w;
+      const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+      const float xp[3] = {(r0.x - f.ox) * f.inv_dx, (r0.y - f.oy) * f.inv_dx, (r0.z - f.oz) * f.inv_dx};
+      float wgt[3][3], fx[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float bf = floorf(xp[a] - 0.5f);
+        fx[a] = xp[a] - bf;
+        quad_weights(fx[a], wgt[a]);
+      }
+      // slab i of the stencil: x offset i, all (j, k)
+      const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
+      const float di = ((float)slab - fx[0]) * f.dx;
+      const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float wij = wi * wgt[1][j];
+        const float dj = ((float)j - fx[1]) * f.dx;
+        const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          const float wt = wij * wgt[2][kk];
+          const float dk = ((float)kk - fx[2]) * f.dx;
+          am[3 * j + kk] += wt * mass;
+          apx[3 * j + kk] += wt * (qy[0] + B[6] * dk);
+          apy[3 * j + kk] += wt * (qy[1] + B[7] * dk);
+          apz[3 * j + kk] += wt * (qy[2] + B[8] * dk);
+        }
+      }
+    }
+    return end > first;
+  };
+  // Adds the accumulated slab of local cell lc to the shared block.
+  auto flush = [&](int lc, int slab) {
+    const int r0 = region_index(lc % 6, (lc / 6) % 6, lc / 36) + slab;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int kk = 0; kk < 3; ++kk) {
+        const int r = r0 + kRsy * j + kRsz * kk;
+        atomicAdd(&ss.acc[0][r], am[3 * j + kk]);
+        atomicAdd(&ss.acc[1][r], apx[3 * j + kk]);
+        atomicAdd(&ss.acc[2][r], apy[3 * j + kk]);
+        atomicAdd(&ss.acc[3][r], apz[3 * j + kk]);
+      }
+  };
+  if (threadIdx.x < 192) {
+    const int slab = (int)(threadIdx.x >> 6);
+    const uint32_t c = order[threadIdx.x & 63u];
+    const int lc = (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
+    if (accumulate(lc, slab)) flush(lc, slab);
+  }
+#pragma unroll 1
+  for (int u = (int)threadIdx.x; u < 3 * kLocalCells; u += T) {
+    const int lc = u % kLocalCells, slab = u / kLocalCells;
+    const int lx = lc % 6, ly = (lc / 6) % 6, lz = lc / 36;
+    const bool core = lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4;
+    if (!core && accumulate(lc, slab)) flush(lc, slab);
+  }
+}
+
+// Scatter step 4 (flush): every non-empty node of the 8^3 block goes to HBM
+// with one float4 atomic and is cleared for the next item, as are the cell
+// counters.  The caller synchronises before the block is reused.
+template <int T>
+__device__ __forceinline__ void flush_item(const ItemFrame& f, ScatterShared& ss) {
+  for (int r = threadIdx.x; r < kRegionNodes; r += T) {
+    const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
+    const int q = region_index(lx, ly, lz);
+    const float m = ss.acc[0][q], px = ss.acc[1][q], py = ss.acc[2][q], pz = ss.acc[3][q];
+    if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
+      ss.acc[0][q] = 0.f;
+      ss.acc[1][q] = 0.f;
+      ss.acc[2][q] = 0.f;
+      ss.acc[3][q] = 0.f;
+      const int ix = f.rx + lx, iy = f.ry + ly, iz = f.rz + lz;
+      if ((unsigned)ix < (unsigned)f.n && (unsigned)iy < (unsigned)f.n && (unsigned)iz < (unsigned)f.n) {
+        const uint64_t c =
+            f.grid_off + (uint64_t)ix + (uint64_t)f.n * ((uint64_t)iy + (uint64_t)f.n * (uint64_t)iz);
+        atomicAdd(&f.acc[c], make_float4(m, px, py, pz));
+        touch(f.touched, c);
+      }
+    }
+  }
+  for (int r = threadIdx.x; r < kLocalCells; r += T) ss.cell[r] = 0u;
+}
+
+__device__ __forceinline__ void clear_scatter_shared(ScatterShared& ss, int threads) {
+  for (int r = threadIdx.x; r < 4 * kRegionFloats; r += threads) (&ss.acc[0][0])[r] = 0.f;
+  for (int r = threadIdx.x; r < kLocalCells; r += threads) ss.cell[r] = 0u;
 }
 
 __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __grid_constant__ CUtensorMap rec_map,
@@ -516,19 +768,12 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __g
   // the swizzle pattern repeats every 512 bytes: align the stage to 1 KiB
   float4* s_stage =
       reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~static_cast<uintptr_t>(1023u));
-  __shared__ float s_acc[4][kRegionFloats];
-  __shared__ uint32_t s_cell[kLocalCells];  // counts, then exclusive starts
-  __shared__ uint16_t s_idx[kStageMax];     // item particles sorted by local cell
-  __shared__ uint32_t s_total;
+  __shared__ ScatterShared ss;
   __shared__ __align__(8) uint64_t s_bar;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
   const uint32_t n_items = *p.n_items;
-  const int slab = threadIdx.x >> 6;
-  const uint32_t lane64 = threadIdx.x & 63u;
-  const uint32_t lane = threadIdx.x & 31u;
-  for (int r = threadIdx.x; r < 4 * kRegionFloats; r += blockDim.x) (&s_acc[0][0])[r] = 0.f;
-  for (int r = threadIdx.x; r < kLocalCells; r += blockDim.x) s_cell[r] = 0u;
+  clear_scatter_shared(ss, kScatterThreads);
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
     fence_mbar_init();
@@ -557,13 +802,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __g
     // A fault latched before this launch freezes the scene; one latched by
     // this substep's gather is handled per particle (m = 0 in its record).
     const uint32_t fault0 = *(volatile uint32_t*)status;
-    const uint32_t w = scp->w;
-    const int n = (int)scp->n;
-    const float ox = scp->ox, oy = scp->oy, oz = scp->oz, inv_dx = scp->inv_dx, dx = scp->dx;
-    const int win[3] = {scp->winx, scp->winy, scp->winz};
-    const uint64_t grid_off = scp->grid_off;
-    const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
-    const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
+    const ItemFrame f = item_frame(*scp, item, acc, touched);
     const bool staged = item.count - 1u < (uint32_t)kStageMax;
     bool ok = staged;
     if (staged) {
@@ -571,141 +810,8 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __g
       parity ^= 1u;
     }
     const bool live = ok && fault0 == 0;
-    // ---- 2. bin by current base cell (rank within the cell from the
-    //         warp-aggregated counter) ----
-    uint32_t bin[kBinRounds];  // local cell << 16 | rank, or 0xffffffff
-#pragma unroll
-    for (int q = 0; q < kBinRounds; ++q) {
-      const uint32_t j = threadIdx.x + q * kScatterThreads;
-      uint32_t lc = 0xffffu;
-      if (live && j < item.count) {
-        const float4 r0 = stage_chunk(s_stage, j, 0);
-        if (r0.w != 0.f) {
-          const int lx = (int)floorf((r0.x - ox) * inv_dx - 0.5f) - win[0] - rx;
-          const int ly = (int)floorf((r0.y - oy) * inv_dx - 0.5f) - win[1] - ry;
-          const int lz = (int)floorf((r0.z - oz) * inv_dx - 0.5f) - win[2] - rz;
-          if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
-            lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
-          } else {
-            deposit_global(r0, stage_chunk(s_stage, j, 1), stage_chunk(s_stage, j, 2), stage_chunk(s_stage, j, 3), acc,
-                           touched, grid_off, n, ox, oy, oz, inv_dx, dx, win[0], win[1], win[2]);
-          }
-        }
-      }
-      const uint32_t peers = __match_any_sync(0xffffffffu, lc);
-      const uint32_t leader = __ffs(peers) - 1;
-      uint32_t base = 0;
-      if (lc != 0xffffu && lane == leader) base = atomicAdd(&s_cell[lc], (uint32_t)__popc(peers));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      bin[q] = lc == 0xffffu ? 0xffffffffu : (lc << 16) | (base + __popc(peers & ((1u << lane) - 1u)));
-    }
-    __syncthreads();
-    // exclusive scan of the 216 cell counts (warp 0, 7 cells per lane)
-    if (threadIdx.x < 32) {
-      uint32_t c[7], sum = 0;
-#pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const int cell = (int)lane * 7 + k;
-        c[k] = cell < kLocalCells ? s_cell[cell] : 0u;
-        sum += c[k];
-      }
-      uint32_t incl = sum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += y;
-      }
-      uint32_t run = incl - sum;
-#pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const int cell = (int)lane * 7 + k;
-        if (cell < kLocalCells) s_cell[cell] = run;
-        run += c[k];
-      }
-      if (lane == 31) s_total = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kBinRounds; ++q) {
-      if (bin[q] != 0xffffffffu)
-        s_idx[s_cell[bin[q] >> 16] + (bin[q] & 0xffffu)] = (uint16_t)(threadIdx.x + q * kScatterThreads);
-    }
-    __syncthreads();
-    // ---- 3. deposit: one cell per lane, the tile's own 64 cells first in the
-    //         order of their counts at the regrouping (so the lanes of a warp
-    //         walk lists of similar length), then the margin cells that
-    //         particles moved into ----
-    if (live) {
-      const uint32_t total = s_total;
-      float am[9], apx[9], apy[9], apz[9];
-      // Accumulates the particles of local cell lc in registers; returns
-      // whether it had any.
-      auto accumulate = [&](int lc) {
-#pragma unroll
-        for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
-        const uint32_t first = s_cell[lc], end = lc == kLocalCells - 1 ? total : s_cell[lc + 1];
-        for (uint32_t t = first; t < end; ++t) {
-          const uint32_t j = s_idx[t];
-          const float4 r0 = stage_chunk(s_stage, j, 0), r1 = stage_chunk(s_stage, j, 1),
-                       r2 = stage_chunk(s_stage, j, 2), r3 = stage_chunk(s_stage, j, 3);
-          const float mass = r0.w;
-          const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
-          const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
-          float wgt[3][3], fx[3];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float bf = floorf(xp[a] - 0.5f);
-            fx[a] = xp[a] - bf;
-            quad_weights(fx[a], wgt[a]);
-          }
-          // slab i of the stencil: x offset i, all (j, k)
-          const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
-          const float di = ((float)slab - fx[0]) * dx;
-          const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            const float wij = wi * wgt[1][j];
-            const float dj = ((float)j - fx[1]) * dx;
-            const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-              const float wt = wij * wgt[2][kk];
-              const float dk = ((float)kk - fx[2]) * dx;
-              am[3 * j + kk] += wt * mass;
-              apx[3 * j + kk] += wt * (qy[0] + B[6] * dk);
-              apy[3 * j + kk] += wt * (qy[1] + B[7] * dk);
-              apz[3 * j + kk] += wt * (qy[2] + B[8] * dk);
-            }
-          }
-        }
-        return end > first;
-      };
-      // Adds the accumulated slab of local cell lc to the shared block.
-      auto flush = [&](int lc) {
-        const int r0 = region_index(lc % 6, (lc / 6) % 6, lc / 36) + slab;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-          for (int kk = 0; kk < 3; ++kk) {
-            const int r = r0 + kRsy * j + kRsz * kk;
-            atomicAdd(&s_acc[0][r], am[3 * j + kk]);
-            atomicAdd(&s_acc[1][r], apx[3 * j + kk]);
-            atomicAdd(&s_acc[2][r], apy[3 * j + kk]);
-            atomicAdd(&s_acc[3][r], apz[3 * j + kk]);
-          }
-      };
-      {
-        const uint32_t c = p.item_order[(size_t)it * 64 + lane64];
-        const int lc = (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
-        if (accumulate(lc)) flush(lc);
-      }
-#pragma unroll 1
-      for (int lc = (int)lane64; lc < kLocalCells; lc += 64) {
-        const int lx = lc % 6, ly = (lc / 6) % 6, lz = lc / 36;
-        const bool core = lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4;
-        if (!core && accumulate(lc)) flush(lc);
-      }
-    }
+    bin_item<kScatterThreads>(s_stage, item.count, live, f, ss);
+    if (live) deposit_item<kScatterThreads>(s_stage, p.item_order + (size_t)it * 64, f, ss);
     if (__syncthreads_or(!ok)) {
       // The stage did not arrive (or the item exceeds the stage): report it,
       // wait once more (bounded) for the copy in flight and stop this CTA.
@@ -715,25 +821,81 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __g
     }
     // Every thread is done with the stage: the next item's copy goes now.
     if (threadIdx.x == 0 && it + gridDim.x < n_items) stage(it + gridDim.x);
-    // ---- 4. flush the block, clear it and the cell counters ----
-    for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-      const int lx = r & 7, ly = (r >> 3) & 7, lz = r >> 6;
-      const int q = region_index(lx, ly, lz);
-      const float m = s_acc[0][q], px = s_acc[1][q], py = s_acc[2][q], pz = s_acc[3][q];
-      if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f) {
-        s_acc[0][q] = 0.f;
-        s_acc[1][q] = 0.f;
-        s_acc[2][q] = 0.f;
-        s_acc[3][q] = 0.f;
-        const int ix = rx + lx, iy = ry + ly, iz = rz + lz;
-        if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-          const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
-          atomicAdd(&acc[c], make_float4(m, px, py, pz));
-          touch(touched, c);
-        }
+    flush_item<kScatterThreads>(f, ss);
+    __syncthreads();
+  }
+}
+
+// Fused gather + scatter of one substep (non-deterministic P2G): per item,
+// the CTA runs the gather of every particle (G2P, F update, return mapping,
+// B record) with the record kept in shared memory instead of HBM, then bins,
+// deposits and flushes the item's records as k_p2g does.  Saves the record's
+// 64-byte write and read per particle and one launch, and lets the gather
+// (FP32/FP64/XU pipes) of one CTA overlap the deposit (shared-memory
+// atomics) of the other CTA on the SM.  Items hold at most kStageMax
+// particles (the regrouping cuts them), so the records fit the stage; an
+// item that does not fit latches kFaultDeviceWait and is skipped.
+//
+// A fault latched before an item starts freezes the item (no gather, no
+// deposit); a particle that faults during the gather deposits nothing (m = 0
+// in its record).  The scene is frozen from the next substep on.
+template <bool WRITE_KEYS, class SR>
+__global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double tol, int sweeps, int reuse_svd,
+                                                              int acc_out) {
+  extern __shared__ __align__(16) float4 s_stage[];  // kStageMax records, 64-byte swizzle
+  __shared__ __align__(16) SceneDev s_sc;
+  __shared__ __align__(16) float4 s_vel[kRegionNodes];
+  __shared__ ScatterShared ss;
+  __shared__ uint32_t s_fault;
+  float4* __restrict__ acc = p.acc[acc_out];
+  uint8_t* __restrict__ touched = p.touched[acc_out];
+  const uint32_t n_items = *p.n_items;
+  const SR stol = (SR)tol;
+  clear_scatter_shared(ss, kFusedThreads);
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item item = p.items[it];
+    {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(p.scenes + item.scene);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
+      for (int k = threadIdx.x; k < (int)(sizeof(SceneDev) / 4); k += kFusedThreads) dst[k] = src[k];
+    }
+    const SceneDev* __restrict__ scp = p.scenes + item.scene;
+    uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
+    const uint32_t fault0 = *(volatile uint32_t*)status;
+    const ItemFrame f = item_frame(*scp, item, acc, touched);
+    const bool fits = item.count <= (uint32_t)kStageMax;
+    {
+      // Stage the 8^3-node velocity block (out-of-grid nodes read as zero).
+      const float4* __restrict__ gvel = p.vel + f.grid_off;
+      for (int r = threadIdx.x; r < kRegionNodes; r += kFusedThreads) {
+        const int ix = f.rx + (r & 7), iy = f.ry + ((r >> 3) & 7), iz = f.rz + (r >> 6);
+        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+        if ((unsigned)ix < (unsigned)f.n && (unsigned)iy < (unsigned)f.n && (unsigned)iz < (unsigned)f.n)
+          g = __ldg(&gvel[(size_t)ix + (size_t)f.n * ((size_t)iy + (size_t)f.n * (size_t)iz)]);
+        s_vel[r] = g;
       }
     }
-    for (int r = threadIdx.x; r < kLocalCells; r += blockDim.x) s_cell[r] = 0u;
+    if (threadIdx.x == 0) {
+      s_fault = fault0;
+      if (!fits) atomicOr(status, kFaultDeviceWait);
+    }
+    __syncthreads();
+    const bool live = s_fault == 0 && fits;
+    if (live) {
+      for (uint32_t k = threadIdx.x; k < item.count; k += kFusedThreads) {
+        float4 rec[4];
+        // the record's own stage slot is the scratch of gather_global
+        particle_step<kG2PRecord, WRITE_KEYS, SR>(p, s_sc, item.start + k, status, s_vel,
+                                                  reinterpret_cast<float*>(s_stage + 4 * (size_t)k), f.rx, f.ry,
+                                                  f.rz, f.n, stol, sweeps, reuse_svd, rec);
+        stage_store(s_stage, k, rec);
+      }
+    }
+    __syncthreads();
+    bin_item<kFusedThreads>(s_stage, item.count, live, f, ss);
+    if (live) deposit_item<kFusedThreads>(s_stage, p.item_order + (size_t)it * 64, f, ss);
+    __syncthreads();
+    flush_item<kFusedThreads>(f, ss);
     __syncthreads();
   }
 }
@@ -958,6 +1120,24 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
   return cudaErrorInvalidValue;
 }
 
+constexpr size_t kFusedStageBytes = (size_t)kStageMax * 64;
+
+template <bool KEYS, class SR>
+static cudaError_t launch_fused_t(const PoolDev& p, double tol, int sweeps, int reuse, int acc_out, int grid,
+                                  cudaStream_t st) {
+  k_g2p2g<KEYS, SR><<<grid, kFusedThreads, kFusedStageBytes, st>>>(p, tol, sweeps, reuse, acc_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fused(bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps, int reuse,
+                         int acc_out, int grid, cudaStream_t st) {
+  if (svd_fp64)
+    return write_keys ? launch_fused_t<true, double>(p, tol, sweeps, reuse, acc_out, grid, st)
+                      : launch_fused_t<false, double>(p, tol, sweeps, reuse, acc_out, grid, st);
+  return write_keys ? launch_fused_t<true, float>(p, tol, sweeps, reuse, acc_out, grid, st)
+                    : launch_fused_t<false, float>(p, tol, sweeps, reuse, acc_out, grid, st);
+}
+
 // stage tiles plus 1 KiB for the alignment of the swizzled stage
 constexpr size_t kStageBytes = (size_t)kStageMax * 64 + 1024;
 static_assert(kStageMax % kStageBoxRows == 0, "the stage holds whole TMA tiles");
@@ -1022,6 +1202,15 @@ static int persistent(const void* fn, int threads, size_t dyn_smem = 0) {
 int gather_grid_size(bool svd_fp64) {
   return svd_fp64 ? persistent((const void*)k_g2p<kG2PRecord, false, double>, kGatherThreads)
                   : persistent((const void*)k_g2p<kG2PRecord, false, float>, kGatherThreads);
+}
+
+int fused_grid_size(bool svd_fp64) {
+  // the record stage needs more than the default 48 KB of dynamic shared memory
+  const void* fns[4] = {(const void*)k_g2p2g<false, double>, (const void*)k_g2p2g<true, double>,
+                        (const void*)k_g2p2g<false, float>, (const void*)k_g2p2g<true, float>};
+  for (const void* fn : fns)
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedStageBytes);
+  return persistent(svd_fp64 ? fns[0] : fns[2], kFusedThreads, kFusedStageBytes);
 }
 
 int scatter_grid_size() {

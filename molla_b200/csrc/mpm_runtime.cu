@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace mpm {
@@ -276,6 +277,9 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   grid_gather32 = gather_grid_size(false);
   grid_gather64 = gather_grid_size(true);
   grid_scatter = scatter_grid_size();
+  grid_fused32 = fused_grid_size(false);
+  grid_fused64 = fused_grid_size(true);
+  if (const char* env = std::getenv("MOLLA_MPM_FUSED")) fused_mode = std::strcmp(env, "0") != 0 ? 1 : 0;
   MPM_CK(cudaStreamSynchronize(stream));
 }
 
@@ -689,6 +693,16 @@ void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
   eng->launches += 1;
 }
 
+void Group::launch_fused_pass(int acc_out, bool keys, cudaStream_t st) {
+  const int grid = svd_fp64 ? grid_fused64 : grid_fused32;
+  const double tol = svd_fp64 ? svd_tol64 : svd_tol32;
+  ProfRec pr;
+  eng->prof_begin(kStageGather, st, &pr);
+  MPM_CK(launch_fused(keys, svd_fp64, pool(), tol, svd_sweeps, reuse_svd ? 1 : 0, acc_out, grid, st));
+  eng->prof_end(&pr, st);
+  eng->launches += 1;
+}
+
 uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_out, cudaStream_t st) {
   eng->check();
   if (!n_live || !probe || n_cands <= 0) return sort_interval;
@@ -848,6 +862,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
   uint32_t since = 0;
+  const bool fused = use_fused();
   for (uint32_t s = 0; s < substeps; ++s) {
     ProfRec pr;
     eng->prof_begin(kStageGrid, st, &pr);
@@ -855,6 +870,16 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
     eng->prof_end(&pr, st);
     const bool last = s + 1 == substeps;
     const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
+    if (!last && fused) {
+      // gather + scatter in one launch; the regrouping follows the deposit
+      launch_fused_pass(a ^ 1, due, st);
+      if (due) {
+        regroup(false, st);
+        since = 0;
+      }
+      a ^= 1;
+      continue;
+    }
     launch_gather_pass(last ? kG2P : kG2PRecord, due, st);
     if (!last) {
       if (deterministic) {
@@ -980,6 +1005,13 @@ void Group::read_rows(uint32_t sid, int first, int count, float* out, cudaStream
   eng->launches += 1;
   MPM_CK(cudaMemcpyAsync(out, d.ptr, d.bytes(), cudaMemcpyDeviceToHost, st));
   MPM_CK(cudaStreamSynchronize(st));
+}
+
+void Group::pack_positions(uint32_t sid, float4* out, cudaStream_t st) {
+  const SceneHost& s = scenes.at(sid);
+  if (!s.n) return;
+  MPM_CK(launch_pack_positions(pool(), slot_of.ptr, s.id_base, s.n, out, st));
+  eng->launches += 1;
 }
 
 void Group::write_rows(uint32_t sid, int first, int count, const float* in, cudaStream_t st) {

@@ -79,13 +79,31 @@ def test_struct_layout_matches_c_header(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "molla_mpm.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(mpm_rheology), sizeof(mpm_config),'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(mpm_rheology), sizeof(mpm_config),'
         ' sizeof(mpm_status_info), sizeof(mpm_server_stats), offsetof(mpm_config, rheology),'
-        ' offsetof(mpm_config, grid_window_cells)); return 0;}\n')
+        ' offsetof(mpm_config, grid_window_cells), sizeof(mpm_render_view), offsetof(mpm_render_view, source),'
+        ' offsetof(mpm_render_view, live_position_bytes)); return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run([cc, "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     exp = [ctypes.sizeof(_ffi.mpm_rheology), ctypes.sizeof(_ffi.mpm_config), ctypes.sizeof(_ffi.mpm_status_info),
            ctypes.sizeof(_ffi.mpm_server_stats), _ffi.mpm_config.rheology.offset,
-           _ffi.mpm_config.grid_window_cells.offset]
+           _ffi.mpm_config.grid_window_cells.offset, ctypes.sizeof(_ffi.mpm_render_view),
+           _ffi.mpm_render_view.source.offset, _ffi.mpm_render_view.live_position_bytes.offset]
     assert got == exp
+
+
+def test_render_view_wrapper_exposes_the_live_prefix():
+    """MpmParticleRenderView (mpm_render_view.rs:20-36) over a raw view
+    struct: count, bytes, source identity and the CUDA array interface of the
+    live float4 prefix."""
+    raw = _ffi.mpm_render_view(positions=0x7F0000001000, count=3, capacity=10, source=42, live_position_bytes=48)
+    v = m.MpmParticleRenderView(raw, owner=None)
+    assert v.particle_count() == 3 and v.capacity == 10 and v.live_position_bytes() == 48
+    assert v.positions() == 0x7F0000001000
+    cai = v.__cuda_array_interface__
+    assert cai["shape"] == (3, 4) and cai["typestr"] == "<f4" and cai["data"] == (0x7F0000001000, False)
+    assert v.matches_source(m.MpmParticleRenderSource(42))
+    assert not v.matches_source(m.MpmParticleRenderSource(43))
+    empty = m.MpmParticleRenderView(_ffi.mpm_render_view(positions=0x7F0000001000, count=0, source=42), None)
+    assert empty.__cuda_array_interface__["shape"] == (0, 4) and empty.matches_source(v.source())

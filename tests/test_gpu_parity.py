@@ -565,3 +565,17 @@ def test_deterministic_p2g_lifecycle_and_repeatability(engine):
     O.step(sc, st, 6)
     assert np.abs(a[0] - st["pos"]).max() <= 2e-5
     assert norm_err(a[3], st["F"]) <= 2e-5
+
+
+def test_simulation_outlives_its_engine_handle():
+    """Destroying the engine handle first is allowed: the simulation keeps the
+    device stream until it is destroyed itself (the order the interpreter
+    may pick at exit)."""
+    e = m.Engine(0)
+    cfg = m.MpmConfig.sand()
+    sim = m.MpmSimulation.new(e, cfg)
+    sim.set_particles([[0.0, 0.3, 0.0], [0.05, 0.3, 0.0]])
+    e.close()
+    sim.step_n(1e-4, 3)
+    assert sim.read_active_grid_status().completed_substeps == 3
+    sim.close()
