@@ -51,11 +51,12 @@ KERNEL_BYTES = {
     "ParticleToGrid": (64, 16),
 }
 # DRAM bytes per particle per launch (dram__bytes_read.sum +
-# dram__bytes_write.sum) from one ncu capture of each kernel on the medium
-# workload (128^3 grid, 2M particles, substep ~280), scaled by particle count.
+# dram__bytes_write.sum) from one ncu capture of each kernel of the separate
+# substep on the medium workload (128^3 grid, 2M particles, substep ~250),
+# scaled by particle count.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "GridToParticle": 215.1,
-    "ParticleToGrid": 74.3,
+    "GridToParticle": 206.6,
+    "ParticleToGrid": 69.2,
 }
 # Whole-step model of the survey (separate P2G and G2P passes):
 # 268 B per particle-step + 56 B per active cell-step.
