@@ -32,7 +32,10 @@ cudaError_t launch_combine_det(const PoolDev& p, const float4* blocks, const uin
 constexpr int kTileNodes = 216;  // 6^3 node footprint of a 4^3-cell tile of base cells
 constexpr uint32_t kFaultNondeterministic = 4u;  // a deposit left the fixed-order path
 constexpr uint32_t kFaultDeviceWait = 8u;        // a bounded device-side wait gave up (or an item was malformed)
-constexpr int kStageMax = 960;                   // particles per scatter item (records staged in shared memory)
+// Particles per scatter item (records staged in shared memory).  640 records
+// (41 KB) let k_p2g run 4 CTAs per SM; a full tile at 8 particles per cell is
+// 512, so only compressed tiles are cut into two items.
+constexpr int kStageMax = 640;
 constexpr int kStageBoxRows = 64;                // records per TMA box of the scatter stage
 // Persistent grid sizes (SMs x resident CTAs).
 int gather_grid_size(bool svd_fp64);

@@ -762,7 +762,7 @@ __device__ __forceinline__ void clear_scatter_shared(ScatterShared& ss, int thre
   for (int r = threadIdx.x; r < kLocalCells; r += threads) ss.cell[r] = 0u;
 }
 
-__global__ void __launch_bounds__(kScatterThreads, 3) k_p2g(PoolDev p, const __grid_constant__ CUtensorMap rec_map,
+__global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __grid_constant__ CUtensorMap rec_map,
                                                             int acc_out) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   // the swizzle pattern repeats every 512 bytes: align the stage to 1 KiB

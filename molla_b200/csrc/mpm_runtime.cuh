@@ -204,12 +204,12 @@ class Group {
   // Fused gather + scatter for the non-final substeps of the atomic P2G
   // (k_g2p2g): -1 picks it for groups of at most kFusedMaxParticles live
   // particles, 1 always, 0 never (MOLLA_MPM_FUSED=1 / 0 in the environment
-  // at construction).  Measured on a B200: +19% particle-steps/s at 133k
-  // particles, +4% at 1M, even at 2M, 2-8% slower at 16M, where the separate
-  // kernels' higher occupancy (4 and 3 CTAs per SM against 2) hides the
+  // at construction).  Measured on a B200: +6% particle-steps/s at 133k
+  // particles, +1.7% at 1M, -4.6% at 2M, -8% at 16M, where the separate
+  // kernels' higher occupancy (4 CTAs per SM each against 2) hides the
   // per-item barriers better than the fusion saves.
   int fused_mode = -1;
-  static constexpr uint32_t kFusedMaxParticles = 2000000;
+  static constexpr uint32_t kFusedMaxParticles = 1500000;
   bool use_fused() const {
     return !deterministic && (fused_mode > 0 || (fused_mode < 0 && n_live <= kFusedMaxParticles));
   }
