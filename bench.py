@@ -325,6 +325,7 @@ def run_ours(args):
     # substeps, read positions back.
     pos_host = torch.from_numpy(scene.positions).pin_memory().numpy()
     ids_host = torch.from_numpy(scene.ids.astype(np.int32)).pin_memory().numpy().view(np.uint32)
+    out_host = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
     e2e_times = []
     for it in range(args.e2e_iters + 1):
         engine.synchronize()
@@ -332,7 +333,7 @@ def run_ours(args):
         sim.set_particles(pos_host)
         sim.set_materials(scene.rows, ids_host)
         sim.step_n(scene.dt, args.e2e_substeps)
-        out = sim.read_positions()
+        out = sim.read_positions(out=out_host)
         e2e_times.append(time.perf_counter() - t)
     e2e_s = float(np.median(e2e_times[1:])) if len(e2e_times) > 1 else float(e2e_times[0])
     e2e_s = max_over_ranks(dist, e2e_s, device)

@@ -485,14 +485,21 @@ class MpmSimulation:
         return MpmCommandBatch(self, stream)
 
     # -- readback -----------------------------------------------------------
-    def _read3(self, fn):
+    def _read3(self, fn, out=None):
         n = C.c_uint32()
-        out = np.empty((max(self.particle_count, 1), 3), np.float32)
+        if out is None:
+            out = np.empty((max(self.particle_count, 1), 3), np.float32)
+        elif (out.dtype != np.float32 or out.ndim != 2 or out.shape[1] != 3 or not out.flags.c_contiguous
+              or out.shape[0] < self.particle_count):
+            raise SolverError(MPM_ERR_INVALID, "out must be a C-contiguous float32 (>= n, 3) array")
         _check(fn(self._h, _fp(out), self.particle_count, C.byref(n)))
         return out[: n.value]
 
-    def read_positions(self) -> np.ndarray:
-        return self._read3(_ffi.lib().mpm_read_positions)
+    def read_positions(self, out=None) -> np.ndarray:
+        """Positions in original particle order.  `out` (optional) is a
+        float32 (>= n, 3) array to fill, e.g. in pinned memory for a fast
+        device-to-host copy; the returned array is its first n rows."""
+        return self._read3(_ffi.lib().mpm_read_positions, out)
 
     def particle_render_view(self, engine=None) -> MpmParticleRenderView:
         """particle_render_view (mpm_render_view.rs:38-56).  The first call
@@ -504,8 +511,8 @@ class MpmSimulation:
         _check(_ffi.lib().mpm_particle_render_view(self._h, C.byref(raw)))
         return MpmParticleRenderView(raw, self)
 
-    def read_velocities(self) -> np.ndarray:
-        return self._read3(_ffi.lib().mpm_read_velocities)
+    def read_velocities(self, out=None) -> np.ndarray:
+        return self._read3(_ffi.lib().mpm_read_velocities, out)
 
     def read_particle_state(self):
         """(C[n,9], F[n,9], jp[n]), matrices column-major per particle."""

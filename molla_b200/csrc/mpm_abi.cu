@@ -387,11 +387,20 @@ static void sim_reseed(mpm_sim* s, const float* xyz, const float* vel, uint32_t 
     s->group->remove_scene(s->sid);
     s->sid = 0xffffffffu;
   }
-  std::vector<uint32_t> mat(n, 0);
-  for (uint32_t i = 0; i < n && i < s->ids.size(); ++i) mat[i] = s->ids[i];
+  // Material ids persist across reseeds (as the reference's id buffer does):
+  // the first n of the last set_materials, zero past its end.
+  std::vector<uint32_t> mat;
+  const uint32_t* ids = nullptr;
+  if (n && s->ids.size() >= n) {
+    ids = s->ids.data();
+  } else if (n && !s->ids.empty()) {
+    mat.assign(n, 0u);
+    std::copy(s->ids.begin(), s->ids.end(), mat.begin());
+    ids = mat.data();
+  }
   const float* mass = s->mass.size() == n && n ? s->mass.data() : nullptr;
   const float* vol = s->volume.size() == n && n ? s->volume.data() : nullptr;
-  s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, n ? mat.data() : nullptr, n, s->dt);
+  s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, ids, n, s->dt);
   s->count = n;
   s->apply_group_settings();
   if (!s->spheres.empty())
@@ -460,11 +469,15 @@ int mpm_set_materials(mpm_sim* sim, const mpm_rheology* rows, uint32_t n_rows, c
     REQUIRE(n == sim->count, MPM_ERR_INVALID,
             "MPM set_materials: " + std::to_string(n) + " particle ids for " + std::to_string(sim->count) +
                 " particles — seed particles first");
-    for (uint32_t i = 0; i < n; ++i)
-      REQUIRE(ids[i] < n_rows, MPM_ERR_INVALID,
-              "MPM set_materials: particle material id " + std::to_string(ids[i]) + " out of range (" +
-                  std::to_string(n_rows) + " rows)");
     for (uint32_t i = 0; i < n_rows; ++i) REQUIRE(rows[i].kind <= 2, MPM_ERR_INVALID, "unknown MPM rheology");
+    // range check as a branch-free max (vectorises); name the first bad id
+    uint32_t top = 0;
+    for (uint32_t i = 0; i < n; ++i) top = std::max(top, ids[i]);
+    if (top >= n_rows) {
+      const uint32_t bad = *std::find_if(ids, ids + n, [&](uint32_t v) { return v >= n_rows; });
+      throw Error(MPM_ERR_INVALID, "MPM set_materials: particle material id " + std::to_string(bad) +
+                                       " out of range (" + std::to_string(n_rows) + " rows)");
+    }
     sim->rows.assign(rows, rows + n_rows);
     sim->ids.assign(ids, ids + n);
     if (sim->sid != 0xffffffffu) {

@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace mpm {
@@ -370,6 +371,20 @@ __device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sw
 }
 
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+// Two independent FP32 fused multiply-adds in one instruction (sm_100
+// fma.rn.f32x2): (a.x b.x + c.x, a.y b.y + c.y), each rounded once, the same
+// values as two fmaf calls.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  uint64_t ua, ub, uc, r;
+  memcpy(&ua, &a, 8);
+  memcpy(&ub, &b, 8);
+  memcpy(&uc, &c, 8);
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(ua), "l"(ub), "l"(uc));
+  float2 o;
+  memcpy(&o, &r, 8);
+  return o;
+}
 
 // Quadratic B-spline weights (mpm.wgsl:285-294).
 __device__ __forceinline__ void quad_weights(float fx, float* w) {

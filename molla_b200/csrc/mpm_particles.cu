@@ -659,12 +659,13 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
                                              ScatterShared& ss) {
   static_assert(T >= 192, "the core cells take 3 x 64 threads");
   const uint32_t total = ss.total;
-  float am[9], apx[9], apy[9], apz[9];
+  // per node of the slab: (p.x, p.y) and (p.z, m), accumulated in pairs
+  float2 axy[9], azm[9];
   // Accumulates slab `slab` of the particles of local cell lc in registers;
   // returns whether it had any.
   auto accumulate = [&](int lc, int slab) {
 #pragma unroll
-    for (int q = 0; q < 9; ++q) am[q] = apx[q] = apy[q] = apz[q] = 0.f;
+    for (int q = 0; q < 9; ++q) axy[q] = azm[q] = make_float2(0.f, 0.f);
     const uint32_t first = ss.cell[lc], end = lc == kLocalCells - 1 ? total : ss.cell[lc + 1];
     for (uint32_t t = first; t < end; ++t) {
       const uint32_t j = ss.idx[t];
@@ -684,19 +685,23 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
       const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
       const float di = ((float)slab - fx[0]) * f.dx;
       const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
+      const float dks[3] = {-fx[2] * f.dx, (1.0f - fx[2]) * f.dx, (2.0f - fx[2]) * f.dx};
+      const float2 b67 = make_float2(B[6], B[7]);
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         const float wij = wi * wgt[1][j];
         const float dj = ((float)j - fx[1]) * f.dx;
-        const float qy[3] = {qx[0] + B[3] * dj, qx[1] + B[4] * dj, qx[2] + B[5] * dj};
+        const float2 qy01 = make_float2(qx[0] + B[3] * dj, qx[1] + B[4] * dj);
+        const float qy2 = qx[2] + B[5] * dj;
 #pragma unroll
         for (int kk = 0; kk < 3; ++kk) {
           const float wt = wij * wgt[2][kk];
-          const float dk = ((float)kk - fx[2]) * f.dx;
-          am[3 * j + kk] += wt * mass;
-          apx[3 * j + kk] += wt * (qy[0] + B[6] * dk);
-          apy[3 * j + kk] += wt * (qy[1] + B[7] * dk);
-          apz[3 * j + kk] += wt * (qy[2] + B[8] * dk);
+          const float dk = dks[kk];
+          const float2 w2 = make_float2(wt, wt);
+          const float2 q01 = fma2(b67, make_float2(dk, dk), qy01);
+          const float2 q2m = make_float2(qy2 + B[8] * dk, mass);
+          axy[3 * j + kk] = fma2(w2, q01, axy[3 * j + kk]);
+          azm[3 * j + kk] = fma2(w2, q2m, azm[3 * j + kk]);
         }
       }
     }
@@ -710,10 +715,10 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
 #pragma unroll
       for (int kk = 0; kk < 3; ++kk) {
         const int r = r0 + kRsy * j + kRsz * kk;
-        atomicAdd(&ss.acc[0][r], am[3 * j + kk]);
-        atomicAdd(&ss.acc[1][r], apx[3 * j + kk]);
-        atomicAdd(&ss.acc[2][r], apy[3 * j + kk]);
-        atomicAdd(&ss.acc[3][r], apz[3 * j + kk]);
+        atomicAdd(&ss.acc[0][r], azm[3 * j + kk].y);
+        atomicAdd(&ss.acc[1][r], axy[3 * j + kk].x);
+        atomicAdd(&ss.acc[2][r], axy[3 * j + kk].y);
+        atomicAdd(&ss.acc[3][r], azm[3 * j + kk].x);
       }
   };
   if (threadIdx.x < 192) {

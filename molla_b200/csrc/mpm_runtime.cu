@@ -431,27 +431,23 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
 
   // upload particles
   if (n) {
-    DevBuf<float> dx(3 * (size_t)n), dv, dm, dvol;
-    DevBuf<uint32_t> dmat;
-    MPM_CK(cudaMemcpyAsync(dx.ptr, xyz, dx.bytes(), cudaMemcpyHostToDevice, stream));
-    if (velp) {
-      dv.alloc(3 * (size_t)n);
-      MPM_CK(cudaMemcpyAsync(dv.ptr, velp, dv.bytes(), cudaMemcpyHostToDevice, stream));
-    }
-    if (mass) {
-      dm.alloc(n);
-      MPM_CK(cudaMemcpyAsync(dm.ptr, mass, dm.bytes(), cudaMemcpyHostToDevice, stream));
-    }
-    if (vol) {
-      dvol.alloc(n);
-      MPM_CK(cudaMemcpyAsync(dvol.ptr, vol, dvol.bytes(), cudaMemcpyHostToDevice, stream));
-    }
-    if (mat_ids) {
-      dmat.alloc(n);
-      MPM_CK(cudaMemcpyAsync(dmat.ptr, mat_ids, dmat.bytes(), cudaMemcpyHostToDevice, stream));
-    }
-    MPM_CK(launch_init_particles(pool(), slot_of.ptr, n_live, (uint32_t)id0, n, dx.ptr, dv.ptr, dm.ptr, dvol.ptr,
-                                 cfg.particle_mass, cfg.particle_volume, dmat.ptr, sid, stream));
+    // carve the uploads out of the staging buffer (256-byte aligned pieces)
+    const size_t b3 = round_up((size_t)n * 12, 256), b1 = round_up((size_t)n * 4, 256);
+    unsigned char* st = staging_bytes(b3 + (velp ? b3 : 0) + (mass ? b1 : 0) + (vol ? b1 : 0) + (mat_ids ? b1 : 0));
+    auto take = [&](const void* src, size_t bytes, size_t span) -> void* {
+      if (!src) return nullptr;
+      void* dst = st;
+      MPM_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+      st += span;
+      return dst;
+    };
+    const float* dx = static_cast<const float*>(take(xyz, (size_t)n * 12, b3));
+    const float* dv = static_cast<const float*>(take(velp, (size_t)n * 12, b3));
+    const float* dm = static_cast<const float*>(take(mass, (size_t)n * 4, b1));
+    const float* dvol = static_cast<const float*>(take(vol, (size_t)n * 4, b1));
+    const uint32_t* dmat = static_cast<const uint32_t*>(take(mat_ids, (size_t)n * 4, b1));
+    MPM_CK(launch_init_particles(pool(), slot_of.ptr, n_live, (uint32_t)id0, n, dx, dv, dm, dvol,
+                                 cfg.particle_mass, cfg.particle_volume, dmat, sid, stream));
     eng->launches += 1;
     MPM_CK(cudaStreamSynchronize(stream));
   }
@@ -610,13 +606,21 @@ void Group::set_scene_cfg(uint32_t sid, const mpm_config& cfg) {
   set_scene_dt(sid, dt);
 }
 
+unsigned char* Group::staging_bytes(size_t bytes) {
+  if (staging.count < bytes) {
+    MPM_CK(cudaStreamSynchronize(stream));
+    staging.alloc(bytes + bytes / 4);
+  }
+  return staging.ptr;
+}
+
 void Group::set_material_ids(uint32_t sid, const uint32_t* host_ids, uint32_t n) {
   SceneHost& s = scenes.at(sid);
   if (n != s.n) throw Error(MPM_ERR_INVALID, "material id count does not match the particle count");
   if (!n) return;
-  DevBuf<uint32_t> d(n);
-  MPM_CK(cudaMemcpyAsync(d.ptr, host_ids, d.bytes(), cudaMemcpyHostToDevice, stream));
-  MPM_CK(launch_set_material_ids(pool(), slot_of.ptr, s.id_base, n, d.ptr, stream));
+  uint32_t* d = reinterpret_cast<uint32_t*>(staging_bytes((size_t)n * 4));
+  MPM_CK(cudaMemcpyAsync(d, host_ids, (size_t)n * 4, cudaMemcpyHostToDevice, stream));
+  MPM_CK(launch_set_material_ids(pool(), slot_of.ptr, s.id_base, n, d, stream));
   eng->launches += 1;
   MPM_CK(cudaStreamSynchronize(stream));
 }
@@ -997,13 +1001,14 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
 void Group::read_rows(uint32_t sid, int first, int count, float* out, cudaStream_t st) {
   const SceneHost& s = scenes.at(sid);
   if (!s.n) return;
-  DevBuf<float> d((size_t)count * s.n);
+  const size_t bytes = (size_t)count * s.n * sizeof(float);
+  float* d = reinterpret_cast<float*>(staging_bytes(bytes));
   if (count == 3)
-    MPM_CK(launch_gather_xyz(pool(), first, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+    MPM_CK(launch_gather_xyz(pool(), first, slot_of.ptr, s.id_base, s.n, d, st));
   else
-    MPM_CK(launch_gather_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+    MPM_CK(launch_gather_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d, st));
   eng->launches += 1;
-  MPM_CK(cudaMemcpyAsync(out, d.ptr, d.bytes(), cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, st));
   MPM_CK(cudaStreamSynchronize(st));
 }
 
@@ -1017,9 +1022,10 @@ void Group::pack_positions(uint32_t sid, float4* out, cudaStream_t st) {
 void Group::write_rows(uint32_t sid, int first, int count, const float* in, cudaStream_t st) {
   const SceneHost& s = scenes.at(sid);
   if (!s.n) return;
-  DevBuf<float> d((size_t)count * s.n);
-  MPM_CK(cudaMemcpyAsync(d.ptr, in, d.bytes(), cudaMemcpyHostToDevice, st));
-  MPM_CK(launch_scatter_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d.ptr, st));
+  const size_t bytes = (size_t)count * s.n * sizeof(float);
+  float* d = reinterpret_cast<float*>(staging_bytes(bytes));
+  MPM_CK(cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, st));
+  MPM_CK(launch_scatter_rows(pool(), first, count, slot_of.ptr, s.id_base, s.n, d, st));
   eng->launches += 1;
   MPM_CK(cudaStreamSynchronize(st));
 }

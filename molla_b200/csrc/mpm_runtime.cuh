@@ -166,6 +166,13 @@ class Group {
   // grid pool
   DevBuf<float4> acc[2], vel;
   DevBuf<float4> vel2;  // semi-implicit Jacobi ping-pong (allocated when a scene needs it)
+  // Device side of host uploads and readbacks, grown on demand and kept: a
+  // per-call allocation would cost a cudaMalloc and a device-synchronising
+  // cudaFree of up to ~36 bytes per particle on every set_particles / read.
+  // Every user synchronises the stream before returning, so one buffer
+  // serves them all.
+  DevBuf<unsigned char> staging;
+  unsigned char* staging_bytes(size_t bytes);
   DevBuf<uint8_t> rigid_blocks;  // per 256-cell block: a rigid sphere may reach it
   DevBuf<RigidDev> rigid_d;      // kMaxRigid per scene
   DevBuf<float> wrench_d;        // 8 floats per sphere slot
