@@ -99,3 +99,27 @@ def test_render_view_follows_regroup_and_batches(engine):
     np.testing.assert_array_equal(got[:, :3], sim.read_positions())
     assert not np.array_equal(got[:, :3], pts)
     sim.close()
+
+
+def test_read_positions_into_caller_buffers(engine):
+    """read_positions(out=...) fills a caller array (pageable or pinned) with
+    the same values as the allocating form and rejects a wrong buffer."""
+    import torch
+    cfg = m.MpmConfig.sand()
+    sim = m.MpmSimulation(engine, cfg)
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-0.2, 0.2, size=(3000, 3)).astype(np.float32)
+    pts[:, 1] += 0.5
+    sim.set_particles(pts)
+    sim.step_n(1e-4, 7)
+    ref = sim.read_positions()
+    pinned = torch.empty((4000, 3), dtype=torch.float32).pin_memory().numpy()
+    got = sim.read_positions(out=pinned)
+    assert got.shape == (3000, 3) and np.shares_memory(got, pinned)
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(sim.read_positions(out=np.zeros((3000, 3), np.float32)), ref)
+    np.testing.assert_array_equal(sim.read_velocities(out=np.zeros((3000, 3), np.float32)), sim.read_velocities())
+    for bad in (np.zeros((2999, 3), np.float32), np.zeros((3000, 3), np.float64), np.zeros((3000, 4), np.float32)):
+        with pytest.raises(m.SolverError):
+            sim.read_positions(out=bad)
+    sim.close()
