@@ -579,3 +579,30 @@ def test_simulation_outlives_its_engine_handle():
     sim.step_n(1e-4, 3)
     assert sim.read_active_grid_status().completed_substeps == 3
     sim.close()
+
+
+@pytest.mark.parametrize("preset,window", [("sand", (3, -2, 1)), ("snow", (-5, 4, 0))])
+def test_grid_window_parity(engine, preset, window):
+    """A shifted lattice (grid_window_cells, mpm.wgsl:513-516: base cell minus
+    the window, node position o + (index + window) dx): the block sits in the
+    shifted domain, falls against its floor, and matches the oracle; the tile
+    keys of the sort subtract the window too."""
+    cfg = getattr(m.MpmConfig, preset)()
+    cfg.grid_window_cells = window
+    dx, n = cfg.cell_size, cfg.grid_size
+    lo = [cfg.grid_origin[a] + (window[a] + 0.35 * n) * dx for a in range(3)]
+    hi = [cfg.grid_origin[a] + (window[a] + 0.65 * n) * dx for a in range(3)]
+    lo[1] = cfg.grid_origin[1] + (window[1] + 6) * dx  # near the shifted floor
+    hi[1] = lo[1] + 0.25 * n * dx
+    pts = scenes.fill_box_lcg(lo, hi, 8, 7)
+    sim, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 480, 60)
+    assert gpu["status"].completed_substeps == 60 and not gpu["status"].numerical_fault
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 1e-4
+    assert np.abs(gpu["vel"] - st["vel"]).max() < 1e-2
+    # the block fell (gravity) and stayed inside the shifted walls
+    assert gpu["pos"][:, 1].mean() < pts[:, 1].mean()
+    floor = cfg.grid_origin[1] + (window[1] + 2) * dx
+    assert gpu["pos"][:, 1].min() >= floor - 1e-6
+    keys, ids = sim.read_sort_permutation()
+    ok, oi = O.particle_order(O.make_scene(cfg, [cfg.rheology], 1.0 / 480), gpu["pos"], len(pts), len(pts))
+    assert np.array_equal(keys, ok) and np.array_equal(ids, oi)
