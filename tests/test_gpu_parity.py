@@ -606,3 +606,55 @@ def test_grid_window_parity(engine, preset, window):
     keys, ids = sim.read_sort_permutation()
     ok, oi = O.particle_order(O.make_scene(cfg, [cfg.rheology], 1.0 / 480), gpu["pos"], len(pts), len(pts))
     assert np.array_equal(keys, ok) and np.array_equal(ids, oi)
+
+
+@pytest.mark.parametrize("pad,walls", [(3, 0), (4, 1)])
+def test_wall_extensions_parity(engine, pad, walls):
+    """boundary_pad (the reference's fixed 2 made a parameter) and the sticky
+    no-slip walls extension: a block thrown at the -x wall and dropped onto
+    the floor matches the oracle, and no particle crosses the pad layer."""
+    cfg = m.MpmConfig.sand()
+    cfg.boundary_pad = pad
+    cfg.walls = walls
+    dx, o = cfg.cell_size, cfg.grid_origin
+    lo = [o[0] + (pad + 2) * dx, o[1] + (pad + 3) * dx, o[2] + 0.4 * cfg.grid_size * dx]
+    hi = [lo[0] + 8 * dx, lo[1] + 8 * dx, lo[2] + 8 * dx]
+    pts = scenes.fill_box_lcg(lo, hi, 8, 3)
+    vel = np.tile(np.array([[-2.0, 0.0, 0.0]], np.float32), (len(pts), 1))
+    _, gpu, st = run_both(engine, cfg, None, pts, None, 1.0 / 960, 80, vel=vel)
+    assert gpu["status"].completed_substeps == 80 and not gpu["status"].numerical_fault
+    assert np.abs(gpu["pos"] - st["pos"]).max() < 1e-4
+    assert np.abs(gpu["vel"] - st["vel"]).max() < 1e-2
+    for a in (0, 1):
+        assert gpu["pos"][:, a].min() >= o[a] + pad * dx - 1e-6
+
+
+def test_stage_profile_counts_launches(engine):
+    """MpmProfileStage timing (mpm_profile.rs:8-80): per-stage launch counts
+    and device times of a profiled step_n, nothing while disabled, zero after
+    a reset."""
+    cfg = m.MpmConfig.snow()
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(scenes.fill_box_lcg([-0.1, 0.2, -0.1], [0.1, 0.4, 0.1], 8, 5))
+    sim.set_sort_interval(4)
+    sim.step_n(1.0 / 480, 2)
+    engine.synchronize()
+    engine.reset_profile()
+    engine.profile(True)
+    sim.step_n(1.0 / 480, 10)
+    engine.synchronize()
+    engine.profile(False)
+    prof = engine.read_profile()
+    assert set(prof) == set(m.Engine.STAGES)
+    assert prof["GridUpdate"][0] == 10 and prof["StressRecord"][0] == 1
+    # gathers: every substep; scatters: once per call when fused, else every substep but the last
+    assert prof["GridToParticle"][0] == 10
+    assert prof["ParticleToGrid"][0] in (1, 10)
+    assert prof["ParticleOrdering"][0] >= 2  # the call's first regroup + one every 4 substeps
+    assert all(ms > 0.0 for cnt, ms in prof.values() if cnt)
+    sim.step_n(1.0 / 480, 3)
+    engine.synchronize()
+    assert engine.read_profile() == prof  # disabled: nothing added
+    engine.reset_profile()
+    assert all(v == (0, 0.0) for v in engine.read_profile().values())
+    sim.close()
