@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 //  3. deposit: thread t takes x-slab i = t / 64 of the stencil and one cell
 //     (t mod 64): the tile's own cells in the order of their particle counts
 //     at the regrouping, so that the lanes of a warp walk lists of similar
-//     length, then the margin cells particles moved into.  It adds the nine
+//     length, then the non-empty margin cells particles moved into (listed
+//     by the scan of step 2).  It adds the nine
 //     slab-i node contributions of its cell's particles in registers and
 //     issues 9 x 4 shared-memory atomics for the whole cell, not per
 //     particle; the lanes of a warp own different cells, so those atomics
@@ -574,8 +575,14 @@ struct ScatterShared {
   float acc[4][kRegionFloats];  // the 8^3-node block: m, p.x, p.y, p.z
   uint32_t cell[kLocalCells];   // counts, then exclusive starts
   uint16_t idx[kStageMax];      // item records sorted by local cell
-  uint32_t total;
+  uint8_t margin[kLocalCells];  // non-empty local cells outside the tile's own 4^3
+  uint32_t total, n_margin;
 };
+
+__device__ __forceinline__ bool core_cell_index(int lc) {
+  const int lx = lc % 6, ly = (lc / 6) % 6, lz = lc / 36;
+  return lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4;
+}
 
 // Scatter step 2 (bin) for a CTA of T threads: every staged record is binned
 // by its current base cell among the 6^3 local cells (counting sort with
@@ -630,13 +637,23 @@ __device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bo
       if (lane >= (uint32_t)o) incl += y;
     }
     uint32_t run = incl - sum;
+    uint32_t n_margin = 0;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
       const int cell = (int)lane * 7 + k;
       if (cell < kLocalCells) ss.cell[cell] = run;
       run += c[k];
+      // compact the non-empty margin cells (particles that left the tile's
+      // own cells since the regrouping) into a short list
+      const bool mar = cell < kLocalCells && c[k] != 0u && !core_cell_index(cell);
+      const uint32_t ballot = __ballot_sync(0xffffffffu, mar);
+      if (mar) ss.margin[n_margin + __popc(ballot & ((1u << lane) - 1u))] = (uint8_t)cell;
+      n_margin += __popc(ballot);
     }
-    if (lane == 31) ss.total = incl;
+    if (lane == 31) {
+      ss.total = incl;
+      ss.n_margin = n_margin;
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -650,7 +667,9 @@ __device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bo
 // takes x-slab t / 64 of the stencil and one of the tile's own 64 cells, in
 // the order of their particle counts at the regrouping (`order`), so that the
 // lanes of a warp walk lists of similar length; then all T threads share the
-// (margin cell, slab) pairs of the cells particles moved into.  A thread adds
+// (margin cell, slab) pairs of the non-empty cells particles moved into (the
+// compact list the scan built; scanning all 152 margin cells per item cost
+// 10% of the scatter).  A thread adds
 // the nine slab nodes of its cell's particles in registers and issues 9 x 4
 // shared-memory atomics for the whole cell; the lanes of a warp own
 // different cells, so those atomics do not collide.
@@ -727,12 +746,12 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
     const int lc = (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
     if (accumulate(lc, slab)) flush(lc, slab);
   }
+  // then the (margin cell, slab) pairs of the non-empty margin cells
+  const int n_margin = (int)ss.n_margin;
 #pragma unroll 1
-  for (int u = (int)threadIdx.x; u < 3 * kLocalCells; u += T) {
-    const int lc = u % kLocalCells, slab = u / kLocalCells;
-    const int lx = lc % 6, ly = (lc / 6) % 6, lz = lc / 36;
-    const bool core = lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4;
-    if (!core && accumulate(lc, slab)) flush(lc, slab);
+  for (int u = (int)threadIdx.x; u < 3 * n_margin; u += T) {
+    const int lc = ss.margin[u % n_margin], slab = u / n_margin;
+    if (accumulate(lc, slab)) flush(lc, slab);
   }
 }
 
