@@ -129,6 +129,15 @@ __device__ __forceinline__ void touch(uint8_t* touched, uint64_t g) { touched[g 
 __device__ __forceinline__ bool finitef(float x) {
   return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u;  // mpm.wgsl:217-219
 }
+// Finiteness of many values at once: 0 * v is NaN exactly when v is infinite
+// or NaN, so an accumulator started at 0 stays 0 (or -0) while every value
+// folded in is finite -- one fused multiply-add per value in a chain beside
+// the arithmetic it checks, and one compare at the end (nf_ok), instead of a
+// classify-and-branch per value.  Relies on IEEE arithmetic (no fast-math).
+__device__ __forceinline__ float nf_acc(float acc, float v) { return fmaf(0.0f, v, acc); }
+__device__ __forceinline__ double nf_acc(double acc, double v) { return fma(0.0, v, acc); }
+__device__ __forceinline__ bool nf_ok(float acc) { return acc == 0.0f; }
+__device__ __forceinline__ bool nf_ok(double acc) { return acc == 0.0; }
 
 // ---------------------------------------------------------------------------
 // 3x3 helpers on register arrays, column-major a[3*col+row].
@@ -495,10 +504,18 @@ __device__ __forceinline__ void p2g_affine(const SvdOut<T>& svd, const MatDev& m
 template <class T>
 __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev& md, float& jp, bool& changed) {
   float s[3] = {(float)svd.s[0], (float)svd.s[1], (float)svd.s[2]};
-  if (!finitef(s[0]) || !finitef(s[1]) || !finitef(s[2])) return false;
+  {
+    float nf = 0.0f;
+    T nfv = T(0);
 #pragma unroll
-  for (int i = 0; i < 9; ++i)
-    if (!finitef(svd.u[i]) || !finitef((float)svd.v[i])) return false;
+    for (int a = 0; a < 3; ++a) nf = nf_acc(nf, s[a]);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      nf = nf_acc(nf, svd.u[i]);
+      nfv = nf_acc(nfv, svd.v[i]);  // |v| <= 1: finite in T is finite in FP32
+    }
+    if (!nf_ok(nf) || !nf_ok(nfv)) return false;
+  }
   T ns[3] = {svd.s[0], svd.s[1], svd.s[2]};
   float dq = 0.0f;
   bool jp_replace = false;
@@ -547,9 +564,12 @@ __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev&
       }
     }
   }
-  if (!finitef((float)ns[0]) || !finitef((float)ns[1]) || !finitef((float)ns[2]) || !finitef(dq) ||
-      !finitef(jp + dq))
-    return false;
+  {
+    // ns comes from FP32 values (clamps of s, expf), so finite in T is finite in FP32
+    const T nfs = nf_acc(nf_acc(nf_acc(T(0), ns[0]), ns[1]), ns[2]);
+    const float nfq = nf_acc(nf_acc(0.0f, dq), jp + dq);
+    if (!nf_ok(nfs) || !nf_ok(nfq)) return false;
+  }
   changed = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {

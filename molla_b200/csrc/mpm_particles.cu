@@ -169,12 +169,13 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
   SvdOut<SR> svd;
   if constexpr (kGather) {
     // ---- g2p (mpm.wgsl:1242-1353) ----
-    bool fin = finitef(x) && finitef(y) && finitef(z) && finitef(jp);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]);
     const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
-    fin = fin && finitef(xp[0]) && finitef(xp[1]) && finitef(xp[2]);
-    if (!fin) {
+    float nf = nf_acc(nf_acc(nf_acc(nf_acc(0.0f, x), y), z), jp);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) nf = nf_acc(nf, F[i]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nf = nf_acc(nf, xp[a]);
+    if (!nf_ok(nf)) {
       atomicOr(status, kFaultNumerical);
       ok = false;
     }
@@ -261,11 +262,12 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         for (int i = 0; i < 9; ++i) C[i] *= md.afac;
       }
       float np[3] = {x + sc.dt * v[0], y + sc.dt * v[1], z + sc.dt * v[2]};
-      bool fin2 = finitef(np[0]) && finitef(np[1]) && finitef(np[2]) && finitef(v[0]) && finitef(v[1]) &&
-                  finitef(v[2]);
+      float nf2 = 0.0f;
 #pragma unroll
-      for (int i = 0; i < 9; ++i) fin2 = fin2 && finitef(C[i]);
-      if (!fin2) {
+      for (int a = 0; a < 3; ++a) nf2 = nf_acc(nf_acc(nf2, np[a]), v[a]);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) nf2 = nf_acc(nf2, C[i]);
+      if (!nf_ok(nf2)) {
         atomicOr(status, kFaultNumerical);
         ok = false;
       }
@@ -281,10 +283,10 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         for (int i = 0; i < 9; ++i) A[i] = sc.dt * C[i] + ((i % 4 == 0) ? 1.f : 0.f);
         float Fn[9];
         matmul(A, F, Fn);
-        bool fin3 = true;
+        float nf3 = 0.0f;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) fin3 = fin3 && finitef(Fn[i]);
-        if (!fin3) {
+        for (int i = 0; i < 9; ++i) nf3 = nf_acc(nf3, Fn[i]);
+        if (!nf_ok(nf3)) {
           atomicOr(status, kFaultNumerical);
           ok = false;
         } else {
@@ -316,10 +318,13 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
                                   ((SR)svd.u[3 + r] * svd.s[1]) * svd.v[3 + c] +
                                   ((SR)svd.u[6 + r] * svd.s[2]) * svd.v[6 + c];
             }
-            bool fin4 = true;
+            // the FP32 copy must be finite too (an FP64 value beyond FP32 range)
+            float nf4 = 0.0f;
+            if (rebuild) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) fin4 = fin4 && (!rebuild || finitef((float)Fr[i]));
-            if (fin4) {
+              for (int i = 0; i < 9; ++i) nf4 = nf_acc(nf4, (float)Fr[i]);
+            }
+            if (nf_ok(nf4)) {
               if (rebuild) {
 #pragma unroll
                 for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
