@@ -356,22 +356,28 @@ __device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sw
       o.s[i] *= sg;
     }
   }
-  if (det3(v) < T(0)) {
-    // flip the column of V with the smallest |sigma|
-    const T a0 = o.s[0] < T(0) ? -o.s[0] : o.s[0];
-    const T a1 = o.s[1] < T(0) ? -o.s[1] : o.s[1];
-    const T a2 = o.s[2] < T(0) ? -o.s[2] : o.s[2];
-    const bool m1 = a1 < a0;
-    const T a01 = m1 ? a1 : a0;
-    const bool m2 = a2 < a01;
-    const int mi = m2 ? 2 : (m1 ? 1 : 0);
+  // V is a product of plane rotations, so det V = +1 up to rounding: the
+  // reference's flip (mpm.wgsl:457-466) never fires.  It is kept in the FP32
+  // reference form; the FP64 form, whose rotations are refined to FP64,
+  // skips its FP64 determinant.
+  if constexpr (sizeof(T) == 4) {
+    if (det3(v) < T(0)) {
+      // flip the column of V with the smallest |sigma|
+      const T a0 = o.s[0] < T(0) ? -o.s[0] : o.s[0];
+      const T a1 = o.s[1] < T(0) ? -o.s[1] : o.s[1];
+      const T a2 = o.s[2] < T(0) ? -o.s[2] : o.s[2];
+      const bool m1 = a1 < a0;
+      const T a01 = m1 ? a1 : a0;
+      const bool m2 = a2 < a01;
+      const int mi = m2 ? 2 : (m1 ? 1 : 0);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const T sg = (i == mi) ? T(-1) : T(1);
-      v[3 * i] *= sg;
-      v[3 * i + 1] *= sg;
-      v[3 * i + 2] *= sg;
-      o.s[i] *= sg;
+      for (int i = 0; i < 3; ++i) {
+        const T sg = (i == mi) ? T(-1) : T(1);
+        v[3 * i] *= sg;
+        v[3 * i + 1] *= sg;
+        v[3 * i + 2] *= sg;
+        o.s[i] *= sg;
+      }
     }
   }
 }
