@@ -55,14 +55,16 @@ KERNEL_BYTES = {
 # substep on the medium workload (128^3 grid, 2M particles, substep ~250),
 # scaled by particle count.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "GridToParticle": 206.6,
+    "GridToParticle": 204.9,
     "ParticleToGrid": 69.2,
 }
 # The fused gather + scatter (k_g2p2g, groups of at most 2M particles) keeps
 # the 64-byte record in shared memory: 228 - 64 B per particle, and per
 # active node the velocity read plus the float4 deposit.
 FUSED_BYTES = (164, 32)
-MEASURED_TRAFFIC_FUSED_PER_PARTICLE = None
+# ncu DRAM bytes per particle of k_g2p2g on the 1M-particle scaled cube
+# (state 160 MB, just above L2).
+MEASURED_TRAFFIC_FUSED_PER_PARTICLE = 118.7
 # Whole-step model of the survey (separate P2G and G2P passes):
 # 268 B per particle-step + 56 B per active cell-step.
 STEP_BYTES_PER_PARTICLE = 268
@@ -366,9 +368,13 @@ def run_ours(args):
         if fused and dom == "GridToParticle":
             kernel_name = "k_g2p2g<gather + return mapping + deposit>"
             per_particle = MEASURED_TRAFFIC_FUSED_PER_PARTICLE
+            traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_g2p2g on the 1M-particle "
+                              "scaled cube, scaled by particle count")
         else:
             kernel_name = {"GridToParticle": "k_g2p<G2P + return mapping + record>", "ParticleToGrid": "k_p2g"}[dom]
             per_particle = MEASURED_TRAFFIC_PER_PARTICLE[dom]
+            traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum on the medium workload, scaled by "
+                              "particle count")
         step_bytes = STEP_BYTES_PER_PARTICLE * n + STEP_BYTES_PER_ACTIVE_CELL * active
         step_achieved = step_bytes / (elapsed / args.steps) / 1e9
         cpu = None
@@ -396,8 +402,7 @@ def run_ours(args):
             "stages_ms_per_step": {k: v[1] / max(args.steps, 1) for k, v in prof.items()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": per_particle * n if per_particle else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on the medium "
-                                           "workload, scaled by particle count",
+                         "traffic_source": traffic_source,
                          "peak_kind": peak_kind,
                          "kernel": kernel_name,
                          "bytes_per_launch": fused_bytes, "avg_launch_ms": fused_ms},
