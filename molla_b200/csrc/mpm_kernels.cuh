@@ -13,7 +13,7 @@ namespace mpm {
 constexpr int kParticleThreads = 256;
 constexpr int kGatherThreads = 128;
 constexpr int kScatterThreads = 192;  // 64 cells x 3 x-slabs of one tile
-constexpr int kFusedThreads = 256;    // fused gather + scatter: 2 CTAs of 128-register threads per SM
+constexpr int kFusedThreads = 256;    // fused gather + scatter: 2 CTAs per SM (128 registers per thread)
 constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 256-cell block
 
 enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };

@@ -1,7 +1,8 @@
 // mpm_particles.cu — the particle kernels of the B200 MLS-MPM substep.
 //
 // One substep of the reference (crates/molla-solvers/src/mpm.rs:2476-2551:
-// reset_grid, p2g, grid_update, g2p, plasticity) runs as three launches:
+// reset_grid, p2g, grid_update, g2p, plasticity) runs as three launches
+// (two for small groups, where the gather and scatter are fused):
 //
 //   grid_update(n)  acc[a] -> velocity, clears acc[b]               (grid sweep)
 //   gather(n)       G2P(n) + F update + return mapping(n); writes the particle
