@@ -41,13 +41,14 @@ UNIT = "particle-steps/s"
 
 # Algorithmic bytes per launch of the two particle kernels (FP32 state):
 #  gather (G2P + F update + return mapping + stress record): reads pos 12,
-#    F 36, jp 4, mass 4, volume 4, material 4 = 64 B and writes pos 12, vel 12,
-#    C 36, F 36, jp 4 and the 64-byte scatter record (x, m, m v, B) = 164 B per
-#    particle; reads the grid velocity once per active node (16 B).
+#    F 36, jp 4, mass 4, volume 4, material 4 = 64 B and writes pos 12, F 36,
+#    jp 4 and the 64-byte scatter record (x, m, m v, B) = 116 B per particle
+#    (velocity and C are written only by the last substep of a call); reads
+#    the grid velocity once per active node (16 B).
 #  scatter (P2G deposit): reads the 64-byte record per particle; adds one
 #    float4 accumulator per active node (16 B).
 KERNEL_BYTES = {
-    "GridToParticle": (228, 16),
+    "GridToParticle": (180, 16),
     "ParticleToGrid": (64, 16),
 }
 # DRAM bytes per particle per launch (dram__bytes_read.sum +
@@ -58,10 +59,10 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
     "GridToParticle": 204.9,
     "ParticleToGrid": 69.2,
 }
-# The fused gather + scatter (k_g2p2g, groups of at most 2M particles) keeps
-# the 64-byte record in shared memory: 228 - 64 B per particle, and per
+# The fused gather + scatter (k_g2p2g, groups of at most 1.5M particles)
+# keeps the 64-byte record in shared memory: 180 - 64 B per particle, and per
 # active node the velocity read plus the float4 deposit.
-FUSED_BYTES = (164, 32)
+FUSED_BYTES = (116, 32)
 # ncu DRAM bytes per particle of k_g2p2g on the 1M-particle scaled cube
 # (state 160 MB, just above L2).
 MEASURED_TRAFFIC_FUSED_PER_PARTICLE = 118.7

@@ -342,14 +342,21 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
           // G2P results are published even when the return mapping
           // faults (the reference's g2p and plasticity are separate
           // dispatches); only the plasticity update is withheld.
+          // v and C are read by nothing before the next call (the next
+          // gather recomputes them from the grid; the scatter takes the
+          // record), so a substep that writes a record skips them unless
+          // the return mapping faulted: the last substep of a call
+          // publishes them.
           plane(p, PX)[s] = x;
           plane(p, PY)[s] = y;
           plane(p, PZ)[s] = z;
-          plane(p, VX)[s] = v[0];
-          plane(p, VY)[s] = v[1];
-          plane(p, VZ)[s] = v[2];
+          if (!kScatter || !ok) {
+            plane(p, VX)[s] = v[0];
+            plane(p, VY)[s] = v[1];
+            plane(p, VZ)[s] = v[2];
 #pragma unroll
-          for (int i = 0; i < 9; ++i) plane(p, C0 + i)[s] = C[i];
+            for (int i = 0; i < 9; ++i) plane(p, C0 + i)[s] = C[i];
+          }
 #pragma unroll
           for (int i = 0; i < 9; ++i) plane(p, F0 + i)[s] = F[i];
           plane(p, JP)[s] = jp;
