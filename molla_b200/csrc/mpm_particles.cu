@@ -497,11 +497,11 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 //     shared memory with warp-aggregated counters), so particles that moved
 //     since the regrouping are grouped with their new cell-mates; one whose
 //     stencil leaves the block deposits straight to HBM;
-//  3. deposit: thread t takes x-slab i = t / 64 of the stencil and one cell
-//     (t mod 64): the tile's own cells in the order of their particle counts
-//     at the regrouping, so that the lanes of a warp walk lists of similar
-//     length, then the non-empty margin cells particles moved into (listed
-//     by the scan of step 2).  It adds the nine
+//  3. deposit: a thread takes one x-slab i of the stencil and one cell: the
+//     tile's own cells in the order of their particle counts at the
+//     regrouping, the three slabs of a cell in adjacent lanes, then the
+//     non-empty margin cells particles moved into (listed by the scan of
+//     step 2).  It adds the nine
 //     slab-i node contributions of its cell's particles in registers and
 //     issues 9 x 4 shared-memory atomics for the whole cell, not per
 //     particle; the lanes of a warp own different cells, so those atomics
@@ -676,20 +676,23 @@ __device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bo
   __syncthreads();
 }
 
-// Scatter step 3 (deposit) for a CTA of T >= 192 threads.  Thread t < 192
-// takes x-slab t / 64 of the stencil and one of the tile's own 64 cells, in
-// the order of their particle counts at the regrouping (`order`), so that the
-// lanes of a warp walk lists of similar length; then all T threads share the
-// (margin cell, slab) pairs of the non-empty cells particles moved into (the
-// compact list the scan built; scanning all 152 margin cells per item cost
-// 10% of the scatter).  A thread adds
-// the nine slab nodes of its cell's particles in registers and issues 9 x 4
-// shared-memory atomics for the whole cell; the lanes of a warp own
-// different cells, so those atomics do not collide.
+// Scatter step 3 (deposit) for a CTA of T >= 192 threads.  The first 192
+// threads take the (cell, x-slab) pairs of the tile's own 64 cells: each
+// warp holds 10 cells in the order of their particle counts at the
+// regrouping (`order`), so that its lanes walk lists of similar length, with
+// the three slab threads of a cell in adjacent lanes (a quarter-warp of a
+// 16-byte record load then reads about three records, not eight, and lanes
+// reading the same record share a broadcast: scatter -10%); the two spare
+// lanes of each warp take the four smallest cells.  Then all T threads share
+// the (margin cell, slab) pairs of the non-empty cells particles moved into
+// (the compact list the scan built; scanning all 152 margin cells per item
+// cost 10% of the scatter).  A thread adds the nine slab nodes of its cell's
+// particles in registers and issues 9 x 4 shared-memory atomics for the whole
+// cell; no two lanes of a warp add to the same node.
 template <int T>
 __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t* __restrict__ order, const ItemFrame& f,
                                              ScatterShared& ss) {
-  static_assert(T >= 192, "the core cells take 3 x 64 threads");
+  static_assert(T >= 192, "the core cells take 6 warps of 10 cells x 3 slabs");
   const uint32_t total = ss.total;
   // per node of the slab: (p.x, p.y) and (p.z, m), accumulated in pairs
   float2 axy[9], azm[9];
@@ -753,10 +756,22 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
         atomicAdd(&ss.acc[3][r], azm[3 * j + kk].x);
       }
   };
+  auto core_cell = [&](uint32_t rank) {
+    const uint32_t c = order[rank];
+    return (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
+  };
+  // The three slab threads of a cell sit in adjacent lanes (10 cells per
+  // warp): a quarter-warp of a 16-byte record load then touches about three
+  // records instead of eight, and the lanes that read the same record are
+  // served by one broadcast, so the record loads conflict far less.
+  // 6 warps x 10 cells take ranks 0..59; the two spare lanes of each warp
+  // (12 in all) take the 3 slabs of the four smallest cells, ranks 60..63.
   if (threadIdx.x < 192) {
-    const int slab = (int)(threadIdx.x >> 6);
-    const uint32_t c = order[threadIdx.x & 63u];
-    const int lc = (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t q = warp * 2u + (lane - 30u);  // spare-lane index when lane >= 30
+    const uint32_t rank = lane < 30u ? warp * 10u + lane / 3u : 60u + q / 3u;
+    const int slab = (int)(lane < 30u ? lane % 3u : q % 3u);
+    const int lc = core_cell(rank);
     if (accumulate(lc, slab)) flush(lc, slab);
   }
   // then the (margin cell, slab) pairs of the non-empty margin cells
