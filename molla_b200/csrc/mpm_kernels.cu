@@ -397,13 +397,26 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
   }
 }
 
-// One 64-thread block per item: thread c counts cell c in the item's slot
-// keys (sorted by cell within a tile) by binary search, then ranks it.
+// One 64-thread block per item: the table that gives the scatter's deposit
+// its cell for each of 64 slots.  Slots 10w..10w+9 are warp w's cells (three
+// adjacent lanes each, one per x-slab), slots 60..63 the spare lanes'.
+// A cell's flush atomics use the shared-memory banks b, b+1, b+2 (b the bank
+// of its node row, region_index(x+1, y+1, z+1) mod 32), and every b is the
+// bank of exactly two of the tile's 64 cells.  Cells with b in 0..29 fall
+// into three classes by b mod 3; within a class the runs of the ten b values
+// tile 30 banks without overlap, so the class's two warps take one cell of
+// each b (the one with more particles to the first warp), and a warp's 30
+// flush atomics of one node and channel fall on 30 different banks.  Inside
+// a warp the cells are in the order of their particle counts (thread c
+// counts cell c in the item's slot keys, sorted by cell within a tile, by
+// binary search).  The four cells with b of 30 or 31 go to the spare lanes.
 __global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ items,
                                                    const uint32_t* __restrict__ n_items,
                                                    const uint32_t* __restrict__ slot_key,
                                                    uint8_t* __restrict__ item_order) {
   __shared__ uint32_t s_cnt[64];
+  __shared__ uint8_t s_pair[32][2];
+  __shared__ uint32_t s_fill[32];
   const uint32_t it = blockIdx.x;
   if (it >= *n_items) return;
   const Item item = items[it];
@@ -418,15 +431,50 @@ __global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ item
     }
     return lo;
   };
-  const uint32_t cnt = (c == 63 ? item.count : lower(c + 1)) - lower(c);
-  s_cnt[c] = cnt;
+  if (c < 32) s_fill[c] = 0;
+  s_cnt[c] = (c == 63 ? item.count : lower(c + 1)) - lower(c);
   __syncthreads();
-  uint32_t rank = 0;
-  for (uint32_t o = 0; o < 64; ++o) {
-    const uint32_t oc = s_cnt[o];
-    rank += (oc > cnt) || (oc == cnt && o < c);
+  static_assert(kRsy == 8 && kRsz % 32 == 4, "with these strides every bank is the row bank of two core cells");
+  const uint32_t bank = (((c & 3u) + 1u) + kRsy * (((c >> 2) & 3u) + 1u) + kRsz * ((c >> 4) + 1u)) & 31u;
+  const uint32_t slot = atomicAdd(&s_fill[bank], 1u);
+  if (slot < 2u) s_pair[bank][slot] = (uint8_t)c;
+  __syncthreads();
+  if (c < 4) {
+    uint8_t* out = item_order + (size_t)it * 64;
+    uint8_t a[10], b[10];
+    uint32_t n = 0;
+    auto more = [&](uint8_t x, uint8_t y) {  // x before y: more particles, then lower index
+      return s_cnt[x] > s_cnt[y] || (s_cnt[x] == s_cnt[y] && x < y);
+    };
+    auto sort = [&](uint8_t* v, uint32_t len) {
+      for (uint32_t i = 1; i < len; ++i)
+        for (uint32_t j = i; j > 0 && more(v[j], v[j - 1]); --j) {
+          const uint8_t t = v[j];
+          v[j] = v[j - 1];
+          v[j - 1] = t;
+        }
+    };
+    if (c < 3) {
+      for (uint32_t bb = c; bb < 30; bb += 3, ++n) {
+        const uint8_t x = s_pair[bb][0], y = s_pair[bb][1];
+        a[n] = more(x, y) ? x : y;
+        b[n] = more(x, y) ? y : x;
+      }
+      sort(a, 10);
+      sort(b, 10);
+      for (uint32_t i = 0; i < 10; ++i) {
+        out[20 * c + i] = a[i];
+        out[20 * c + 10 + i] = b[i];
+      }
+    } else {
+      a[0] = s_pair[30][0];
+      a[1] = s_pair[30][1];
+      a[2] = s_pair[31][0];
+      a[3] = s_pair[31][1];
+      sort(a, 4);
+      for (uint32_t i = 0; i < 4; ++i) out[60 + i] = a[i];
+    }
   }
-  item_order[(size_t)it * 64 + rank] = (uint8_t)c;
 }
 
 // Copy one scene's positions / velocities (3 planes from `first`) into a
