@@ -56,8 +56,8 @@ KERNEL_BYTES = {
 # substep on the medium workload (128^3 grid, 2M particles, substep ~250),
 # scaled by particle count.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "GridToParticle": 156.0,
-    "ParticleToGrid": 68.9,
+    "GridToParticle": 156.3,
+    "ParticleToGrid": 69.3,
 }
 # The fused gather + scatter (k_g2p2g, groups of at most 1.5M particles)
 # keeps the 64-byte record in shared memory: 180 - 64 B per particle, and per
@@ -65,7 +65,7 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
 FUSED_BYTES = (116, 32)
 # ncu DRAM bytes per particle of k_g2p2g on the 1M-particle scaled cube
 # (state 160 MB, just above L2).
-MEASURED_TRAFFIC_FUSED_PER_PARTICLE = 77.2
+MEASURED_TRAFFIC_FUSED_PER_PARTICLE = 76.5
 # Whole-step model of the survey (separate P2G and G2P passes):
 # 268 B per particle-step + 56 B per active cell-step.
 STEP_BYTES_PER_PARTICLE = 268
