@@ -59,7 +59,7 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
     "GridToParticle": 156.3,
     "ParticleToGrid": 69.3,
 }
-# The fused gather + scatter (k_g2p2g, groups of at most 1.5M particles)
+# The fused gather + scatter (k_g2p2g, groups of at most 256k particles)
 # keeps the 64-byte record in shared memory: 180 - 64 B per particle, and per
 # active node the velocity read plus the float4 deposit.
 FUSED_BYTES = (116, 32)

@@ -21,9 +21,9 @@
 // kernels because the gather (SVD, return mapping) needs ~128 registers per
 // thread while the scatter needs fewer: split, each runs at its own
 // occupancy, and the B record's round trip through HBM is cheaper than the
-// fused kernel's lower occupancy.  For small groups (a few thousand items,
+// fused kernel's lower occupancy.  For small groups (a few hundred items,
 // about one wave) the fused k_g2p2g keeps the records in shared memory and
-// saves a launch and a wave tail per substep.  The SVD computed
+// saves a launch per substep.  The SVD computed
 // by the return mapping is reused for the next substep's stress; the first
 // substep of every step_n call runs a record-only gather that computes it
 // from F.

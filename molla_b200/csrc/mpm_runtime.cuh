@@ -216,12 +216,12 @@ class Group {
   // Fused gather + scatter for the non-final substeps of the atomic P2G
   // (k_g2p2g): -1 picks it for groups of at most kFusedMaxParticles live
   // particles, 1 always, 0 never (MOLLA_MPM_FUSED=1 / 0 in the environment
-  // at construction).  Measured on a B200: +6% particle-steps/s at 133k
-  // particles, +1.7% at 1M, -4.6% at 2M, -8% at 16M, where the separate
-  // kernels' higher occupancy (4 CTAs per SM each against 2) hides the
-  // per-item barriers better than the fusion saves.
+  // at construction).  Measured on a B200 with the current separate
+  // scatter: even at 133k particles, -2% at 1M, -8% at 16M, where the
+  // separate kernels' higher occupancy (4 CTAs per SM each against 2) hides
+  // the per-item barriers better than the fusion saves.
   int fused_mode = -1;
-  static constexpr uint32_t kFusedMaxParticles = 1500000;
+  static constexpr uint32_t kFusedMaxParticles = 262144;
   bool use_fused() const {
     return !deterministic && (fused_mode > 0 || (fused_mode < 0 && n_live <= kFusedMaxParticles));
   }
