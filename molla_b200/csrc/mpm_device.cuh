@@ -174,9 +174,10 @@ __device__ __forceinline__ T det3(const T* a) {
 //
 // The FP64 form (svd3<double>) is mixed precision, built for the
 // small-strain regime where F^T F = I + O(strain): the Jacobi iteration runs
-// on the shifted matrix A' = F^T F - I (same eigenvectors), formed in FP64
-// and held in FP32, where its entries keep full relative precision however
-// small the strain.  Each rotation angle t = sgn(d) e / (|d| + sqrt(d^2+e^2))
+// on the shifted matrix A' = F^T F - I (same eigenvectors), held in FP32 and
+// formed there as E + E^T + E^T E from the exact E = F - I, so that its
+// entries keep full relative precision however small the strain.  Each
+// rotation angle t = sgn(d) e / (|d| + sqrt(d^2+e^2))
 // (d = a'_qq - a'_pp, e = 2 a'_pq; algebraically 1/(theta + sgn(theta)
 // sqrt(1 + theta^2))) is computed in FP32; V accumulates the same rotations
 // in FP64 with c = (1 + t^2)^(-1/2) Newton-refined to FP64 and s = t c, so V
@@ -284,22 +285,36 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
 }
 
 template <class T>
-__device__ __forceinline__ void svd3(const T* f, SvdOut<T>& o, T tol, int max_sweeps) {
-  // a[col][row] of A = F^T F (FP32 form) or of A' = F^T F - I formed in
-  // FP64 and held in FP32 (FP64 form); symmetric.
+__device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o, T tol, int max_sweeps) {
+  // a[col][row] of A = F^T F (FP32 form) or of A' = F^T F - I (FP64 form);
+  // symmetric.  f32 is the same F in FP32.  The FP64 form builds A' in FP32
+  // from E = F - I, which is exact (diagonal entries in [0.5, 2], Sterbenz;
+  // off-diagonal entries unchanged): A' = E + E^T + E^T E has no cancellation,
+  // so its entries keep full FP32 relative precision however small the
+  // strain, as forming F^T F - I in FP64 and rounding does.
   float a[3][3];
+  if constexpr (sizeof(T) == 4) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int r = c; r < 3; ++r) {
-      const T acr = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
-      if constexpr (sizeof(T) == 4) {
-        a[c][r] = acr;
-      } else {
-        a[c][r] = (float)(r == c ? acr - 1.0 : acr);
+      for (int r = c; r < 3; ++r) {
+        a[c][r] = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
+        a[r][c] = a[c][r];
       }
-      a[r][c] = a[c][r];
-    }
+  } else {
+    float e[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) e[i] = (i % 4 == 0) ? f32[i] - 1.0f : f32[i];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = c; r < 3; ++r) {
+        // (E^T E)_cr + E_rc + E_cr, column-major e[3 col + row]
+        const float ete = e[3 * r] * e[3 * c] + e[3 * r + 1] * e[3 * c + 1] + e[3 * r + 2] * e[3 * c + 2];
+        a[c][r] = (e[3 * c + r] + e[3 * r + c]) + ete;
+        a[r][c] = a[c][r];
+      }
+  }
   T* v = o.v;
 #pragma unroll
   for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? T(1) : T(0);

@@ -300,7 +300,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
           SR Fs[9];
 #pragma unroll
           for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
-          svd3<SR>(Fs, svd, stol, sweeps);
+          svd3<SR>(Fs, F, svd, stol, sweeps);
           float jp_new = jp;
           bool changed = true;
           if (plasticity_project<SR>(svd, md, jp_new, changed)) {
@@ -394,7 +394,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         SR Fs[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) Fs[i] = (SR)F[i];
-        svd3<SR>(Fs, svd, stol, sweeps);
+        svd3<SR>(Fs, F, svd, stol, sweeps);
       }
       p2g_affine<SR>(svd, sc.mat[mat], jp, mass, vol, C, sc.dt, sc.inv_dx, B);
     }
