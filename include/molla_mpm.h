@@ -243,7 +243,10 @@ MPM_API int mpm_set_rigid_spheres(mpm_sim* sim, const float* spheres, uint32_t n
 MPM_API int mpm_read_rigid_wrenches(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
 /* read_positions / read_velocities (mpm.rs:2718-2798): blocking; writes
  * min(count, cap) rows of 3 floats in the original particle order and
- * stores the particle count in *count_out. */
+ * stores the particle count in *count_out.  `out` may be pinned host memory
+ * (the device-to-host copy is then direct).  Velocities (and C) are those of
+ * the last substep of the last step call; after a numerical fault latched in
+ * the middle of a call they may be those of the previous call's end. */
 MPM_API int mpm_read_positions(mpm_sim* sim, float* out, uint32_t cap, uint32_t* count_out);
 /* particle_render_view (crates/molla-solvers/src/mpm_render_view.rs:20-44):
  * live read-only rendering input on the simulation's device.  `positions`
@@ -378,7 +381,7 @@ MPM_API int mpm_group_autotune(mpm_group* group, uint32_t probe_substeps, const 
 MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const uint32_t* candidates,
                          uint32_t n_candidates, float* ms_per_substep, uint32_t* chosen);
 /* Group tuning: regroup (sort) interval in substeps (0 → default 32).  The
- * `chunk` argument is reserved (work items are 4^3 tiles of at most 1008
+ * `chunk` argument is reserved (work items are 4^3 tiles of at most 640
  * particles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
