@@ -758,22 +758,22 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
         atomicAdd(&ss.acc[3][r], azm[3 * j + kk].x);
       }
   };
-  auto core_cell = [&](uint32_t rank) {
-    const uint32_t c = order[rank];
+  // local cell (in the 6^3 frame) of slot `slot` of the item's table
+  auto core_cell = [&](uint32_t slot) {
+    const uint32_t c = order[slot];
     return (int)((c & 3u) + 1) + 6 * ((int)((c >> 2) & 3u) + 1 + 6 * ((int)(c >> 4) + 1));
   };
-  // The three slab threads of a cell sit in adjacent lanes (10 cells per
-  // warp): a quarter-warp of a 16-byte record load then touches about three
-  // records instead of eight, and the lanes that read the same record are
-  // served by one broadcast, so the record loads conflict far less.
-  // 6 warps x 10 cells take ranks 0..59; the two spare lanes of each warp
-  // (12 in all) take the 3 slabs of the four smallest cells, ranks 60..63.
+  // Warp w takes slots 10w..10w+9, the three slab threads of a cell in
+  // adjacent lanes: a quarter-warp of a 16-byte record load then touches
+  // about three records instead of eight, and the lanes that read the same
+  // record are served by one broadcast.  The two spare lanes of each warp
+  // (12 in all) take the 3 slabs of slots 60..63.
   if (threadIdx.x < 192) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t q = warp * 2u + (lane - 30u);  // spare-lane index when lane >= 30
-    const uint32_t rank = lane < 30u ? warp * 10u + lane / 3u : 60u + q / 3u;
+    const uint32_t slot = lane < 30u ? warp * 10u + lane / 3u : 60u + q / 3u;
     const int slab = (int)(lane < 30u ? lane % 3u : q % 3u);
-    const int lc = core_cell(rank);
+    const int lc = core_cell(slot);
     if (accumulate(lc, slab)) flush(lc, slab);
   }
   // then the (margin cell, slab) pairs of the non-empty margin cells
