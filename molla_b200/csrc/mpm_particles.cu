@@ -498,14 +498,13 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 //     since the regrouping are grouped with their new cell-mates; one whose
 //     stencil leaves the block deposits straight to HBM;
 //  3. deposit: a thread takes one x-slab i of the stencil and one cell: the
-//     tile's own cells in the order of their particle counts at the
-//     regrouping, the three slabs of a cell in adjacent lanes, then the
-//     non-empty margin cells particles moved into (listed by the scan of
-//     step 2).  It adds the nine
-//     slab-i node contributions of its cell's particles in registers and
-//     issues 9 x 4 shared-memory atomics for the whole cell, not per
-//     particle; the lanes of a warp own different cells, so those atomics
-//     do not collide;
+//     tile's own cells as the regrouping dealt them to warps (so that a
+//     warp's flush atomics fall on distinct banks, count-ordered within the
+//     warp), the three slabs of a cell in adjacent lanes, then the non-empty
+//     margin cells particles moved into (listed by the scan of step 2).  It
+//     adds the nine slab-i node contributions of its cell's particles in
+//     registers and issues 9 x 4 shared-memory atomics for the whole cell,
+//     not per particle; no two lanes of a warp add to the same node;
 //  4. flush: every non-empty node of the 8^3 block goes to HBM with one
 //     float4 atomic and is cleared for the next item.
 // Every wait on the stage is bounded (about one second); a wait that gives
