@@ -649,11 +649,11 @@ int mpm_batch_submit(mpm_batch* batch) {
     mpm_sim* sim = batch->sim;
     sim->eng->check();
     cudaStream_t st = batch->stream;
-    cudaEvent_t ev = nullptr;
+    std::unique_ptr<mpm::OwnedEvent> ev;
     if (st != sim->eng->stream) {
-      MPM_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-      MPM_CK(cudaEventRecord(ev, sim->eng->stream));
-      MPM_CK(cudaStreamWaitEvent(st, ev, 0));
+      ev.reset(new mpm::OwnedEvent(cudaEventDisableTiming));
+      MPM_CK(cudaEventRecord(*ev, sim->eng->stream));
+      MPM_CK(cudaStreamWaitEvent(st, *ev, 0));
     }
     for (const auto& w : batch->work) {
       sim->dt = w.first;
@@ -662,9 +662,8 @@ int mpm_batch_submit(mpm_batch* batch) {
     }
     if (!batch->work.empty()) sim->refresh_render(st);
     if (ev) {
-      MPM_CK(cudaEventRecord(ev, st));
-      MPM_CK(cudaStreamWaitEvent(sim->eng->stream, ev, 0));
-      cudaEventDestroy(ev);
+      MPM_CK(cudaEventRecord(*ev, st));
+      MPM_CK(cudaStreamWaitEvent(sim->eng->stream, *ev, 0));
     }
     batch->done = true;
   });
@@ -1071,7 +1070,7 @@ struct mpm_server {
   uint64_t next_id = 1;
   uint64_t admitted = 0, completed = 0, particle_steps = 0;
   std::vector<double> tick_ms, queue_ms;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::unique_ptr<mpm::OwnedEvent> e0, e1;  // tick timing
 };
 
 extern "C" {
@@ -1092,8 +1091,8 @@ int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t ma
       const uint64_t particles = std::min<uint64_t>(hbm_budget_bytes / 5 * 3 / per_particle, 0x7fff0000ull);
       const uint64_t cells = hbm_budget_bytes / 5 * 2 / 48ull;
       s->g.reset(new mpm::Group(s->eng, std::max<uint32_t>(max_scenes, 1), particles, cells));
-      MPM_CK(cudaEventCreate(&s->e0));
-      MPM_CK(cudaEventCreate(&s->e1));
+      s->e0.reset(new mpm::OwnedEvent());
+      s->e1.reset(new mpm::OwnedEvent());
     } catch (...) {
       delete s;
       throw;
@@ -1105,8 +1104,6 @@ int mpm_server_create(mpm_engine* engine, uint64_t hbm_budget_bytes, uint32_t ma
 int mpm_server_destroy(mpm_server* server) {
   return guard([&] {
     if (!server) return;
-    if (server->e0) cudaEventDestroy(server->e0);
-    if (server->e1) cudaEventDestroy(server->e1);
     delete server;
   });
 }
@@ -1177,12 +1174,12 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         if (server->queue.empty()) break;
         continue;
       }
-      MPM_CK(cudaEventRecord(server->e0, server->eng->stream));
+      MPM_CK(cudaEventRecord(*server->e0, server->eng->stream));
       g.step(len, server->eng->stream);
-      MPM_CK(cudaEventRecord(server->e1, server->eng->stream));
-      MPM_CK(cudaEventSynchronize(server->e1));
+      MPM_CK(cudaEventRecord(*server->e1, server->eng->stream));
+      MPM_CK(cudaEventSynchronize(*server->e1));
       float ms = 0.f;
-      MPM_CK(cudaEventElapsedTime(&ms, server->e0, server->e1));
+      MPM_CK(cudaEventElapsedTime(&ms, *server->e0, *server->e1));
       server->tick_ms.push_back(ms / (float)len);
       server->particle_steps += parts * len;
       // retire finished scenes

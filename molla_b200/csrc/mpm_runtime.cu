@@ -753,9 +753,7 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
   const uint64_t done0 = substeps_done;
   const uint32_t interval0 = sort_interval;
   save(true);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  MPM_CK(cudaEventCreate(&e0));
-  MPM_CK(cudaEventCreate(&e1));
+  OwnedEvent e0, e1;
   float best = 1e30f;
   uint32_t best_i = interval0;
   for (int c = 0; c < n_cands; ++c) {
@@ -786,8 +784,6 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
       best_i = cands[c];
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   cur = cur0;
   acc_zero = az0;
   acc_last = al0;

@@ -62,6 +62,18 @@ template <class T> struct DevBuf {
   size_t bytes() const { return count * sizeof(T); }
 };
 
+// An owned CUDA event, destroyed on every exit path (errors are thrown).
+struct OwnedEvent {
+  cudaEvent_t ev = nullptr;
+  explicit OwnedEvent(unsigned flags = cudaEventDefault) { MPM_CK(cudaEventCreateWithFlags(&ev, flags)); }
+  OwnedEvent(const OwnedEvent&) = delete;
+  OwnedEvent& operator=(const OwnedEvent&) = delete;
+  ~OwnedEvent() {
+    if (ev) cudaEventDestroy(ev);
+  }
+  operator cudaEvent_t() const { return ev; }
+};
+
 // Per-stage GPU timing (the equivalent of molla's MpmProfileStage timestamp
 // queries, crates/molla-solvers/src/mpm_profile.rs:8-80): when enabled, each
 // launch of a stage is bracketed by CUDA events on the launching stream.
