@@ -195,7 +195,9 @@ MPM_API int mpm_set_material(mpm_sim* sim, float youngs, float friction_angle);
 MPM_API int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters);
 
 /* set_p2g_mode (mpm.rs:1642-1650).  Both reference modes map to the same
- * tile-accumulated scatter here; the flag is kept for API parity. */
+ * tile-accumulated scatter here; the flag is kept for API parity.  As in the
+ * reference it also turns deterministic P2G off and makes prepared steps
+ * stale. */
 MPM_API int mpm_set_p2g_mode(mpm_sim* sim, int two_pass);
 /* prepare_deterministic_p2g / set_deterministic_p2g
  * (mpm_deterministic_p2g.rs:419-569): fixed-order P2G over particles
@@ -205,6 +207,30 @@ MPM_API int mpm_set_p2g_mode(mpm_sim* sim, int two_pass);
  * the grid) sets bit 4 of the status word. */
 MPM_API int mpm_prepare_deterministic_p2g(mpm_sim* sim);
 MPM_API int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled);
+/* release_deterministic_p2g (mpm_deterministic_p2g.rs:606-617): forgets the
+ * prepare call (particle ordering stays); refused with MPM_ERR_INVALID while
+ * deterministic P2G is enabled.  Prepared steps go stale if it was prepared. */
+MPM_API int mpm_release_deterministic_p2g(mpm_sim* sim);
+
+/* The switches and counts the reference's getters return. */
+typedef struct mpm_sim_info {
+  uint32_t particle_count;          /* particle_count (mpm.rs:1250-1252) */
+  uint32_t uses_two_pass_p2g;       /* uses_two_pass_p2g (mpm.rs:1689-1694): the
+                                       set_p2g_mode flag (default 1), 0 while
+                                       deterministic P2G is enabled */
+  uint32_t deterministic_p2g;       /* deterministic_p2g_enabled
+                                       (mpm_deterministic_p2g.rs:571-573) */
+  uint32_t deterministic_prepared;  /* prepared and not released */
+  uint32_t tile_ordering;           /* particle_tile_ordering_enabled
+                                       (mpm_particle_order.rs:265-267) */
+  uint32_t tile_ordering_capacity;  /* prepared capacity, 0 if never prepared */
+  uint32_t sort_interval;           /* regroup interval in effect (substeps) */
+  uint32_t max_particles;           /* capacity fixed at creation */
+} mpm_sim_info;
+MPM_API int mpm_sim_info_get(mpm_sim* sim, mpm_sim_info* out);
+/* config (mpm.rs:1245-1247): the configuration with every later setter
+ * (rheology, material, time step) applied. */
+MPM_API int mpm_sim_config(mpm_sim* sim, mpm_config* out);
 
 /* prepare_particle_tile_ordering (mpm_particle_order.rs:161-230): capacity in
  * 1..=max_particles and >= the live count. */

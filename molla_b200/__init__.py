@@ -450,6 +450,29 @@ class MpmSimulation:
     def set_deterministic_p2g(self, enabled: bool):
         _check(_ffi.lib().mpm_set_deterministic_p2g(self._h, int(bool(enabled))))
 
+    def release_deterministic_p2g(self):
+        _check(_ffi.lib().mpm_release_deterministic_p2g(self._h))
+
+    def _info(self) -> _ffi.mpm_sim_info:
+        i = _ffi.mpm_sim_info()
+        _check(_ffi.lib().mpm_sim_info_get(self._h, C.byref(i)))
+        return i
+
+    def uses_two_pass_p2g(self) -> bool:
+        return bool(self._info().uses_two_pass_p2g)
+
+    def deterministic_p2g_enabled(self) -> bool:
+        return bool(self._info().deterministic_p2g)
+
+    def particle_tile_ordering_enabled(self) -> bool:
+        return bool(self._info().tile_ordering)
+
+    def config(self) -> MpmConfig:
+        """The configuration with every later setter applied (mpm.rs:1245-1247)."""
+        c = _ffi.mpm_config()
+        _check(_ffi.lib().mpm_sim_config(self._h, C.byref(c)))
+        return MpmConfig.from_c(c)
+
     def prepare_particle_tile_ordering(self, capacity: int):
         _check(_ffi.lib().mpm_prepare_particle_tile_ordering(self._h, capacity))
 

@@ -95,6 +95,19 @@ class mpm_render_view(C.Structure):
     ]
 
 
+class mpm_sim_info(C.Structure):
+    _fields_ = [
+        ("particle_count", C.c_uint32),
+        ("uses_two_pass_p2g", C.c_uint32),
+        ("deterministic_p2g", C.c_uint32),
+        ("deterministic_prepared", C.c_uint32),
+        ("tile_ordering", C.c_uint32),
+        ("tile_ordering_capacity", C.c_uint32),
+        ("sort_interval", C.c_uint32),
+        ("max_particles", C.c_uint32),
+    ]
+
+
 class mpm_profile_stage(C.Structure):
     _fields_ = [("launches", C.c_uint64), ("total_ms", C.c_double)]
 
@@ -132,6 +145,9 @@ SIGNATURES = {
     "mpm_set_p2g_mode": (I, [P, I]),
     "mpm_prepare_deterministic_p2g": (I, [P]),
     "mpm_set_deterministic_p2g": (I, [P, I]),
+    "mpm_release_deterministic_p2g": (I, [P]),
+    "mpm_sim_info_get": (I, [P, C.POINTER(mpm_sim_info)]),
+    "mpm_sim_config": (I, [P, C.POINTER(mpm_config)]),
     "mpm_prepare_particle_tile_ordering": (I, [P, U32]),
     "mpm_set_particle_tile_ordering": (I, [P, I]),
     "mpm_set_sort_interval": (I, [P, U32]),

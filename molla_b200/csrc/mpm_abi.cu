@@ -96,6 +96,7 @@ struct mpm_sim {
   bool order_enabled = false;
   bool det_prepared = false;
   bool det_enabled = false;
+  bool two_pass = true;  // set_p2g_mode flag (API parity; one scatter serves both)
   uint32_t sort_interval = 0;
   std::vector<float> spheres;  // rigid spheres, 7 floats each (kept across set_particles)
   mpm::DevBuf<float4> render;  // render view positions (max_particles float4), allocated on first use
@@ -530,7 +531,7 @@ int mpm_set_time_step(mpm_sim* sim, uint32_t kind, uint32_t jacobi_iters) {
 int mpm_set_p2g_mode(mpm_sim* sim, int two_pass) {
   return guard([&] {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
-    (void)two_pass;
+    sim->two_pass = two_pass != 0;
     sim->det_enabled = false;
     sim->group->set_deterministic(false);
     sim->invalidate();
@@ -555,6 +556,40 @@ int mpm_set_deterministic_p2g(mpm_sim* sim, int enabled) {
     sim->det_enabled = enabled != 0;
     sim->group->set_deterministic(sim->det_enabled);
     sim->invalidate();
+  });
+}
+
+int mpm_release_deterministic_p2g(mpm_sim* sim) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    REQUIRE(!sim->det_enabled, MPM_ERR_INVALID, "Disable deterministic P2G before releasing it");
+    if (sim->det_prepared) {
+      sim->det_prepared = false;
+      sim->invalidate();
+    }
+  });
+}
+
+int mpm_sim_info_get(mpm_sim* sim, mpm_sim_info* out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    mpm_sim_info i{};
+    i.particle_count = sim->count;
+    i.uses_two_pass_p2g = sim->two_pass && !sim->det_enabled;
+    i.deterministic_p2g = sim->det_enabled;
+    i.deterministic_prepared = sim->det_prepared;
+    i.tile_ordering = sim->order_enabled;
+    i.tile_ordering_capacity = sim->order_prepared ? sim->order_capacity : 0u;
+    i.sort_interval = sim->group->sort_interval;
+    i.max_particles = sim->cfg.max_particles;
+    *out = i;
+  });
+}
+
+int mpm_sim_config(mpm_sim* sim, mpm_config* out) {
+  return guard([&] {
+    REQUIRE(sim && out, MPM_ERR_INVALID, "null argument");
+    *out = sim->cfg;
   });
 }
 

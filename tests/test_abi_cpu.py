@@ -79,17 +79,19 @@ def test_struct_layout_matches_c_header(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "molla_mpm.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(mpm_rheology), sizeof(mpm_config),'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(mpm_rheology), sizeof(mpm_config),'
         ' sizeof(mpm_status_info), sizeof(mpm_server_stats), offsetof(mpm_config, rheology),'
         ' offsetof(mpm_config, grid_window_cells), sizeof(mpm_render_view), offsetof(mpm_render_view, source),'
-        ' offsetof(mpm_render_view, live_position_bytes)); return 0;}\n')
+        ' offsetof(mpm_render_view, live_position_bytes), sizeof(mpm_sim_info),'
+        ' offsetof(mpm_sim_info, max_particles)); return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run([cc, "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     exp = [ctypes.sizeof(_ffi.mpm_rheology), ctypes.sizeof(_ffi.mpm_config), ctypes.sizeof(_ffi.mpm_status_info),
            ctypes.sizeof(_ffi.mpm_server_stats), _ffi.mpm_config.rheology.offset,
            _ffi.mpm_config.grid_window_cells.offset, ctypes.sizeof(_ffi.mpm_render_view),
-           _ffi.mpm_render_view.source.offset, _ffi.mpm_render_view.live_position_bytes.offset]
+           _ffi.mpm_render_view.source.offset, _ffi.mpm_render_view.live_position_bytes.offset,
+           ctypes.sizeof(_ffi.mpm_sim_info), _ffi.mpm_sim_info.max_particles.offset]
     assert got == exp
 
 

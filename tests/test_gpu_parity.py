@@ -173,6 +173,90 @@ def test_grid_mass_matches_particle_mass(engine):
     assert abs(tot[0] - exp) / exp < 1e-6 and abs(tot[4] - exp) / exp < 1e-6
 
 
+def jittered_block_1k():
+    """The 10x10x10 block of mpm_perf.rs:377-398: spacing 0.04 from
+    (-0.2, 0.2, -0.2), each coordinate jittered by 0.005 * u, u in [-1, 1]
+    from a 64-bit LCG (multiplier 6364136223846793005, increment
+    1442695040888963407, seed 0xdeadbeef, high 32 bits / u32::MAX)."""
+    s = 0xDEADBEEF
+    mask = (1 << 64) - 1
+
+    def nxt():
+        nonlocal s
+        s = (s * 6364136223846793005 + 1442695040888963407) & mask
+        return float(np.float32(np.float32(s >> 32) / np.float32(0xFFFFFFFF))) * 2.0 - 1.0
+
+    pts = []
+    for ix in range(10):
+        for iy in range(10):
+            for iz in range(10):
+                pts.append([np.float32(-0.2 + 0.04 * ix + 0.005 * nxt()),
+                            np.float32(0.2 + 0.04 * iy + 0.005 * nxt()),
+                            np.float32(-0.2 + 0.04 * iz + 0.005 * nxt())])
+    return np.asarray(pts, np.float32)
+
+
+def test_p2g_modes_agree_with_each_other_and_the_oracle(engine):
+    """mpm_perf.rs:364-477 (legacy vs two-pass P2G): one sand substep of the
+    jittered 1k block on a 32^3 grid, grid mass and momentum compared with
+    the reference's tolerances.  Both reference modes map to the one tiled
+    scatter here, so each is also held to the oracle's grid; the switch
+    turns deterministic P2G off and makes prepared steps stale
+    (mpm.rs:1642-1650)."""
+    cfg = m.MpmConfig.sand()
+    cfg.grid_size = 32
+    cfg.cell_size = 0.05
+    cfg.grid_origin = (-0.8, 0.0, -0.8)
+    cfg.max_particles = 4096
+    pts = jittered_block_1k()
+    dt = 1.0 / 240
+    sim = m.MpmSimulation.new(engine, cfg)
+    grids = []
+    for two_pass in (False, True):
+        sim.set_p2g_mode(two_pass)
+        sim.set_particles(pts)
+        sim.step(dt)
+        grids.append(sim.read_grid_mass_momentum())
+    (m0, p0), (m1, p1) = grids
+    tot0 = m0.sum(dtype=np.float64)
+    assert abs(m1.sum(dtype=np.float64) - tot0) / tot0 < 1e-4
+    dm = np.abs(m1 - m0)
+    assert dm.max() < 1e-4 or (dm / np.maximum(np.abs(m0), 1e-12)).max() < 1e-3
+    assert np.abs(p1 - p0).max() < 1e-3
+    sc = O.make_scene(cfg, [cfg.rheology], dt)
+    st = O.init_state(pts, mass=cfg.particle_mass, volume=cfg.particle_volume)
+    om, op = O.step(sc, st, 1, want_grid=True)
+    for gm, gp in grids:
+        d = np.abs(gm - om)
+        assert np.all((d < 1e-4) | (d / np.maximum(om, 1e-30) < 1e-3))
+        assert np.abs(gp - op).max() < 1e-3
+    # the switch turns deterministic P2G off and makes prepared steps stale;
+    # the getters follow mpm.rs:1245-1252,1689-1694
+    assert sim.uses_two_pass_p2g() and not sim.deterministic_p2g_enabled()
+    sim.prepare_particle_tile_ordering(cfg.max_particles)
+    sim.set_particle_tile_ordering(True)
+    sim.prepare_deterministic_p2g()
+    sim.set_deterministic_p2g(True)
+    assert sim.deterministic_p2g_enabled() and not sim.uses_two_pass_p2g()
+    with pytest.raises(m.SolverError):
+        sim.release_deterministic_p2g()
+    prepared = sim.prepare_step(dt, 1)
+    sim.set_p2g_mode(False)
+    assert not sim.deterministic_p2g_enabled() and not sim.uses_two_pass_p2g()
+    assert sim.particle_tile_ordering_enabled()
+    batch = sim.begin_command_batch()
+    with pytest.raises(m.StaleError):
+        batch.encode_step(prepared)
+    sim.release_deterministic_p2g()
+    with pytest.raises(m.SolverError):
+        sim.set_deterministic_p2g(True)  # released: needs a new prepare call
+    sim.set_p2g_mode(True)
+    assert sim.uses_two_pass_p2g()
+    sim.set_rheology(m.MpmRheology.Snow())
+    got = sim.config()
+    assert got.grid_size == 32 and got.max_particles == 4096 and got.rheology.kind == m.MpmRheology.Snow().kind
+
+
 def test_momentum_drift_closed_system(engine):
     """mpm_gpu.rs:780-837."""
     cfg = m.MpmConfig.sand()
