@@ -32,6 +32,22 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(_ffi.SIGNATURES), set(syms) ^ set(_ffi.SIGNATURES)
 
 
+def test_rust_binding_covers_every_declared_symbol():
+    """The extern "C" blocks a molla maintainer would paste
+    name every entry point of the header with its argument count."""
+    hdr = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "molla_mpm.h").read_text(), flags=re.S)
+    arity = {}
+    for name, args in re.findall(r"MPM_API\s+[\w\s\*]+?\b(mpm_\w+)\s*\(([^)]*)\)\s*;", hdr):
+        arity[name] = len([a for a in args.split(",") if a.strip() and a.strip() != "void"])
+    doc = (ROOT / "INTEGRATION.md").read_text()
+    bound = {}
+    for name, args in re.findall(r"pub fn (mpm_\w+)\(([^)]*)\)", doc, flags=re.S):
+        bound[name] = len([a for a in args.split(",") if a.strip()])
+    assert set(arity) == set(declared_symbols())
+    assert set(bound) == set(arity), set(bound) ^ set(arity)
+    assert {k: v for k, v in bound.items() if arity[k] != v} == {}
+
+
 def test_abi_version_and_error_channel():
     L = _ffi.lib()
     assert L.mpm_abi_version() == 1
