@@ -353,6 +353,14 @@ MPM_API int mpm_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values, u
  * crates/molla-core/src/gpu_metrics.rs:330-381). */
 MPM_API uint64_t mpm_engine_launch_count(mpm_engine* engine);
 
+/* Failure-detection self-test of the scatter's bounded stage wait: one warp
+ * waits on a device barrier that nothing completes, gives up after about
+ * one second and latches the device-wait bit (8) the way the scatter does.
+ * Blocking.  Writes that status word to *fault_bits and the time waited to
+ * *waited_ms (may be NULL); the engine stays usable.  The reference's
+ * equivalent is its device-health check (molla-core engine.rs:76-119). */
+MPM_API int mpm_selftest_device_wait(mpm_engine* engine, uint32_t* fault_bits, double* waited_ms);
+
 /* Per-stage GPU timing, the equivalent of molla's step profiling
  * (prepare_step_profiling / read_step_profile, mpm_profile.rs:542-732):
  * while enabled, each launch of a stage is bracketed by CUDA events on its

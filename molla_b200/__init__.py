@@ -253,6 +253,14 @@ class Engine:
     def launch_count(self) -> int:
         return int(_ffi.lib().mpm_engine_launch_count(self._h))
 
+    def selftest_device_wait(self):
+        """Runs the scatter's bounded-wait timeout path on a barrier nothing
+        completes (about one second).  Returns (fault_bits, waited_ms)."""
+        bits = C.c_uint32()
+        ms = C.c_double()
+        _check(_ffi.lib().mpm_selftest_device_wait(self._h, C.byref(bits), C.byref(ms)))
+        return int(bits.value), float(ms.value)
+
     STAGES = ("ParticleOrdering", "StressRecord", "GridUpdate", "GridToParticle", "ParticleToGrid")
 
     def profile(self, enabled: bool = True):

@@ -131,6 +131,7 @@ SIGNATURES = {
     "mpm_engine_check": (I, [P]),
     "mpm_engine_synchronize": (I, [P]),
     "mpm_engine_launch_count": (U64, [P]),
+    "mpm_selftest_device_wait": (I, [P, U32P, C.POINTER(C.c_double)]),
     "mpm_engine_stream": (P, [P]),
     "mpm_config_preset": (I, [U32, C.POINTER(mpm_config)]),
     "mpm_dp_alpha": (C.c_float, [C.c_float]),

@@ -242,6 +242,27 @@ int mpm_engine_synchronize(mpm_engine* engine) {
 
 uint64_t mpm_engine_launch_count(mpm_engine* engine) { return engine ? engine->e->launches : 0; }
 
+int mpm_selftest_device_wait(mpm_engine* engine, uint32_t* fault_bits, double* waited_ms) {
+  return guard([&] {
+    REQUIRE(engine && fault_bits, MPM_ERR_INVALID, "null argument");
+    mpm::Engine* e = engine->e.get();
+    e->check();
+    mpm::DevBuf<uint32_t> status(1);
+    mpm::DevBuf<unsigned long long> waited(1);
+    MPM_CK(cudaMemsetAsync(status.ptr, 0, sizeof(uint32_t), e->stream));
+    MPM_CK(cudaMemsetAsync(waited.ptr, 0, sizeof(unsigned long long), e->stream));
+    MPM_CK(mpm::launch_selftest_wait(status.ptr, waited.ptr, e->stream));
+    e->launches += 1;
+    uint32_t bits = 0;
+    unsigned long long ns = 0;
+    MPM_CK(cudaMemcpyAsync(&bits, status.ptr, sizeof(bits), cudaMemcpyDeviceToHost, e->stream));
+    MPM_CK(cudaMemcpyAsync(&ns, waited.ptr, sizeof(ns), cudaMemcpyDeviceToHost, e->stream));
+    MPM_CK(cudaStreamSynchronize(e->stream));
+    *fault_bits = bits;
+    if (waited_ms) *waited_ms = (double)ns * 1.0e-6;
+  });
+}
+
 void* mpm_engine_stream(mpm_engine* engine) { return engine ? (void*)engine->e->stream : nullptr; }
 
 int mpm_profile_enable(mpm_engine* engine, int enabled) {

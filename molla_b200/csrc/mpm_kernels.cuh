@@ -24,6 +24,9 @@ cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDe
 // map of the record buffer (16 floats x cap, 64-byte swizzle) built by
 // make_record_map.
 cudaError_t launch_scatter(const PoolDev& p, const CUtensorMap& rec_map, int acc_out, int grid, cudaStream_t st);
+// One warp waits (bounded, about one second) on an mbarrier nothing
+// completes and reports kFaultDeviceWait: the scatter's timeout path.
+cudaError_t launch_selftest_wait(uint32_t* status, unsigned long long* waited_ns, cudaStream_t st);
 bool make_record_map(CUtensorMap* out, const float* rec, uint32_t cap, std::string* err);
 // Deterministic (fixed-order) scatter: per-tile blocks, then a combine pass.
 cudaError_t launch_scatter_det(const PoolDev& p, float4* blocks, int acc_out, int grid, cudaStream_t st);

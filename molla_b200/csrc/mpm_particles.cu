@@ -1225,6 +1225,33 @@ bool make_record_map(CUtensorMap* out, const float* rec, uint32_t cap, std::stri
   return true;
 }
 
+// Self-test of the scatter's bounded stage wait: one warp waits, through the
+// same mbar_wait_bounded, on an mbarrier phase that nothing completes (one
+// expected arrival, none made), then reports the way k_p2g does
+// (kFaultDeviceWait in the status word) and records how long it waited.  No
+// copy is in flight, so the CTA may end there.
+__global__ void __launch_bounds__(32) k_selftest_wait(uint32_t* status, unsigned long long* waited_ns) {
+  __shared__ __align__(8) uint64_t s_bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const uint64_t t0 = global_ns();
+  const bool ok = mbar_wait_bounded(&s_bar, 0u);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) {
+    atomicOr(status, kFaultDeviceWait);
+    *waited_ns = global_ns() - t0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&s_bar)) : "memory");
+}
+
+cudaError_t launch_selftest_wait(uint32_t* status, unsigned long long* waited_ns, cudaStream_t st) {
+  k_selftest_wait<<<1, 32, 0, st>>>(status, waited_ns);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_scatter(const PoolDev& p, const CUtensorMap& rec_map, int acc_out, int grid, cudaStream_t st) {
   k_p2g<<<grid, kScatterThreads, kStageBytes, st>>>(p, rec_map, acc_out);
   return cudaGetLastError();

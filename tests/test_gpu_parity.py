@@ -529,6 +529,21 @@ def test_soil_checkpoint_rejects_incompatible_or_faulted_state(engine):
 
 # ---- fault latch (mpm_numerical_fault_tests.rs:19-100) -----------------------------
 
+def test_bounded_device_wait_reports_and_keeps_the_engine(engine):
+    """The scatter's stage wait, run on a barrier that nothing completes,
+    gives up after about a second, latches the device-wait bit (8) and
+    leaves the context usable: a simulation still steps afterwards."""
+    bits, waited_ms = engine.selftest_device_wait()
+    assert bits == 8
+    assert 900.0 <= waited_ms <= 5000.0
+    cfg = m.MpmConfig.snow()
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles([[0.013, 0.2, 0.017]])
+    sim.step_n(1.0 / 480, 4)
+    st = sim.read_active_grid_status()
+    assert st.completed_substeps == 4 and not st.numerical_fault
+
+
 @pytest.mark.parametrize("bits", [np.nan, np.inf, -np.inf])
 def test_fault_latches_without_repair(engine, bits):
     cfg = m.MpmConfig.sand()
