@@ -38,9 +38,10 @@ __device__ __forceinline__ uint32_t tile_key_of(const SceneDev& sc, float x, flo
 
 }  // namespace
 
-// grid_update (mpm.wgsl:1013-1058) over the grid pool, one block per
-// 256-cell block.  Only blocks the last scatter touched (or a rigid sphere
-// may reach) are converted; the blocks touched by the scatter before it are
+// grid_update (mpm.wgsl:1013-1058) over the grid pool, kGridBlocksPerCta
+// 256-cell pool blocks per thread block, one node of each per thread
+// (grid_node is the per-node body).  Only blocks the last scatter touched
+// (or a rigid sphere may reach) are converted; the blocks touched by the scatter before it are
 // cleared in the other accumulator (ready for the next scatter) and
 // unmarked.  Counts completed substeps.  The rigid-sphere imprint
 // (rigid_imprint, mpm.wgsl:939-1003) is fused in front of the conversion: a
@@ -48,32 +49,14 @@ __device__ __forceinline__ uint32_t tile_key_of(const SceneDev& sc, float x, flo
 // 1e6, its sand mass and momentum give the reaction wrench, and the node is
 // marked rigid (negative w in the velocity buffer) so that gravity, walls
 // and the implicit sweeps leave it alone.
-__global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
-                                                              uint64_t total_cells, int acc_in, int count_substep) {
-  static_assert(kCellThreads == kCellBlock, "one thread block per grid-pool block");
-  const uint64_t blk = blockIdx.x;
-  const uint64_t g = blk * kCellThreads + threadIdx.x;
-  if (blk * kCellThreads >= total_cells) return;
-  const uint32_t sid = block_scene[blk];
-  if (sid == 0xffffffffu) return;
-  const bool in_a = p.touched[acc_in][blk] != 0;
-  const bool in_b = p.touched[acc_in ^ 1][blk] != 0;
-  const bool rb = p.rigid_blocks[blk] != 0;
-  if (in_b) p.acc[acc_in ^ 1][g] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const SceneDev& sc = p.scenes[sid];
-  const uint64_t local64 = g - sc.grid_off;
+constexpr int kGridBlocksPerCta = 4;
+
+__device__ __forceinline__ void grid_node(const PoolDev& p, uint32_t sid, const SceneDev& sc, uint64_t blk,
+                                          uint64_t g, float4 a, bool in_a, bool rb, int acc_in) {
   const uint32_t n = sc.n;
-  if (count_substep && local64 == 0) {
-    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
-    if (*(volatile uint32_t*)status == 0u) atomicAdd(status + 1, 1u);
-  }
-  __syncthreads();  // every thread has read the marks
-  if (threadIdx.x == 0 && in_b) p.touched[acc_in ^ 1][blk] = 0;
-  if ((!in_a && !rb) || local64 >= (uint64_t)n * n * n) return;
-  const uint32_t local = (uint32_t)local64;  // grids hold fewer than 2^32 cells
+  const uint32_t local = (uint32_t)(g - sc.grid_off);  // grids hold fewer than 2^32 cells
   const uint32_t q = local / n;
   const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
-  float4 a = p.acc[acc_in][g];
   bool rigid = false;
   if (rb && sc.n_rigid) {
     const float node[3] = {sc.ox + (float)(ix + sc.winx) * sc.dx, sc.oy + (float)(iy + sc.winy) * sc.dx,
@@ -130,6 +113,53 @@ __global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const u
     if (iz >= nn - pad) { v[2] = fminf(v[2], 0.f); v[0] *= f; v[1] *= f; }
   }
   p.vel[g] = make_float4(v[0], v[1], v[2], m);
+}
+
+__global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
+                                                              uint64_t total_cells, int acc_in, int count_substep) {
+  static_assert(kCellThreads == kCellBlock, "one thread per cell of a grid-pool block");
+  constexpr int K = kGridBlocksPerCta;
+  // Every load of the marks and of the accumulators is issued before any is
+  // used, so that a thread keeps K requests in flight.
+  uint32_t sid[K];
+  bool in_a[K], in_b[K], rb[K], conv[K];
+  float4 acc_v[K];
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    const uint64_t blk = (uint64_t)blockIdx.x * K + b;
+    const bool exists = blk * kCellThreads < total_cells;
+    sid[b] = exists ? block_scene[blk] : 0xffffffffu;
+    in_a[b] = exists && p.touched[acc_in][blk] != 0;
+    in_b[b] = exists && p.touched[acc_in ^ 1][blk] != 0;
+    rb[b] = exists && p.rigid_blocks[blk] != 0;
+  }
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    conv[b] = false;
+    if (sid[b] == 0xffffffffu) continue;
+    const uint64_t g = ((uint64_t)blockIdx.x * K + b) * kCellThreads + threadIdx.x;
+    if (in_b[b]) p.acc[acc_in ^ 1][g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const SceneDev& sc = p.scenes[sid[b]];
+    const uint64_t local64 = g - sc.grid_off;
+    if (count_substep && local64 == 0) {
+      uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
+      if (*(volatile uint32_t*)status == 0u) atomicAdd(status + 1, 1u);
+    }
+    conv[b] = (in_a[b] || rb[b]) && local64 < (uint64_t)sc.n * sc.n * sc.n;
+    if (conv[b]) acc_v[b] = p.acc[acc_in][g];
+  }
+  __syncthreads();  // every thread has read the marks
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int b = 0; b < K; ++b)
+      if (sid[b] != 0xffffffffu && in_b[b]) p.touched[acc_in ^ 1][(uint64_t)blockIdx.x * K + b] = 0;
+  }
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    if (!conv[b]) continue;
+    const uint64_t blk = (uint64_t)blockIdx.x * K + b;
+    grid_node(p, sid[b], p.scenes[sid[b]], blk, blk * kCellThreads + threadIdx.x, acc_v[b], in_a[b], rb[b], acc_in);
+  }
 }
 
 // mpm_rigid_force_integrate (mpm.wgsl:1175-1228): every non-rigid node with
@@ -555,7 +585,8 @@ __global__ void k_totals(PoolDev p, int acc_idx, uint64_t grid_off, uint64_t cel
 
 cudaError_t launch_grid_update(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
                                int count_substep, cudaStream_t st) {
-  const uint64_t blocks = (total_cells + kCellThreads - 1) / kCellThreads;
+  const uint64_t pool_blocks = (total_cells + kCellThreads - 1) / kCellThreads;
+  const uint64_t blocks = (pool_blocks + kGridBlocksPerCta - 1) / kGridBlocksPerCta;
   if (blocks == 0) return cudaSuccess;
   k_grid_update<<<(unsigned)blocks, kCellThreads, 0, st>>>(p, block_scene, total_cells, acc_in, count_substep);
   return cudaGetLastError();
