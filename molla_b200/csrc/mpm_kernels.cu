@@ -115,7 +115,7 @@ __device__ __forceinline__ void grid_node(const PoolDev& p, uint32_t sid, const 
   p.vel[g] = make_float4(v[0], v[1], v[2], m);
 }
 
-__global__ void __launch_bounds__(kCellThreads) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
+__global__ void __launch_bounds__(kCellThreads, 5) k_grid_update(PoolDev p, const uint32_t* __restrict__ block_scene,
                                                               uint64_t total_cells, int acc_in, int count_substep) {
   static_assert(kCellThreads == kCellBlock, "one thread per cell of a grid-pool block");
   constexpr int K = kGridBlocksPerCta;
