@@ -109,7 +109,6 @@ struct mpm_sim {
     return {cfg.rheology};
   }
   void apply_group_settings() {
-    group->svd_fp64 = cfg.svd_precision == MPM_SVD_FP64;
     const uint32_t interval = order_enabled ? 1u : (sort_interval ? sort_interval : 32u);
     group->sort_interval = interval;
   }
@@ -973,7 +972,6 @@ int mpm_group_add_scene(mpm_group* group, const mpm_config* cfg, const mpm_rheol
       for (uint32_t i = 0; i < n; ++i)
         REQUIRE(ids_or_null[i] < r.size(), MPM_ERR_INVALID, "particle material id out of range");
     *scene_id = group->g->add_scene(*cfg, r, xyz, nullptr, nullptr, nullptr, ids_or_null, n, dt);
-    if (cfg->svd_precision == MPM_SVD_FP64) group->g->svd_fp64 = true;
   });
 }
 
@@ -1195,20 +1193,40 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
   return guard([&] {
     REQUIRE(server && substeps_per_tick > 0, MPM_ERR_INVALID, "invalid argument");
     mpm::Group& g = *server->g;
+    cudaStream_t st = server->eng->stream;
     for (uint32_t tick = 0; tick < ticks; ++tick) {
       // admit in arrival order while the budget and pools allow
       while (!server->queue.empty()) {
         Ticket& t = server->tickets.at(server->queue.front());
+        if (t.steps == 0) {
+          // nothing to step: the result is the submitted state
+          t.result = t.xyz;
+          t.state = 2;
+          t.t_admit = now_ms();
+          server->queue_ms.push_back(t.t_admit - t.t_submit);
+          server->admitted++;
+          server->completed++;
+          server->queue.pop_front();
+          continue;
+        }
         if (server->resident + t.bytes > server->budget) break;
         uint32_t sid = 0;
-        try {
-          sid = g.add_scene(t.cfg, t.rows, t.xyz.data(), nullptr, nullptr, nullptr,
-                            t.ids.empty() ? nullptr : t.ids.data(), t.n, t.dt);
-        } catch (const Error& e) {
-          if (e.code == MPM_ERR_BUSY) break;
-          throw;
+        bool added = false;
+        for (int attempt = 0; attempt < 2 && !added; ++attempt) {
+          try {
+            sid = g.add_scene(t.cfg, t.rows, t.xyz.data(), nullptr, nullptr, nullptr,
+                              t.ids.empty() ? nullptr : t.ids.data(), t.n, t.dt);
+            added = true;
+          } catch (const Error& e) {
+            if (e.code != MPM_ERR_BUSY) throw;
+            // the pools may be held by retired scenes awaiting compaction
+            if (attempt == 0 && g.n_retiring) g.compact(st);
+            else break;
+          }
         }
-        if (t.cfg.svd_precision == MPM_SVD_FP64) g.svd_fp64 = true;
+        if (!added) break;
+        // the scene stops on the device after exactly its requested substeps
+        g.set_scene_budget(sid, t.steps, st);
         t.sid = sid;
         t.state = 1;
         t.t_admit = now_ms();
@@ -1218,35 +1236,34 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         server->queue.pop_front();
         std::vector<float>().swap(t.xyz);
       }
-      // step the resident scenes
-      uint32_t len = substeps_per_tick;
+      // One tick of a fixed length through a captured graph: every resident
+      // scene advances min(remaining, substeps_per_tick) substeps (a scene
+      // whose budget ends inside the tick stands still for the rest of it).
+      const uint32_t len = substeps_per_tick;
       uint64_t parts = 0;
       for (auto& kv : server->tickets)
-        if (kv.second.state == 1) {
-          len = std::min(len, std::max<uint32_t>(kv.second.remaining, 1));
-          parts += kv.second.n;
-        }
+        if (kv.second.state == 1) parts += (uint64_t)kv.second.n * std::min(kv.second.remaining, len);
       if (parts == 0 && g.live_scenes() == 0) {
         if (server->queue.empty()) break;
         continue;
       }
-      MPM_CK(cudaEventRecord(*server->e0, server->eng->stream));
-      g.step(len, server->eng->stream);
-      MPM_CK(cudaEventRecord(*server->e1, server->eng->stream));
+      MPM_CK(cudaEventRecord(*server->e0, st));
+      g.step_graph(len, 1, st);
+      MPM_CK(cudaEventRecord(*server->e1, st));
       MPM_CK(cudaEventSynchronize(*server->e1));
       float ms = 0.f;
       MPM_CK(cudaEventElapsedTime(&ms, *server->e0, *server->e1));
       server->tick_ms.push_back(ms / (float)len);
-      server->particle_steps += parts * len;
-      // retire finished scenes
+      server->particle_steps += parts;
+      // retire finished scenes: their slots go back at the next regrouping
       for (auto& kv : server->tickets) {
         Ticket& t = kv.second;
         if (t.state != 1) continue;
         t.remaining = t.remaining > len ? t.remaining - len : 0;
         if (t.remaining == 0) {
           t.result.resize(3 * (size_t)t.n);
-          if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), server->eng->stream);
-          g.remove_scene(t.sid);
+          if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), st);
+          g.retire_scene(t.sid);
           server->resident -= t.bytes;
           t.state = 2;
           server->completed++;

@@ -32,7 +32,11 @@ enum Plane : int {
 };
 
 constexpr uint32_t kFaultNumerical = 2u;  // mpm.wgsl:229 numerical_fault()
-constexpr uint32_t kStatusWords = 4u;     // [fault bits, completed substeps, spare, spare]
+// Status words per scene: [fault bits, completed substeps, substep budget
+// (0 = unlimited), spare].  A scene with a budget stops after that many
+// substeps: the grid update counts one past the budget and stops counting,
+// and the particle kernels skip a scene whose count is past its budget.
+constexpr uint32_t kStatusWords = 4u;
 constexpr int kMaxMaterials = 8;          // MAX_MPM_MATERIALS, mpm.rs:660
 
 // Work items cover the particles regrouped under one 4^3 tile of base cells
@@ -80,7 +84,7 @@ struct SceneDev {
   uint32_t jacobi_iters;  // semi-implicit sweeps per substep (MpmTimeStep::Implicit), 0 explicit
   float youngs;           // the configuration's Young's modulus (implicit stiffness estimate)
   uint32_t n_rigid;       // rigid spheres of this scene (slots scene * kMaxRigid ...)
-  uint32_t pad_rigid;
+  uint32_t svd64;         // 1: the mixed-precision (FP64) SVD and principal-frame stress, 0: the FP32 reference form
   MatDev mat[kMaxMaterials];
 };
 
@@ -115,12 +119,39 @@ struct PoolDev {
   const uint32_t* slot_key;  // regroup key of each slot: (tile << 6) | cell in tile
   const SceneDev* scenes;
   uint32_t* status;     // kStatusWords per scene
+  // Work list: items of FP32-SVD scenes fill it from slot 0 up (count
+  // n_items[0]), items of FP64-SVD scenes from slot item_top - 1 down (count
+  // n_items[1]), so that each SVD form is one contiguous range of logical
+  // item indices (item_slot).
   const Item* items;
   const uint32_t* n_items;
+  uint32_t item_top;
   const uint8_t* item_order;  // per item: its tile's 64 cells by descending count at the regrouping
 };
 
 __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }
+
+// Slot of logical item i (0 <= i < n_items[0] + n_items[1]): the FP32-SVD
+// items first, then the FP64-SVD items.
+__device__ __forceinline__ uint32_t item_slot(const PoolDev& p, uint32_t n32, uint32_t i) {
+  return i < n32 ? i : p.item_top - 1u - (i - n32);
+}
+
+// Whether a scene's particles stand still this substep: a latched fault, or
+// a substep budget (status word 2) that the completed-substep count (word 1)
+// has passed.
+__device__ __forceinline__ bool scene_frozen(const uint32_t* status) {
+  const volatile uint32_t* s = status;
+  const uint32_t fault = s[0], done = s[1], budget = s[2];
+  return fault != 0u || (budget != 0u && done > budget);
+}
+// Whether this substep is the last one of the scene's budget (its gather then
+// publishes v and C, as the last substep of a call does).
+__device__ __forceinline__ bool budget_ends(const uint32_t* status) {
+  const volatile uint32_t* s = status;
+  const uint32_t done = s[1], budget = s[2];
+  return budget != 0u && done == budget;
+}
 
 // Marks the 256-cell block of grid-pool cell g as holding deposits (the grid
 // update then converts and later clears only marked blocks).

@@ -142,8 +142,11 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_grid_update(PoolDev p, cons
     const SceneDev& sc = p.scenes[sid[b]];
     const uint64_t local64 = g - sc.grid_off;
     if (count_substep && local64 == 0) {
-      uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
-      if (*(volatile uint32_t*)status == 0u) atomicAdd(status + 1, 1u);
+      // completed substeps; a scene with a budget counts one past it and
+      // stops there (its particle kernels then stand still)
+      volatile uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
+      if (status[0] == 0u && (status[2] == 0u || status[1] <= status[2]))
+        atomicAdd(const_cast<uint32_t*>(status) + 1, 1u);
     }
     conv[b] = (in_a[b] || rb[b]) && local64 < (uint64_t)sc.n * sc.n * sc.n;
     if (conv[b]) acc_v[b] = p.acc[acc_in][g];
@@ -397,10 +400,14 @@ __global__ void k_tile_start(const uint32_t* __restrict__ sorted_keys, uint32_t 
 }
 
 // Work items: every occupied tile, cut into chunks of at most `chunk` slots.
-// scene_of_tile is found by a search over the scene key offsets.
+// scene_of_tile is found by a search over the scene key offsets.  Items of
+// FP32-SVD scenes take slots from 0 up (count n_items[0]), items of FP64-SVD
+// scenes slots from item_top - 1 down (count n_items[1]), so that the gather
+// of each SVD form is one launch over a contiguous range.
 __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, const uint32_t* __restrict__ key_offs,
-                        uint32_t n_scenes, const uint32_t* __restrict__ scene_ids, uint32_t chunk,
-                        Item* __restrict__ items, uint32_t* __restrict__ n_items, uint32_t* __restrict__ tile_item) {
+                        uint32_t n_scenes, const uint32_t* __restrict__ scene_ids, const SceneDev* __restrict__ scenes,
+                        uint32_t chunk, uint32_t item_top, Item* __restrict__ items, uint32_t* __restrict__ n_items,
+                        uint32_t* __restrict__ tile_item) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= K) return;
   const uint32_t a = tile_start[t], b = tile_start[t + 1];
@@ -415,15 +422,18 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
   const uint32_t cnt = b - a;
   chunk = chunk ? chunk : cnt;
   const uint32_t pieces = (cnt + chunk - 1) / chunk;
-  const uint32_t base = atomicAdd(n_items, pieces);
-  if (tile_item) tile_item[t] = base;
+  const uint32_t scene = scene_ids[lo];
+  const bool up = scenes[scene].svd64 == 0u;
+  const uint32_t base = atomicAdd(&n_items[up ? 0 : 1], pieces);
   for (uint32_t i = 0; i < pieces; ++i) {
     Item it;
     it.start = a + i * chunk;
     it.count = min(chunk, cnt - i * chunk);
-    it.scene = scene_ids[lo];
+    it.scene = scene;
     it.tile = t - key_offs[lo];
-    items[base + i] = it;
+    const uint32_t slot = up ? base + i : item_top - 1u - (base + i);
+    items[slot] = it;
+    if (tile_item && i == 0) tile_item[t] = slot;
   }
 }
 
@@ -441,14 +451,14 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
 // counts cell c in the item's slot keys, sorted by cell within a tile, by
 // binary search).  The four cells with b of 30 or 31 go to the spare lanes.
 __global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ items,
-                                                   const uint32_t* __restrict__ n_items,
+                                                   const uint32_t* __restrict__ n_items, uint32_t item_top,
                                                    const uint32_t* __restrict__ slot_key,
                                                    uint8_t* __restrict__ item_order) {
   __shared__ uint32_t s_cnt[64];
   __shared__ uint8_t s_pair[32][2];
   __shared__ uint32_t s_fill[32];
-  const uint32_t it = blockIdx.x;
-  if (it >= *n_items) return;
+  const uint32_t it = blockIdx.x;  // an item slot: [0, n_items[0]) or [item_top - n_items[1], item_top)
+  if (it >= n_items[0] && it < item_top - n_items[1]) return;
   const Item item = items[it];
   const uint32_t c = threadIdx.x;
   const uint32_t* keys = slot_key + item.start;
@@ -656,21 +666,22 @@ cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uin
 }
 
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
-                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
-                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st) {
-  cudaMemsetAsync(n_items, 0, sizeof(uint32_t), st);
+                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids,
+                         const SceneDev* scenes, uint32_t chunk, uint32_t item_top, Item* items, uint32_t* n_items,
+                         uint32_t* tile_item, cudaStream_t st) {
+  cudaMemsetAsync(n_items, 0, 2 * sizeof(uint32_t), st);
   if (tile_item) cudaMemsetAsync(tile_item, 0xff, (size_t)(K + 1) * sizeof(uint32_t), st);
   k_tile_start<<<(K + 1 + 255) / 256, 256, 0, st>>>(sorted_keys, n_live, K, shift, tile_start);
   if (K > 0)
-    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, chunk, items, n_items,
-                                             tile_item);
+    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, scenes, chunk, item_top,
+                                             items, n_items, tile_item);
   return cudaGetLastError();
 }
 
-cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, const uint32_t* slot_key,
-                              uint8_t* item_order, uint32_t max_items, cudaStream_t st) {
-  if (!max_items) return cudaSuccess;
-  k_item_order<<<max_items, 64, 0, st>>>(items, n_items, slot_key, item_order);
+cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, uint32_t item_top, const uint32_t* slot_key,
+                              uint8_t* item_order, cudaStream_t st) {
+  if (!item_top) return cudaSuccess;
+  k_item_order<<<item_top, 64, 0, st>>>(items, n_items, item_top, slot_key, item_order);
   return cudaGetLastError();
 }
 

@@ -64,8 +64,8 @@ cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uin
                            cudaStream_t st);
 // Per item the 64 cells of its tile ranked by particle count at this
 // regrouping (descending, ties by cell index): the scatter's lane order.
-cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, const uint32_t* slot_key,
-                              uint8_t* item_order, uint32_t max_items, cudaStream_t st);
+cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, uint32_t item_top, const uint32_t* slot_key,
+                              uint8_t* item_order, cudaStream_t st);
 // Semi-implicit Jacobi sweep `sweep` (src -> dst) over the touched blocks.
 cudaError_t launch_grid_jacobi(const PoolDev& p, const uint32_t* block_scene, uint64_t total_cells, int acc_in,
                                const float4* src, float4* dst, uint32_t sweep, cudaStream_t st);
@@ -74,9 +74,12 @@ cudaError_t launch_rigid_shell(const PoolDev& p, const uint32_t* block_scene, ui
                                cudaStream_t st);
 cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene, uint64_t total_cells,
                             const float4* src, float4* dst, cudaStream_t st);
+// Work list of the regrouped particles (see k_items): FP32-SVD items in slots
+// [0, n_items[0]), FP64-SVD items in [item_top - n_items[1], item_top).
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
-                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids, uint32_t chunk,
-                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);
+                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids,
+                         const SceneDev* scenes, uint32_t chunk, uint32_t item_top, Item* items, uint32_t* n_items,
+                         uint32_t* tile_item, cudaStream_t st);
 cudaError_t launch_pack_positions(const PoolDev& p, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
                                   float4* out, cudaStream_t st);
 cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,

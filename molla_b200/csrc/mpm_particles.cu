@@ -154,7 +154,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 template <int MODE, bool WRITE_KEYS, class SR>
 __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, uint32_t* status,
                                               const float4* __restrict__ vblock, float* fallback, int rx, int ry,
-                                              int rz, int n, SR stol, int sweeps, int reuse_svd, float4 (&rec)[4]) {
+                                              int rz, int n, SR stol, int sweeps, int reuse_svd, bool publish_vc,
+                                              float4 (&rec)[4]) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   float x = plane(p, PX)[s], y = plane(p, PY)[s], z = plane(p, PZ)[s];
@@ -350,7 +351,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
           plane(p, PX)[s] = x;
           plane(p, PY)[s] = y;
           plane(p, PZ)[s] = z;
-          if (!kScatter || !ok) {
+          if (!kScatter || !ok || publish_vc) {
             plane(p, VX)[s] = v[0];
             plane(p, VY)[s] = v[1];
             plane(p, VZ)[s] = v[2];
@@ -428,10 +429,13 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
   __shared__ __align__(16) SceneDev s_sc;
   __shared__ __align__(16) SharedGather s_gath;
   __shared__ uint32_t s_fault;
-  const uint32_t n_items = *p.n_items;
+  // this SVD form's range of the work list: FP32-SVD items, then FP64-SVD items
+  const uint32_t n32 = p.n_items[0];
+  const uint32_t it_lo = sizeof(SR) == 8 ? n32 : 0u;
+  const uint32_t it_hi = sizeof(SR) == 8 ? n32 + p.n_items[1] : n32;
   const SR stol = (SR)tol;
-  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item item = p.items[it];
+  for (uint32_t it = it_lo + blockIdx.x; it < it_hi; it += gridDim.x) {
+    const Item item = p.items[item_slot(p, n32, it)];
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(p.scenes + item.scene);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
@@ -439,7 +443,9 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
     }
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
-    const uint32_t fault0 = *(volatile uint32_t*)status;
+    // a latched fault, a spent substep budget or a retired scene: stand still
+    const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
+    const bool publish_vc = budget_ends(status);
     const uint32_t w = scp->w;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
@@ -464,7 +470,7 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
         const uint32_t s = item.start + k;
         float4 rec[4];
         particle_step<MODE, WRITE_KEYS, SR>(p, sc, s, status, s_gath.vel, s_gath.fallback[threadIdx.x], rx, ry, rz, n,
-                                            stol, sweeps, reuse_svd, rec);
+                                            stol, sweeps, reuse_svd, publish_vc, rec);
         if constexpr (kScatter) {
           float4* r4 = reinterpret_cast<float4*>(p.rec) + 4 * (size_t)s;
           r4[0] = rec[0];
@@ -825,7 +831,8 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
   __shared__ __align__(8) uint64_t s_bar;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
-  const uint32_t n_items = *p.n_items;
+  const uint32_t n32 = p.n_items[0];
+  const uint32_t n_items = n32 + p.n_items[1];
   clear_scatter_shared(ss, kScatterThreads);
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
@@ -835,7 +842,7 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
   // Thread 0 stages item `it` (items of 1..kStageMax particles) as
   // ceil(count / 64) tiles; rows past the item are loaded but not read.
   auto stage = [&](uint32_t it) {
-    const Item nx = p.items[it];
+    const Item nx = p.items[item_slot(p, n32, it)];
     if (nx.count - 1u < (uint32_t)kStageMax) {
       const uint32_t boxes = (nx.count + kStageBoxRows - 1) / kStageBoxRows;
       fence_proxy_async_smem();
@@ -849,12 +856,14 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
   if (threadIdx.x == 0 && blockIdx.x < n_items) stage(blockIdx.x);
   uint32_t parity = 0;
   for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item item = p.items[it];
+    const uint32_t slot = item_slot(p, n32, it);
+    const Item item = p.items[slot];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
-    // A fault latched before this launch freezes the scene; one latched by
-    // this substep's gather is handled per particle (m = 0 in its record).
-    const uint32_t fault0 = *(volatile uint32_t*)status;
+    // A fault latched before this launch (or a spent substep budget, or a
+    // retired scene) freezes the scene; one latched by this substep's gather
+    // is handled per particle (m = 0 in its record).
+    const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
     const ItemFrame f = item_frame(*scp, item, acc, touched);
     const bool staged = item.count - 1u < (uint32_t)kStageMax;
     bool ok = staged;
@@ -864,7 +873,7 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
     }
     const bool live = ok && fault0 == 0;
     bin_item<kScatterThreads>(s_stage, item.count, live, f, ss);
-    if (live) deposit_item<kScatterThreads>(s_stage, p.item_order + (size_t)it * 64, f, ss);
+    if (live) deposit_item<kScatterThreads>(s_stage, p.item_order + (size_t)slot * 64, f, ss);
     if (__syncthreads_or(!ok)) {
       // The stage did not arrive (or the item exceeds the stage): report it,
       // wait once more (bounded) for the copy in flight and stop this CTA.
@@ -902,11 +911,15 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
   __shared__ uint32_t s_fault;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
-  const uint32_t n_items = *p.n_items;
+  // this SVD form's range of the work list: FP32-SVD items, then FP64-SVD items
+  const uint32_t n32 = p.n_items[0];
+  const uint32_t it_lo = sizeof(SR) == 8 ? n32 : 0u;
+  const uint32_t it_hi = sizeof(SR) == 8 ? n32 + p.n_items[1] : n32;
   const SR stol = (SR)tol;
   clear_scatter_shared(ss, kFusedThreads);
-  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item item = p.items[it];
+  for (uint32_t it = it_lo + blockIdx.x; it < it_hi; it += gridDim.x) {
+    const uint32_t slot = item_slot(p, n32, it);
+    const Item item = p.items[slot];
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(p.scenes + item.scene);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
@@ -914,7 +927,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
     }
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
-    const uint32_t fault0 = *(volatile uint32_t*)status;
+    const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
+    const bool publish_vc = budget_ends(status);
     const ItemFrame f = item_frame(*scp, item, acc, touched);
     const bool fits = item.count <= (uint32_t)kStageMax;
     {
@@ -940,13 +954,13 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
         // the record's own stage slot is the scratch of gather_global
         particle_step<kG2PRecord, WRITE_KEYS, SR>(p, s_sc, item.start + k, status, s_vel,
                                                   reinterpret_cast<float*>(s_stage + 4 * (size_t)k), f.rx, f.ry,
-                                                  f.rz, f.n, stol, sweeps, reuse_svd, rec);
+                                                  f.rz, f.n, stol, sweeps, reuse_svd, publish_vc, rec);
         stage_store(s_stage, k, rec);
       }
     }
     __syncthreads();
     bin_item<kFusedThreads>(s_stage, item.count, live, f, ss);
-    if (live) deposit_item<kFusedThreads>(s_stage, p.item_order + (size_t)it * 64, f, ss);
+    if (live) deposit_item<kFusedThreads>(s_stage, p.item_order + (size_t)slot * 64, f, ss);
     __syncthreads();
     flush_item<kFusedThreads>(f, ss);
     __syncthreads();
@@ -969,11 +983,13 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
   __shared__ float s_part[3 * 64 * 9 * 4];
   __shared__ uint32_t s_fault;
   const float4* __restrict__ rec = reinterpret_cast<const float4*>(p.rec);
-  const uint32_t n_items = *p.n_items;
+  const uint32_t n32 = p.n_items[0];
+  const uint32_t n_items = n32 + p.n_items[1];
   const int cell = threadIdx.x & 63;
   const int slab = threadIdx.x >> 6;
   for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item item = p.items[it];
+    const uint32_t slot = item_slot(p, n32, it);
+    const Item item = p.items[slot];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
     const uint32_t w = scp->w;
     const int n = (int)scp->n;
@@ -982,7 +998,7 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
     const uint64_t grid_off = scp->grid_off;
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
-    if (threadIdx.x == 0) s_fault = *(volatile uint32_t*)status;
+    if (threadIdx.x == 0) s_fault = (scene_frozen(status) || !scp->live) ? 1u : 0u;
     if (threadIdx.x < 64) {
       s_first[threadIdx.x] = 0;
       s_end[threadIdx.x] = 0;
@@ -1074,7 +1090,7 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
     // Node (nx, ny, nz) of the 6^3 footprint receives, from cell (cx, cy, cz)
     // with 0 <= n - c <= 2 per axis, the partial sum stored by thread
     // (cell, slab = nx - cx) at index 3 (ny - cy) + (nz - cz).
-    float4* blk = blocks + (size_t)it * kTileNodes;
+    float4* blk = blocks + (size_t)slot * kTileNodes;
     for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
       const int nx = q % 6, ny = (q / 6) % 6, nz = q / 36;
       float sm = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
@@ -1098,8 +1114,9 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
 // it, summed in (tz, ty, tx) order by the first such tile's thread.
 __global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, const uint32_t* __restrict__ tile_item,
                               int acc_out) {
-  const uint32_t it = blockIdx.x;
-  if (it >= *p.n_items) return;
+  const uint32_t n32 = p.n_items[0];
+  if (blockIdx.x >= n32 + p.n_items[1]) return;
+  const uint32_t it = item_slot(p, n32, blockIdx.x);  // the item's slot, as tile_item holds it
   const Item item = p.items[it];
   const SceneDev* __restrict__ scp = p.scenes + item.scene;
   const int w = (int)scp->w, n = (int)scp->n;

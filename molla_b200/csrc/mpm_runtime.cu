@@ -188,6 +188,7 @@ SceneDev make_scene_dev(const mpm_config& cfg, const std::vector<mpm_rheology>& 
   }
   d.n_mat = (uint32_t)rows.size();
   d.live = 1;
+  d.svd64 = cfg.svd_precision == MPM_SVD_FP64 ? 1u : 0u;
   d.jacobi_iters = cfg.time_step == MPM_TIME_STEP_IMPLICIT ? cfg.jacobi_iters : 0u;
   d.youngs = cfg.youngs;
   for (size_t i = 0; i < rows.size() && i < (size_t)kMaxMaterials; ++i) {
@@ -256,7 +257,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   status_d.alloc((size_t)kStatusWords * max_scenes);
   key_offs_d.alloc(max_scenes);
   scene_ids_d.alloc(max_scenes);
-  n_items.alloc(1);
+  n_items.alloc(2);
   totals_d.alloc(8);
   MPM_CK(cudaMallocHost((void**)&scenes_h, sizeof(SceneDev) * max_scenes));
   std::memset(scenes_h, 0, sizeof(SceneDev) * max_scenes);
@@ -317,6 +318,7 @@ PoolDev Group::pool() const {
   p.status = status_d.ptr;
   p.items = items.ptr;
   p.n_items = n_items.ptr;
+  p.item_top = item_top;
   p.item_order = item_order.ptr;
   return p;
 }
@@ -349,14 +351,16 @@ void Group::rebuild_layout() {
     if ((k << kCellBits) >= 0xfffffff0ull) throw Error(MPM_ERR_INVALID, "MPM group key space exceeds 32 bits");
   }
   key_space = (uint32_t)k;
+  layout_scenes = (uint32_t)offs.size();
   if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
   const size_t max_items = max_item_count();
   if (items.count < max_items) items.alloc(max_items);
   if (item_order.count < 64 * max_items) item_order.alloc(64 * max_items);
+  item_top = (uint32_t)max_items;
   if (deterministic) {
     const size_t tiles = (size_t)key_space + 2;
     if (tile_item.count < tiles) tile_item.alloc(tiles);
-    if (det_blocks.count < tiles * kTileNodes) det_blocks.alloc(tiles * kTileNodes);
+    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
   }
   if (!offs.empty()) {
     MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -403,7 +407,7 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   const uint64_t n3 = (uint64_t)cfg.grid_size * cfg.grid_size * cfg.grid_size;
   uint32_t sid = (uint32_t)scenes.size();
   for (uint32_t i = 0; i < scenes.size(); ++i)
-    if (!scenes[i].live) {
+    if (!scenes[i].live && !scenes[i].retiring) {
       sid = i;
       break;
     }
@@ -478,13 +482,14 @@ void Group::remove_scene(uint32_t sid) {
   s.n_rigid = 0;
   rebuild_layout();  // marks the scene record dead, new key offsets
   // Compact: keys of every pooled particle (dead ones get 0xffffffff), sort,
-  // keep the live prefix.
+  // keep the live prefix (scenes retired earlier leave with it).
   sync_scenes(stream);
   const uint32_t n_slots = n_live;
-  n_live -= removed;
   MPM_CK(launch_keys(pool(), n_slots, stream));
   eng->launches += 1;
+  n_live -= removed;
   regroup(false, stream);
+  finish_retirements();
   // Dead identities keep key 0xffffffff for later sorts.
   MPM_CK(cudaMemsetAsync(keys_by_id.ptr + s.id_base, 0xff, (size_t)s.n * 4, stream));
   {
@@ -497,6 +502,68 @@ void Group::remove_scene(uint32_t sid) {
   cells.release(s.grid_off, s.grid_len);
   s.n = 0;
   need_regroup = n_live > 0;
+}
+
+void Group::retire_scene(uint32_t sid) {
+  if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
+  SceneHost& s = scenes[sid];
+  s.live = false;
+  s.retiring = true;
+  s.n_rigid = 0;
+  scenes_h[sid].live = 0;
+  scenes_h[sid].n_rigid = 0;
+  scenes_dirty = true;
+  // Removed-particle keys, so that the next regrouping (the gather does not
+  // write keys for a dead scene) sorts these identities behind every live one.
+  if (s.n) MPM_CK(cudaMemsetAsync(keys_by_id.ptr + s.id_base, 0xff, (size_t)s.n * 4, stream));
+  retiring.push_back(sid);
+  n_retiring += s.n;
+  // The regrouping baked into a captured graph moves a fixed particle count.
+  invalidate_graphs();
+}
+
+void Group::finish_retirements() {
+  if (!compact_issued) return;
+  compact_issued = false;
+  std::vector<uint32_t> bs;
+  for (uint32_t sid : retiring) {
+    SceneHost& s = scenes[sid];
+    bs.assign(s.grid_len / kCellBlock, 0xffffffffu);
+    if (!bs.empty()) {
+      MPM_CK(cudaMemcpyAsync(block_scene.ptr + s.grid_off / kCellBlock, bs.data(), bs.size() * 4,
+                             cudaMemcpyHostToDevice, stream));
+      MPM_CK(cudaStreamSynchronize(stream));  // bs is reused
+    }
+    ids.release(s.id_base, s.n);
+    cells.release(s.grid_off, s.grid_len);
+    n_live -= s.n;
+    s.n = 0;
+    s.retiring = false;
+  }
+  retiring.clear();
+  n_retiring = 0;
+}
+
+void Group::set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st) {
+  if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
+  uint32_t done = 0;
+  MPM_CK(cudaMemcpyAsync(&done, status_d.ptr + (size_t)sid * kStatusWords + 1, 4, cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  const uint32_t budget = substeps ? done + substeps : 0u;
+  MPM_CK(cudaMemcpyAsync(status_d.ptr + (size_t)sid * kStatusWords + 2, &budget, 4, cudaMemcpyHostToDevice, st));
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
+bool Group::any_svd32() const {
+  for (size_t i = 0; i < scenes.size(); ++i)
+    if (scenes[i].live && scenes[i].cfg.svd_precision != MPM_SVD_FP64) return true;
+  return false;
+}
+
+bool Group::any_svd64() const {
+  for (size_t i = 0; i < scenes.size(); ++i)
+    if (scenes[i].live && scenes[i].cfg.svd_precision == MPM_SVD_FP64) return true;
+  return false;
 }
 
 void Group::set_scene_dt(uint32_t sid, float dt) {
@@ -653,34 +720,44 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
                           bits_for((uint64_t)key_space << kCellBits), &skeys, &sids, &eng->launches));
   const float4* rsrc = move_records ? reinterpret_cast<const float4*>(rec[rec_cur].ptr) : nullptr;
   float4* rdst = move_records ? reinterpret_cast<float4*>(rec[rec_cur ^ 1].ptr) : nullptr;
+  // Particles of retired scenes sorted behind the live ones: only the live
+  // prefix moves, which drops them.
+  const uint32_t n_keep = n_live - n_retiring;
   MPM_CK(launch_reorder(planes[cur].ptr, planes[cur ^ 1].ptr, cap, meta[cur].ptr, meta[cur ^ 1].ptr,
-                        orig[cur ^ 1].ptr, slot_of.ptr, sids, skeys, slot_key.ptr, rsrc, rdst, n_live, st));
+                        orig[cur ^ 1].ptr, slot_of.ptr, sids, skeys, slot_key.ptr, rsrc, rdst, n_keep, st));
   eng->launches += 1;
   cur ^= 1;
   if (move_records) rec_cur ^= 1;
+  if (n_retiring) compact_issued = true;
   // Items: whole tiles for the fixed-order scatter (one item per tile);
   // otherwise tiles cut into pieces of at most kStageMax particles, whose
   // scatter records fit the shared-memory stage.
-  MPM_CK(launch_items(skeys, kCellBits, n_live, key_space, tile_start.ptr, key_offs_d.ptr, live_scenes(),
-                      scene_ids_d.ptr, deterministic ? 0u : (uint32_t)kStageMax, items.ptr, n_items.ptr,
-                      deterministic ? tile_item.ptr : nullptr, st));
+  MPM_CK(launch_items(skeys, kCellBits, n_keep, key_space, tile_start.ptr, key_offs_d.ptr, layout_scenes,
+                      scene_ids_d.ptr, scenes_d.ptr, deterministic ? 0u : (uint32_t)kStageMax, item_top, items.ptr,
+                      n_items.ptr, deterministic ? tile_item.ptr : nullptr, st));
   eng->launches += key_space ? 2 : 1;
   if (!deterministic && key_space) {
-    MPM_CK(launch_item_order(items.ptr, n_items.ptr, slot_key.ptr, item_order.ptr, (uint32_t)max_item_count(), st));
+    MPM_CK(launch_item_order(items.ptr, n_items.ptr, item_top, slot_key.ptr, item_order.ptr, st));
     eng->launches += 1;
   }
   need_regroup = false;
+  since = 0;
+  ++regroups;
   eng->prof_end(&pr, st);
 }
 
+// The gather runs once per SVD form present: over the FP32-SVD items, then
+// over the FP64-SVD items of the work list.
 void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
-  const int grid = svd_fp64 ? grid_gather64 : grid_gather32;
-  const double tol = svd_fp64 ? svd_tol64 : svd_tol32;
   ProfRec pr;
   eng->prof_begin(mode == kRecord ? kStageRecord : kStageGather, st, &pr);
-  MPM_CK(launch_gather(mode, keys, svd_fp64, pool(), tol, svd_sweeps, reuse_svd ? 1 : 0, grid, st));
+  for (int f64 = 0; f64 < 2; ++f64) {
+    if (!(f64 ? any_svd64() : any_svd32())) continue;
+    MPM_CK(launch_gather(mode, keys, f64 != 0, pool(), f64 ? svd_tol64 : svd_tol32, svd_sweeps, reuse_svd ? 1 : 0,
+                         f64 ? grid_gather64 : grid_gather32, st));
+    eng->launches += 1;
+  }
   eng->prof_end(&pr, st);
-  eng->launches += 1;
 }
 
 void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
@@ -698,13 +775,15 @@ void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
 }
 
 void Group::launch_fused_pass(int acc_out, bool keys, cudaStream_t st) {
-  const int grid = svd_fp64 ? grid_fused64 : grid_fused32;
-  const double tol = svd_fp64 ? svd_tol64 : svd_tol32;
   ProfRec pr;
   eng->prof_begin(kStageGather, st, &pr);
-  MPM_CK(launch_fused(keys, svd_fp64, pool(), tol, svd_sweeps, reuse_svd ? 1 : 0, acc_out, grid, st));
+  for (int f64 = 0; f64 < 2; ++f64) {
+    if (!(f64 ? any_svd64() : any_svd32())) continue;
+    MPM_CK(launch_fused(keys, f64 != 0, pool(), f64 ? svd_tol64 : svd_tol32, svd_sweeps, reuse_svd ? 1 : 0, acc_out,
+                        f64 ? grid_fused64 : grid_fused32, st));
+    eng->launches += 1;
+  }
   eng->prof_end(&pr, st);
-  eng->launches += 1;
 }
 
 uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_out, cudaStream_t st) {
@@ -750,8 +829,11 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
   };
   const int cur0 = cur, az0 = acc_zero, al0 = acc_last;
   const bool nr0 = need_regroup;
-  const uint64_t done0 = substeps_done;
+  const uint64_t done0 = substeps_done, regroups0 = regroups;
   const uint32_t interval0 = sort_interval;
+  // The probes regroup; retired scenes must not leave the pool behind the
+  // host's back.
+  if (n_retiring) throw Error(MPM_ERR_BUSY, "MPM autotune with retired scenes awaiting compaction");
   save(true);
   OwnedEvent e0, e1;
   float best = 1e30f;
@@ -792,6 +874,8 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
   (void)nr0;
   need_regroup = true;  // the work list belongs to the probes; rebuild it
   substeps_done = done0;
+  regroups = regroups0;
+  since = 0;
   sort_interval = best_i;
   invalidate_graphs();
   return best_i;
@@ -808,9 +892,11 @@ void Group::set_deterministic(bool on) {
       std::string err;
       if (!make_record_map(&rec_map[1], rec[1].ptr, cap, &err)) throw Error(MPM_ERR_GPU, "MPM scatter stage: " + err);
     }
-    const size_t max_items = (size_t)key_space + 2;
-    if (tile_item.count < max_items) tile_item.alloc(max_items);
-    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
+    const size_t tiles = (size_t)key_space + 2;
+    if (tile_item.count < tiles) tile_item.alloc(tiles);
+    // blocks are indexed by item slot (one item per tile in this mode)
+    const size_t slots = std::max<size_t>(item_top, tiles);
+    if (det_blocks.count < slots * kTileNodes) det_blocks.alloc(slots * kTileNodes);
   }
   need_regroup = true;
   invalidate_graphs();
@@ -854,6 +940,20 @@ void Group::jacobi_pass(int a, uint32_t max_jacobi, cudaStream_t st) {
   }
 }
 
+bool Group::regroup_due(uint32_t s, uint32_t substeps) {
+  const bool last = s + 1 == substeps;
+  if (deterministic) return !last;
+  if (sort_interval == 0) return false;
+  if (++since < sort_interval) return false;
+  if (last) {
+    // the last substep of a call writes no record and no keys: the
+    // regrouping opens the next call instead (keys computed there)
+    need_regroup = true;
+    return false;
+  }
+  return true;
+}
+
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   if (need_regroup || deterministic) regroup(true, st);
   const uint32_t max_jacobi = max_jacobi_iters();
@@ -861,7 +961,6 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   launch_gather_pass(kRecord, false, st);
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
-  uint32_t since = 0;
   const bool fused = use_fused();
   for (uint32_t s = 0; s < substeps; ++s) {
     ProfRec pr;
@@ -869,14 +968,11 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
     grid_pass(a, max_jacobi, rigid, st);
     eng->prof_end(&pr, st);
     const bool last = s + 1 == substeps;
-    const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
+    const bool due = regroup_due(s, substeps);
     if (!last && fused) {
       // gather + scatter in one launch; the regrouping follows the deposit
       launch_fused_pass(a ^ 1, due, st);
-      if (due) {
-        regroup(false, st);
-        since = 0;
-      }
+      if (due) regroup(false, st);
       a ^= 1;
       continue;
     }
@@ -889,10 +985,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
         launch_scatter_pass(a ^ 1, st);
       } else {
         launch_scatter_pass(a ^ 1, st);
-        if (due) {
-          regroup(false, st);
-          since = 0;
-        }
+        if (due) regroup(false, st);
       }
       a ^= 1;
     }
@@ -902,11 +995,21 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   substeps_done += substeps;
 }
 
+void Group::compact(cudaStream_t st) {
+  eng->check();
+  if (!n_retiring) return;
+  sync_scenes(st);
+  regroup(true, st);
+  finish_retirements();
+}
+
 void Group::step(uint32_t substeps, cudaStream_t st) {
   eng->check();
-  if (!substeps || !n_live) return;
+  if (substeps && n_live == n_retiring) compact(st);
+  if (!substeps || n_live == 0) return;
   sync_scenes(st);
   run_substeps(substeps, st);
+  finish_retirements();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     eng->note_error(e);
@@ -914,19 +1017,27 @@ void Group::step(uint32_t substeps, cudaStream_t st) {
   }
 }
 
-uint64_t Group::graph_key(uint32_t substeps) const {
-  return ((uint64_t)substeps << 8) | ((uint64_t)rec_cur << 3) | ((uint64_t)cur << 2) | ((uint64_t)acc_zero << 1) |
-         (need_regroup ? 1u : 0u);
+Group::GraphKey Group::graph_key(uint32_t substeps) const {
+  GraphKey k;
+  k.substeps = substeps;
+  k.since = deterministic ? 0u : since;
+  k.interval = sort_interval;
+  k.flags = ((uint32_t)rec_cur << 5) | ((uint32_t)cur << 4) | ((uint32_t)acc_zero << 3) |
+            ((uint32_t)any_svd64() << 2) | ((uint32_t)any_svd32() << 1) | (need_regroup ? 1u : 0u);
+  return k;
 }
 
 void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
   eng->check();
-  if (!substeps || !n_live || !repeat) return;
+  if (substeps && repeat && n_live == n_retiring) compact(st);
+  if (!substeps || n_live == 0 || !repeat) return;
   sync_scenes(st);
   for (uint32_t r = 0; r < repeat; ++r) {
-    const uint64_t key = graph_key(substeps);
-    const int cur0 = cur, az0 = acc_zero;
+    const GraphKey key = graph_key(substeps);
+    const int cur0 = cur, az0 = acc_zero, rc0 = rec_cur;
     const bool nr0 = need_regroup;
+    const uint32_t since0 = since;
+    const uint64_t regroups0 = regroups;
     auto it = graphs.find(key);
     Graph g;
     if (it == graphs.end() || it->second.epoch != epoch) {
@@ -951,41 +1062,44 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
       g.epoch = epoch;
       // run_substeps advanced the host bookkeeping; rewind it, the launch
       // below applies the same transition.
-      const int cur1 = cur, az1 = acc_zero, al1 = acc_last;
       cur = cur0;
       acc_zero = az0;
+      rec_cur = rc0;
       need_regroup = nr0;
+      since = since0;
+      regroups = regroups0;
+      compact_issued = false;
       substeps_done -= substeps;
       if (it != graphs.end() && it->second.exec) cudaGraphExecDestroy(it->second.exec);
       graphs[key] = g;
-      (void)cur1;
-      (void)az1;
-      (void)al1;
     } else {
       g = it->second;
     }
     MPM_CK(cudaGraphLaunch(g.exec, st));
     eng->launches += g.kernels;
-    // Replay the host-side state transition of the captured sequence.
-    uint32_t since = 0;
-    if (need_regroup || deterministic) {
+    // Replay the host-side state transition of the captured sequence (the
+    // same decisions run_substeps made while it was captured).
+    auto regrouped = [&](bool records) {
       cur ^= 1;
+      if (records) rec_cur ^= 1;
       need_regroup = false;
-    }
+      since = 0;
+      ++regroups;
+      if (n_retiring) compact_issued = true;
+    };
+    if (need_regroup || deterministic) regrouped(false);
     int a = acc_zero;
     for (uint32_t s = 0; s < substeps; ++s) {
       const bool last = s + 1 == substeps;
-      const bool due = !last && (deterministic || (sort_interval > 0 && ++since >= sort_interval));
-      if (due) {
-        cur ^= 1;
-        since = 0;
-        if (deterministic) rec_cur ^= 1;
-      }
+      const bool due = regroup_due(s, substeps);
+      if (deterministic && !last) regrouped(true);
+      else if (due) regrouped(false);
       if (!last) a ^= 1;
     }
     acc_last = a;
     acc_zero = a ^ 1;
     substeps_done += substeps;
+    finish_retirements();
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -1057,7 +1171,8 @@ void Group::status(uint32_t sid, mpm_status_info* out, cudaStream_t st) {
   MPM_CK(cudaStreamSynchronize(st));
   out->fault_bits = w[0];
   out->numerical_fault = (w[0] & kFaultNumerical) ? 1u : 0u;
-  out->completed_substeps = w[1];
+  // a scene stopped by its substep budget counts one past it (see k_grid_update)
+  out->completed_substeps = (w[2] != 0u && w[1] > w[2]) ? w[2] : w[1];
   out->reserved = 0;
 }
 

@@ -129,6 +129,7 @@ struct SceneHost {
   uint32_t key_off = 0;
   uint32_t tiles = 0;      // w^3
   uint32_t n_rigid = 0;    // rigid spheres set on this scene
+  bool retiring = false;   // retired, its particles not yet compacted out (the slot is not reusable)
 };
 
 struct Range {
@@ -206,6 +207,9 @@ class Group {
   RangeAlloc ids, cells;
   uint32_t n_live = 0;
   uint32_t key_space = 0;
+  // Scenes listed in key_offs_d / scene_ids_d (those live at the last layout
+  // change; a scene retired since keeps its empty key range until the next).
+  uint32_t layout_scenes = 0;
   int cur = 0;       // current particle buffer
   int acc_zero = 0;  // accumulator known to be all zero
   int acc_last = 1;  // accumulator holding the last scatter
@@ -213,8 +217,21 @@ class Group {
   bool scenes_dirty = true;
   bool keys_dirty = true;  // scene key offsets changed
   uint32_t sort_interval = 32;
+  // Substeps since the last regrouping, carried across calls: the cadence
+  // does not depend on how a caller cuts its stepping into step_n calls (a
+  // regrouping that falls due on a call's last substep opens the next call).
+  uint32_t since = 0;
+  uint64_t regroups = 0;  // regroupings issued (device work enqueued or replayed)
   uint32_t chunk = 512;
-  bool svd_fp64 = false;
+  // Item slots of the work list: FP32-SVD items fill [0, n32), FP64-SVD items
+  // [item_top - n64, item_top) (see k_items).
+  uint32_t item_top = 0;
+  // Scenes retired by retire_scene and not yet compacted out of the pool:
+  // their particles keep their slots (the kernels skip them) until the next
+  // regrouping, which sorts them behind every live particle and drops them.
+  std::vector<uint32_t> retiring;
+  uint32_t n_retiring = 0;    // their particles
+  bool compact_issued = false;  // a regrouping that drops them was enqueued
   bool deterministic = false;
   bool reuse_svd = true;
   double svd_tol32 = 1.0e-7;
@@ -247,12 +264,37 @@ class Group {
     uint64_t kernels = 0;
     uint64_t epoch = 0;
   };
-  std::map<uint64_t, Graph> graphs;
+  struct GraphKey {
+    uint32_t substeps, since, interval, flags;
+    bool operator<(const GraphKey& o) const {
+      if (substeps != o.substeps) return substeps < o.substeps;
+      if (since != o.since) return since < o.since;
+      if (interval != o.interval) return interval < o.interval;
+      return flags < o.flags;
+    }
+  };
+  std::map<GraphKey, Graph> graphs;
 
   uint32_t add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
                      const float* vel, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
                      float dt);
   void remove_scene(uint32_t sid);
+  // Retires a scene without touching the rest of the pool: its record is
+  // marked dead (the kernels skip its items), its identities get the
+  // removed-particle key, and its slots, identities and grid range are given
+  // back after the next regrouping has sorted its particles out.
+  void retire_scene(uint32_t sid);
+  // Stops scene sid after `substeps` more substeps (0: no limit).  The
+  // particle kernels skip the scene once its completed-substep count has
+  // passed the budget, so a scene advances by exactly that many substeps
+  // however long the calls that step the group are.
+  void set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st);
+  // Regroups now if retired scenes await compaction, and gives their
+  // slots, identities and grid ranges back.
+  void compact(cudaStream_t st);
+  // SVD forms present among the live scenes.
+  bool any_svd32() const;
+  bool any_svd64() const;
   void set_scene_dt(uint32_t sid, float dt);
   void set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows);
   void set_scene_cfg(uint32_t sid, const mpm_config& cfg);
@@ -297,6 +339,12 @@ class Group {
  private:
   void rebuild_layout();
   void invalidate_graphs();
+  // Host bookkeeping after a regrouping that dropped the retiring scenes.
+  void finish_retirements();
+  // Whether a regrouping follows substep s (0-based) of a call of `substeps`
+  // substeps; advances `since`.  Sets need_regroup when one falls due on
+  // the last substep (it opens the next call instead).
+  bool regroup_due(uint32_t s, uint32_t substeps);
   void launch_gather_pass(int mode, bool keys, cudaStream_t st);
   void launch_scatter_pass(int acc_out, cudaStream_t st);
   void launch_fused_pass(int acc_out, bool keys, cudaStream_t st);
@@ -309,7 +357,7 @@ class Group {
   uint32_t autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_per_substep, cudaStream_t st);
  private:
   void run_substeps(uint32_t substeps, cudaStream_t st);
-  uint64_t graph_key(uint32_t substeps) const;
+  GraphKey graph_key(uint32_t substeps) const;
 };
 
 }  // namespace mpm

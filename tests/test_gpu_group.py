@@ -163,3 +163,131 @@ def test_autotune_keeps_state_and_picks_a_candidate(engine):
     g.step(5)
     for k, i in enumerate(ids):
         assert np.abs(g.read_positions(i) - alone(engine, ss[k], 10)).max() < TOL
+
+
+def alone_prec(engine, s, steps, svd, sort_interval=16, deterministic=False):
+    cfg = m.config_for_scene(s, svd_precision=svd)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(s.positions)
+    sim.set_materials(s.rows, s.ids)
+    sim.set_sort_interval(sort_interval)
+    if deterministic:
+        sim.prepare_deterministic_p2g()
+        sim.set_deterministic_p2g(True)
+    sim.step_n(s.dt, steps)
+    out = sim.read_positions()
+    sim.close()
+    return out
+
+
+def test_group_mixed_svd_precision_each_matches_alone(engine):
+    """FP32-SVD and FP64-SVD scenes share a group: each SVD form runs over its
+    own scenes' items, so every scene matches its own precision run alone."""
+    ss = small_scenes()
+    prec = [0, 1, 0, 1, 0]
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 256 * len(ss)
+    g = m.MpmGroup(engine, 16, total, cells)
+    ids = [g.add_scene(m.config_for_scene(s, svd_precision=p), s.rows, s.positions, s.ids, s.dt)
+           for s, p in zip(ss, prec)]
+    g.step(20)
+    g.step_graph(10, 1)
+    for sid, s, p in zip(ids, ss, prec):
+        got = g.read_positions(sid)
+        assert np.abs(got - alone_prec(engine, s, 30, p)).max() < TOL, (sid, p)
+        assert g.read_status(sid).completed_substeps == 30
+    g.close()
+
+
+def test_deterministic_mixed_precision_bit_identical_alone_and_in_mix(engine):
+    ss = small_scenes()
+    prec = [1, 0, 1, 0, 0]
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 256 * len(ss)
+
+    def run(indices):
+        g = m.MpmGroup(engine, 16, total, cells)
+        g.set_deterministic(True)
+        ids = {i: g.add_scene(m.config_for_scene(ss[i], svd_precision=prec[i]), ss[i].rows, ss[i].positions,
+                              ss[i].ids, ss[i].dt) for i in indices}
+        g.step(9)
+        g.step_graph(5, 2)
+        out = {i: g.read_positions(sid) for i, sid in ids.items()}
+        g.close()
+        return out
+
+    mix = run(range(len(ss)))
+    for i in (0, 1):
+        assert np.array_equal(run([i])[i], mix[i]), i
+
+
+def test_server_mixed_precision_exact_budgets(engine):
+    """Requests of both SVD forms and step counts that are not multiples of
+    the tick length: each result equals the scene run alone for exactly its
+    own step count (the device-side budget stops it mid-tick)."""
+    ss = small_scenes()
+    steps = [23, 40, 7, 33, 16]
+    prec = [1, 0, 0, 1, 1]
+    srv = m.MpmServer(engine, hbm_budget_bytes=64 << 20, max_scenes=8)
+    tickets = [srv.submit(m.config_for_scene(s, svd_precision=p), s.rows, s.positions, s.ids, s.dt, n)
+               for s, n, p in zip(ss, steps, prec)]
+    for _ in range(100):
+        srv.run(1, substeps_per_tick=16)
+        if all(srv.poll(t)[0] == 2 for t in tickets):
+            break
+    assert srv.stats()["completed"] == len(ss)
+    for t, s, n, p in zip(tickets, ss, steps, prec):
+        state, pos = srv.poll(t)
+        assert state == 2
+        assert np.abs(pos - alone_prec(engine, s, n, p)).max() < TOL, (n, p)
+
+
+def test_retired_scenes_leave_at_the_next_regroup(engine):
+    """Retirement through the server does not regroup the pool: the
+    remaining scenes keep stepping (and match their alone runs) while the
+    retired scenes' slots come back for new admissions."""
+    ss = small_scenes()
+    srv = m.MpmServer(engine, hbm_budget_bytes=64 << 20, max_scenes=8)
+    first = [srv.submit(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt, n)
+             for s, n in zip(ss[:3], (8, 60, 8))]
+    srv.run(1, substeps_per_tick=8)
+    assert srv.poll(first[0])[0] == 2 and srv.poll(first[2])[0] == 2
+    late = [srv.submit(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt, 24) for s in ss[3:]]
+    for _ in range(40):
+        srv.run(1, substeps_per_tick=8)
+        if all(srv.poll(t)[0] == 2 for t in first + late):
+            break
+    assert np.abs(srv.poll(first[1])[1] - alone(engine, ss[1], 60)).max() < TOL
+    for t, s in zip(late, ss[3:]):
+        assert np.abs(srv.poll(t)[1] - alone(engine, s, 24)).max() < TOL
+
+
+def test_regroup_cadence_independent_of_call_chunking(engine):
+    """The regrouping cadence is carried across calls: 64 calls of
+    step_n(1) regroup as often as one step_n(64) (the reference regroups on
+    its own schedule inside step_n, crates/molla-solvers/src/mpm.rs:2274-2353),
+    and both give the same state."""
+    s = small_scenes()[1]
+
+    def run(chunks):
+        sim = m.MpmSimulation.new(engine, m.config_for_scene(s))
+        sim.set_particles(s.positions)
+        sim.set_materials(s.rows, s.ids)
+        sim.set_sort_interval(8)
+        engine.synchronize()
+        engine.reset_profile()
+        engine.profile(True)
+        for c in chunks:
+            sim.step_n(s.dt, c)
+        engine.synchronize()
+        engine.profile(False)
+        count = engine.read_profile()["ParticleOrdering"][0]
+        pos = sim.read_positions()
+        sim.close()
+        return count, pos
+
+    n_one, p_one = run([64])
+    n_many, p_many = run([1] * 64)
+    n_mixed, p_mixed = run([5, 3, 17, 1, 30, 8])
+    assert n_one == n_many == n_mixed == 8
+    assert np.abs(p_one - p_many).max() < TOL and np.abs(p_one - p_mixed).max() < TOL
