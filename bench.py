@@ -5,18 +5,22 @@ Workload (default, one GPU): the single large scene — 256^3 grid, dx = 1/256,
 16M particles in 4 seeded random boxes (8 particles per cell, per-box elastic
 modulus log-uniform in [1e4, 1e5] or snow with theta_c 2.5e-2, theta_s
 7.5e-3), FP32 state with the FP64 SVD/polar decomposition, dt = 2e-5.  A
-"step" is one substep of the whole scene.  Particle state (1.8 GB) and grid
-(0.8 GB) are far larger than the 126 MB L2, so no L2 flush is needed between
-steps.
+"step" is one substep of the whole scene; the K timed substeps are centred on
+substep 250 of the scene's 500-substep run and open with a regrouping.
+Particle state (1.8 GB) and grid (0.8 GB) are far larger than the 126 MB L2,
+so no L2 flush is needed between steps.  The line also carries the accuracy
+against the FP64 oracle on a sample, the batched (64 scenes, graphs) and
+served (continuous batching) forms next to the plain one, the end-to-end rate
+through the C ABI with host buffers, and the CPU oracle's rate.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload large|medium|cube|cube128|batched|served]
+                    [--workload large|medium|cube|cube128|batched|served|precision]
 
 N > 1 runs under torchrun: every rank steps its own replica of the scene
 (independent scenes, no data-path collective; "scaling": "weak"); time is the
 max over ranks.  `--impl reference` times the CPU restatement of the
-reference step (the oracle, OpenMP on all host cores) on a bounded sample of
-the same workload and prints the same metric.
+reference step (the oracle, OpenMP on all host cores) on the same workload and
+prints the same metric.
 """
 
 from __future__ import annotations
@@ -229,14 +233,21 @@ def run_reference(args):
     rate, _ = time_cpu_oracle(probe, 1, 0, threads)
     budget_s = float(args.reference_budget_s)
     per_step = budget_s / max(args.steps + args.warmup, 1)
+    # The whole 16M-particle scene when the run fits the budget, else the
+    # largest sample of the same generator that does.
     n_sample = int(min(16_000_000, max(20_000, rate * per_step * 0.8)))
-    scene = cpu_sample_scene(n_sample)
+    if n_sample >= 16_000_000 or args.workload != "large":
+        scene, meta = make_workload(args.workload, 0)
+        whole = True
+    else:
+        scene = cpu_sample_scene(n_sample)
+        whole = False
+        _, meta = None, {"workload": f"sample of the single large scene: {scene.n} particles of its generator "
+                                    "(256^3 grid, 4 seeded boxes, elastic E 1e4..1e5 / snow), FP32 + FP64 SVD, "
+                                    "dt 2e-5", "grid": 256, "particles": scene.n, "svd": "fp64"}
     value, secs = time_cpu_oracle(scene, args.steps, args.warmup, threads)
-    _, meta = make_workload(args.workload, 0) if args.workload != "large" else (None, {
-        "workload": "single large scene: 256^3 grid, 16M particles in 4 seeded boxes (elastic E 1e4..1e5 / snow), "
-                    "FP32 + FP64 SVD, dt 2e-5", "grid": 256, "particles": 16_000_000, "svd": "fp64"})
-    sample = (f"{scene.n} particles of the same generator (256^3 grid, 4 boxes, same materials, dt 2e-5), "
-              f"{args.steps} substeps after {args.warmup} warm-up")
+    sample = (("the whole scene" if whole else f"{scene.n} particles of the same generator (256^3 grid, 4 boxes, "
+               "same materials, dt 2e-5)") + f", {args.steps} substeps after {args.warmup} warm-up")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True,
@@ -248,6 +259,60 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# The large scene's benchmark run is 500 substeps.  The timed window of K
+# substeps is centred on its midpoint (substeps 250 - K/2 .. 250 + K/2, at
+# least --warmup untimed substeps first), so that a short window costs what
+# the run costs on average: the SVD and the scatter both grow as the scene
+# deforms and spreads, and a window right after the start would be cheap.
+RUN_SUBSTEPS = 500
+
+
+def measure_accuracy(n_sample: int, substeps: int, threads: int):
+    """Errors of the GPU's FP32 + FP64-SVD step against the FP64 oracle (FP64
+    state, FP64 Jacobi SVD to 1e-14) on a sample of the large scene's
+    generator: positions, grid mass and momentum of the last substep, and the
+    GPU's own mass / momentum bookkeeping (grid against particles)."""
+    import molla_b200 as m
+    from oracle import oracle as O
+    scene = cpu_sample_scene(n_sample)
+    cfg = m.config_for_scene(scene, svd_precision=1)
+    engine = m.Engine(0)
+    sim = m.MpmSimulation.new(engine, cfg)
+    sim.set_particles(scene.positions)
+    sim.set_materials(scene.rows, scene.ids)
+    sim.step_n(scene.dt, substeps)
+    pos = sim.read_positions().astype(np.float64)
+    gmass, gmom = sim.read_grid_mass_momentum()
+    tot = sim.conservation_totals()
+    sim.close()
+    engine.close()
+    osc = O.make_scene(cfg, scene.rows, scene.dt, svd_tol=1e-14, svd_sweeps=30)
+    st = O.cast_state(O.init_state(scene.positions, mass=cfg.particle_mass, volume=cfg.particle_volume,
+                                   ids=scene.ids), np.float64)
+    t0 = time.perf_counter()
+    om, op = O.step(osc, st, substeps, precision="f64", nthreads=threads, want_grid=True)
+    secs = time.perf_counter() - t0
+    ref = st["pos"]
+    d = pos - ref
+    ref_mom = op.reshape(-1, 3).sum(axis=0)
+    gpu_mom = gmom.astype(np.float64).reshape(-1, 3).sum(axis=0)
+    node_mom_err = np.abs(gmom.astype(np.float64) - op).max() / max(np.abs(op).max(), 1e-30)
+    mass0 = float(np.float32(cfg.particle_mass)) * scene.n
+    return {
+        "reference": "FP64 CPU oracle (FP64 state, FP64 Jacobi SVD tol 1e-14)",
+        "sample": f"{scene.n} particles of the large scene's generator, {substeps} substeps from rest",
+        "oracle_s": round(secs, 2),
+        "pos_rel_max": float((np.abs(d) / np.maximum(np.abs(ref), 1e-30)).max()),
+        "pos_rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+        "grid_mass_rel": float(abs(float(gmass.astype(np.float64).sum()) - float(om.sum())) / float(om.sum())),
+        "grid_momentum_rel": float(np.linalg.norm(gpu_mom - ref_mom) / max(np.linalg.norm(ref_mom), 1e-30)),
+        "grid_node_momentum_max_rel": float(node_mom_err),
+        "mass_drift": float(tot[0] / mass0 - 1.0),
+        "momentum_grid_vs_particles_rel": float(np.linalg.norm(tot[1:4] - tot[5:8]) /
+                                                max(np.linalg.norm(tot[5:8]), 1e-30)),
+    }
 
 
 def run_ours(args):
@@ -271,21 +336,31 @@ def run_ours(args):
     sim.set_materials(scene.rows, scene.ids)
     n = scene.n
 
-    # warm-up, then the regroup interval: fixed by --sort-interval, or (0)
-    # picked by the autotuner on a snapshot of the warmed-up state.
-    sim.step_n(scene.dt, max(args.warmup, 3))
+    # Untimed: advance to the fixed trajectory point (the --warmup substeps
+    # are part of it), picking the regroup interval on the way: fixed by
+    # --sort-interval, or (0) by the autotuner on a snapshot of the state.
+    start_at = args.trajectory_start if args.trajectory_start >= 0 else RUN_SUBSTEPS // 2 - args.steps // 2
+    start_at = max(args.warmup, start_at)
+    first = max(3, min(start_at, start_at - 50))
+    sim.step_n(scene.dt, first)
     engine.synchronize()
     tune = None
     if args.sort_interval > 0:
         interval = args.sort_interval
-        sim.set_sort_interval(interval)
     else:
         interval, tune = sim.autotune(scene.dt, probe_substeps=32)
-    sim.step_n(scene.dt, 1)
+    sim.set_sort_interval(interval)
+    if start_at > first:
+        sim.step_n(scene.dt, start_at - first)
     engine.synchronize()
     gm, _ = sim.read_grid_mass_momentum()
     active = int((gm > 0).sum())
     del gm
+    # The regroup cadence starts afresh so that the timed call opens with a
+    # regrouping: the window holds 1 + floor((K - 1) / interval) of them,
+    # at least its share at the regular cadence.
+    sim.set_sort_interval(interval)
+    regroups_in_window = 1 + (args.steps - 1) // interval
 
     # timed region: K substeps in one step_n call, bracketed by a barrier
     # and synchronisation on both sides; device time from CUDA events
@@ -323,9 +398,10 @@ def run_ours(args):
         engine.synchronize()
         lat.append(1000.0 * (time.perf_counter() - t))
 
-    # end to end through the C ABI with host buffers: upload the scene
-    # (positions + material ids from pinned host memory), run e2e_substeps
-    # substeps, read positions back.
+    # End to end through the C ABI with host buffers: each call uploads the
+    # scene (positions and material ids from pinned host memory), runs the
+    # benchmark's whole trajectory (e2e_substeps, 500 by default) and reads
+    # the positions back into a pinned buffer.
     pos_host = torch.from_numpy(scene.positions).pin_memory().numpy()
     ids_host = torch.from_numpy(scene.ids.astype(np.int32)).pin_memory().numpy().view(np.uint32)
     out_host = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
@@ -341,6 +417,8 @@ def run_ours(args):
     e2e_s = float(np.median(e2e_times[1:])) if len(e2e_times) > 1 else float(e2e_times[0])
     e2e_s = max_over_ranks(dist, e2e_s, device)
     e2e_value = n * args.e2e_substeps * ws / e2e_s
+    sim.close()
+    engine.close()
 
     result = None
     if rank == 0:
@@ -379,6 +457,8 @@ def run_ours(args):
         step_bytes = STEP_BYTES_PER_PARTICLE * n + STEP_BYTES_PER_ACTIVE_CELL * active
         step_achieved = step_bytes / (elapsed / args.steps) / 1e9
         cpu = None
+        accuracy = None
+        threads = None
         if ws == 1 and not args.no_cpu_baseline:
             from oracle import oracle as O
             threads = O.max_threads()
@@ -390,13 +470,25 @@ def run_ours(args):
             cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{cs.n} particles of the same generator (256^3 grid, 4 boxes), 3 substeps, "
                              f"{csecs:.1f} s"}
+            if args.workload == "large" and not args.no_accuracy:
+                accuracy = measure_accuracy(n_sample, 3, threads)
+        batched = served = None
+        if ws == 1 and args.workload == "large" and not args.no_batched:
+            batched = measure_batched(args, quiet=True)
+        if ws == 1 and args.workload == "large" and not args.no_served:
+            served = measure_served(args, quiet=True)
+        e2e_h2d = int(pos_host.nbytes + ids_host.nbytes)
+        e2e_d2h = int(out.nbytes)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed_max / args.steps, "higher_is_better": True,
+            "warmup": start_at, "ms_per_step": 1000.0 * elapsed_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 svd)" if svd_prec else "f32",
             "data": "synthetic (seeded boxes; no dataset)",
             "config": dict(meta, active_cells=active, sort_interval=interval,
                            autotune_ms_per_substep=tune,
+                           timed_substeps=f"{start_at}..{start_at + args.steps} of the scene's trajectory "
+                                          f"(untimed advance of {start_at} substeps, --warmup included)",
+                           regroups_in_window=regroups_in_window,
                            parallelism=f"replicas x{ws}" if ws > 1 else "single scene"),
             "p50_step_ms": float(np.percentile(lat, 50)) if lat else None,
             "p99_step_ms": float(np.percentile(lat, 99)) if lat else None,
@@ -411,9 +503,16 @@ def run_ours(args):
             "step_roofline": {"achieved": step_achieved, "frac": step_achieved / hbm,
                               "bytes_per_step": step_bytes, "model": "268 B/particle + 56 B/active cell"},
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
+            "batched": batched,
+            "served": served,
             "e2e": {"value": e2e_value, "unit": UNIT, "substeps_per_call": args.e2e_substeps,
-                    "h2d_bytes_per_step": int(pos_host.nbytes + ids_host.nbytes),
-                    "d2h_bytes_per_step": int(out.nbytes), "call_s": [round(x, 4) for x in e2e_times]},
+                    "h2d_bytes_per_step": e2e_h2d / args.e2e_substeps,
+                    "d2h_bytes_per_step": e2e_d2h / args.e2e_substeps,
+                    "h2d_bytes_per_call": e2e_h2d, "d2h_bytes_per_call": e2e_d2h,
+                    "call": f"set_particles + set_materials (pinned host), step_n({args.e2e_substeps}) from rest, "
+                            f"read_positions (pinned host)",
+                    "call_s": [round(x, 4) for x in e2e_times]},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "wall_s": wall,
@@ -421,8 +520,6 @@ def run_ours(args):
     barrier(dist, device)
     if rank == 0:
         print(json.dumps(result), flush=True)
-    sim.close()
-    engine.close()
     if dist is not None:
         dist.destroy_process_group()
 
@@ -537,40 +634,44 @@ def run_precision(args):
     engine.close()
 
 
-def run_batched(args):
-    """64 independent scenes of uneven size (grids log-uniform 32^3..128^3,
-    10k..2M particles at 8 per cell, half elastic half snow) stepped in the
-    same launches through captured CUDA graphs, after the autotuner picked
-    the regrouping interval; compared with the plain form (one simulation
-    per scene, stepped one after the other, no graphs) on the same GPU."""
+def measure_batched(args, quiet=False):
+    """64 independent scenes of uneven size (grids log-uniform
+    32^3..128^3, 10k..2M particles at 8 per cell, half elastic half snow,
+    FP32) stepped in the same launches through captured CUDA graphs, with the
+    regroup interval autotuned; compared with the plain form (one simulation
+    per scene, stepped one after the other without graphs) at the same point
+    of the same scenes' trajectories on the same GPU.  Both forms first
+    advance `batched_advance` substeps untimed."""
     import torch
 
     import molla_b200 as m
     from molla_b200 import scenes
 
-    torch.cuda.set_device(0)
     ss = scenes.batch_scenes(count=args.scenes, seed=3)
     total = sum(s.n for s in ss)
     cells = sum(s.grid_size ** 3 + 256 for s in ss)
     engine = m.Engine(0)
-    g = m.MpmGroup(engine, len(ss), total, cells)
-    ids = [g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt) for s in ss]
-    chosen, tune = g.autotune(probe_substeps=32)
-    g.step_graph(max(args.warmup, 3), 1)
-    engine.synchronize()
     stream = torch.cuda.ExternalStream(engine.stream_handle, device=torch.device("cuda", 0))
-    engine.reset_profile()
+    steps = args.batched_steps
+    g = m.MpmGroup(engine, len(ss), total, cells)
+    for s in ss:
+        g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt)
+    g.step_graph(max(3, args.batched_advance // 2), 1)
+    chosen, tune = g.autotune(probe_substeps=32)
+    g.step_graph(max(3, args.batched_advance - args.batched_advance // 2), 1)
+    g.step_graph(steps, 1)  # captures the timed sequence's graph
+    engine.synchronize()
     launches0 = engine.launch_count
     with ClockSampler(0) as clocks:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        g.step_graph(args.steps, 1)
+        g.step_graph(steps, 1)
         e1.record(stream)
         e1.synchronize()
     launches = engine.launch_count - launches0
     t_batched = e0.elapsed_time(e1) / 1000.0
-    value = total * args.steps / t_batched
+    value = total * steps / t_batched
     lat = []
     for _ in range(args.latency_samples):
         a = torch.cuda.Event(enable_timing=True)
@@ -580,9 +681,10 @@ def run_batched(args):
         b.record(stream)
         b.synchronize()
         lat.append(a.elapsed_time(b))
-    # stage shares of the batched form (profiled pass, not timed above)
     engine.profile(True)
+    engine.reset_profile()
     g.step(8)
+    engine.synchronize()
     engine.profile(False)
     prof = engine.read_profile()
     g.close()
@@ -592,89 +694,104 @@ def run_batched(args):
         sim = m.MpmSimulation.new(engine, m.config_for_scene(s))
         sim.set_particles(s.positions)
         sim.set_materials(s.rows, s.ids)
-        sim.step_n(s.dt, max(args.warmup, 3))
+        sim.set_sort_interval(chosen)
         sims.append((sim, s))
+    for sim, s in sims:
+        sim.step_n(s.dt, args.batched_advance + steps)
     engine.synchronize()
     e0.record(stream)
     for sim, s in sims:
-        sim.step_n(s.dt, args.steps)
+        sim.step_n(s.dt, steps)
     e1.record(stream)
     e1.synchronize()
     t_plain = e0.elapsed_time(e1) / 1000.0
-    plain = total * args.steps / t_plain
+    plain = total * steps / t_plain
     for sim, _ in sims:
         sim.close()
-    hbm, peak_kind = peaks()
-    n_mean = total  # per substep every scene advances once
-    dom, kernels = _stage_roofline(prof, n_mean, 0, hbm)
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * t_batched / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes; no dataset)",
-        "config": {"workload": f"batched: {len(ss)} scenes, grids 32^3..128^3, {total} particles, mixed "
-                               "elastic/snow, FP32, CUDA-graph captured, autotuned regroup interval",
-                   "scenes": len(ss), "particles": total, "regroup_interval": chosen,
-                   "autotune_ms_per_substep": tune},
-        "plain": {"value": plain, "ms_per_step": 1000.0 * t_plain / args.steps},
+    engine.close()
+    return {
+        "workload": f"batched: {len(ss)} scenes, grids 32^3..128^3, {total} particles, mixed elastic/snow, FP32, "
+                    f"CUDA-graph captured, autotuned regroup interval; {steps} substeps timed after "
+                    f"{args.batched_advance + steps} untimed",
+        "value": value, "unit": UNIT, "ms_per_step": 1000.0 * t_batched / steps,
+        "plain": {"value": plain, "ms_per_step": 1000.0 * t_plain / steps,
+                  "form": "one MpmSimulation per scene, step_n one after the other, no graphs"},
         "batched_over_plain": value / plain,
         "p50_step_ms": float(np.percentile(lat, 50)) if lat else None,
         "p99_step_ms": float(np.percentile(lat, 99)) if lat else None,
+        "scenes": len(ss), "particles": total, "regroup_interval": chosen, "autotune_ms_per_substep": tune,
         "stages_ms_per_step": {k: v[1] / 8 for k, v in prof.items()},
-        "kernels": kernels, "gpu_launches": int(launches), "clocks": clocks.summary(),
+        "gpu_launches": int(launches), "clocks": clocks.summary(),
     }
+
+
+def run_batched(args):
+    d = measure_batched(args)
+    line = {"metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": 1, "steps": args.batched_steps,
+            "warmup": args.batched_advance, "ms_per_step": d["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes; no dataset)",
+            "config": {"workload": d["workload"]}, **{k: v for k, v in d.items() if k not in ("value", "workload")}}
     print(json.dumps(line), flush=True)
-    engine.close()
 
 
-def run_served(args):
-    """Continuous batching: Poisson arrivals (200 scenes/s) of scenes sized as
-    the batched workload, 200..2000 substeps each, admitted by an HBM budget
-    as slots and memory free up, stepped together, retired when done.  The
-    offered load exceeds the GPU's throughput, so the queue grows; arrivals
-    beyond 512 queued requests are refused and counted."""
+def measure_served(args, quiet=False):
+    """configs[4], continuous batching: Poisson arrivals (200 scenes/s) of
+    scenes sized as the batched workload, 200..2000 substeps each, admitted by
+    an HBM budget as slots and memory free up, stepped together in
+    fixed-length ticks (each scene stops on the device after its own step
+    count), retired at the next regrouping.  The offered load exceeds the
+    GPU's throughput, so the queue grows; arrivals beyond 512 queued requests
+    are refused and counted."""
     import time as _t
 
     import molla_b200 as m
     from molla_b200 import scenes
 
     pool = scenes.batch_scenes(count=args.scenes, seed=3)
+    cfgs = [m.config_for_scene(s) for s in pool]
     engine = m.Engine(0)
     srv = m.MpmServer(engine, hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_scenes=2048)
     rng = np.random.default_rng(7)
     t0 = _t.perf_counter()
     next_arrival = 0.0
     submitted = refused = 0
-    tickets = []
     while _t.perf_counter() - t0 < args.serve_seconds:
         now = _t.perf_counter() - t0
         while next_arrival <= now:
-            s = pool[submitted % len(pool)]
+            k = submitted % len(pool)
+            s = pool[k]
             st = srv.stats()
             if submitted - st["admitted"] >= 512:
                 refused += 1
             else:
                 steps = int(rng.integers(200, 2001))
-                tickets.append(srv.submit(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt, steps))
+                srv.submit(cfgs[k], s.rows, s.positions, s.ids, s.dt, steps)
                 submitted += 1
             next_arrival += rng.exponential(1.0 / args.arrival_rate)
         srv.run(1, substeps_per_tick=args.tick_substeps)
     elapsed = _t.perf_counter() - t0
     st = srv.stats()
-    line = {
-        "metric": METRIC, "value": st["particle_steps"] / elapsed, "unit": UNIT, "n_gpus": 1,
-        "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded scenes; no dataset)",
-        "config": {"workload": f"served: Poisson {args.arrival_rate}/s arrivals, scenes as the batched workload, "
-                               f"200..2000 substeps, HBM budget {args.budget_gb} GB, {args.tick_substeps} substeps "
-                               "per tick", "seconds": elapsed},
+    srv.close()
+    engine.close()
+    return {
+        "workload": f"served: Poisson {args.arrival_rate}/s arrivals, scenes as the batched workload, 200..2000 "
+                    f"substeps each, HBM budget {args.budget_gb} GB, {args.tick_substeps}-substep ticks "
+                    "(graph-replayed), device-side per-scene budgets",
+        "value": st["particle_steps"] / elapsed, "unit": UNIT, "seconds": elapsed,
         "p50_step_ms": st["tick_ms_p50"], "p99_step_ms": st["tick_ms_p99"],
         "queue_ms_p50": st["queue_ms_p50"], "queue_ms_p99": st["queue_ms_p99"],
         "submitted": submitted, "refused": refused, "admitted": st["admitted"], "completed": st["completed"],
         "resident_scenes": st["resident_scenes"], "resident_bytes": st["resident_bytes"],
     }
+
+
+def run_served(args):
+    d = measure_served(args)
+    line = {"metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": 1, "steps": None, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scenes; no dataset)", "config": {"workload": d["workload"]},
+            **{k: v for k, v in d.items() if k not in ("value", "workload")}}
     print(json.dumps(line), flush=True)
-    srv.close()
-    engine.close()
 
 
 def main():
@@ -687,14 +804,23 @@ def main():
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--arrival-rate", type=float, default=200.0)
-    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-seconds", type=float, default=15.0)
     ap.add_argument("--tick-substeps", type=int, default=20)
     ap.add_argument("--sort-interval", type=int, default=0,
                     help="substeps between regroups; 0 = autotuned on the warmed-up scene")
     ap.add_argument("--latency-samples", type=int, default=20)
-    ap.add_argument("--e2e-iters", type=int, default=3)
-    ap.add_argument("--e2e-substeps", type=int, default=100)
+    ap.add_argument("--e2e-iters", type=int, default=2)
+    ap.add_argument("--e2e-substeps", type=int, default=500,
+                    help="substeps per end-to-end call (the large scene's whole 500-substep trajectory)")
+    ap.add_argument("--trajectory-start", type=int, default=-1,
+                    help="substep of the scene's trajectory where the timed window starts (default: the window "
+                         "is centred on substep 250 of the 500-substep run)")
+    ap.add_argument("--batched-steps", type=int, default=64)
+    ap.add_argument("--batched-advance", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--precision-grid", type=int, default=128)
     ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--reference-budget-s", type=float, default=120.0,

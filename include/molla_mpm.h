@@ -238,7 +238,9 @@ MPM_API int mpm_prepare_particle_tile_ordering(mpm_sim* sim, uint32_t capacity);
 /* set_particle_tile_ordering (mpm_particle_order.rs:232-252). */
 MPM_API int mpm_set_particle_tile_ordering(mpm_sim* sim, int enabled);
 /* Sort interval of the hot path: particles are physically regrouped by 4^3
- * tile every `interval` substeps (0 → autotuned default). */
+ * tile every `interval` substeps (0 → autotuned default).  The cadence runs
+ * across step_n calls (it does not restart per call); setting the interval
+ * starts a new cadence, whose first regrouping opens the next call. */
 MPM_API int mpm_set_sort_interval(mpm_sim* sim, uint32_t interval);
 
 /* step / step_n (mpm.rs:2232-2353): asynchronous; dt finite and > 0. */
@@ -337,7 +339,7 @@ MPM_API int mpm_radix_sort_pairs_device(mpm_engine* engine, uint32_t* d_keys, ui
  * whole device budget up front, and hot paths held to an allocation-free
  * guarantee.  Sorts d_keys/d_values (n pairs, device pointers on the current
  * device) in place on `stream` (NULL: the default stream), stably by the low
- * key_bits bits, using an 8.3 MiB scratch array that the library keeps in
+ * key_bits bits, using an 8.25 MiB (8,651,776-byte) scratch array that the library keeps in
  * device memory for the whole process (every GPU that loads the library
  * holds one).  n above 1,048,576 is rejected with MPM_ERR_INVALID.  It calls
  * no allocation routine.  The first call on a device looks up the scratch

@@ -643,6 +643,8 @@ int mpm_set_sort_interval(mpm_sim* sim, uint32_t interval) {
     REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
     sim->sort_interval = interval;
     sim->apply_group_settings();
+    // a new interval starts a new cadence: the next call opens with a regrouping
+    sim->group->need_regroup = true;
     sim->invalidate();
   });
 }

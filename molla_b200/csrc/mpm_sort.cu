@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/molla_mpm.h"
@@ -214,13 +216,14 @@ cudaError_t radix_sort_pairs(cudaStream_t stream, const uint32_t* keys_in, const
 // synchronise the device), hosts that reserve the whole device budget up
 // front and forbid allocations afterwards, and hot paths held to an
 // allocation-free guarantee.  The sort's ping-pong buffers and digit
-// histograms live in the file-scope array below (8.3 MiB, sized for
-// kNoAllocMaxPairs pairs); every GPU that loads this library holds it until
-// the process exits.
+// histograms live in the file-scope array below (8.25 MiB = 8,651,776 bytes,
+// sized for kNoAllocMaxPairs pairs); every GPU that loads this library holds
+// it until the process exits.
 
 constexpr uint32_t kNoAllocMaxPairs = 1u << 20;  // 1,048,576 (key, value) pairs
 constexpr size_t kNoAllocHistWords = (size_t)256 * ((kNoAllocMaxPairs + kSortTile - 1) / kSortTile) + 256;
 constexpr size_t kNoAllocWords = 2ull * kNoAllocMaxPairs + kNoAllocHistWords;
+static_assert(kNoAllocWords * 4 == 8651776, "the documented size of the allocation-free scratch");
 
 // One key buffer, one value buffer and the histogram/digit totals.  In host
 // code this name is only a stand-in for the device array, never a device
@@ -228,25 +231,64 @@ constexpr size_t kNoAllocWords = 2ull * kNoAllocMaxPairs + kNoAllocHistWords;
 static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocWords];
 
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-uint32_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// Scratch address per CUDA context, keyed by the context's process-unique
+// id: a symbol's device address belongs to the context that loaded the
+// module, so a non-primary context, or a primary context recreated after
+// cudaDeviceReset, gets its own lookup rather than a stale address.
+struct NoAllocEntry {
+  unsigned long long ctx_id;
+  uint32_t* ptr;
+};
+std::vector<NoAllocEntry> g_noalloc_cache;
 
-// Device address of the scratch array on the current device, looked up once
-// per device.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the context current on this thread; false if the driver cannot say.
+bool current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    resolved = true;
+  }
+  if (!get_current || !get_id) return false;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch array in the current context: looked up
+// with cudaGetSymbolAddress once per context (every call when the driver
+// cannot identify the context).
 cudaError_t noalloc_scratch(uint32_t** out) {
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  cudaError_t e = cudaGetDevice(&dev);  // makes the device's primary context current if none is
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    uint32_t* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_noalloc_sort_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+  unsigned long long id = 0;
+  const bool known = current_context_id(&id);
+  if (known)
+    for (const NoAllocEntry& en : g_noalloc_cache)
+      if (en.ctx_id == id) {
+        *out = en.ptr;
+        return cudaSuccess;
+      }
+  uint32_t* p = nullptr;
+  e = cudaGetSymbolAddress((void**)&p, g_noalloc_sort_scratch);
+  if (e != cudaSuccess) return e;
+  if (known) g_noalloc_cache.push_back({id, p});
+  *out = p;
   return cudaSuccess;
 }
 }  // namespace

@@ -33,15 +33,16 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_rust_binding_covers_every_declared_symbol():
-    """The extern "C" blocks a molla maintainer would paste
-    name every entry point of the header with its argument count."""
+    """The Rust extern "C" declarations a molla maintainer adds to
+    molla-solvers (molla_b200/ffi/mpm_b200_ffi.rs) name every entry point of
+    the header with its argument count."""
     hdr = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "molla_mpm.h").read_text(), flags=re.S)
     arity = {}
     for name, args in re.findall(r"MPM_API\s+[\w\s\*]+?\b(mpm_\w+)\s*\(([^)]*)\)\s*;", hdr):
         arity[name] = len([a for a in args.split(",") if a.strip() and a.strip() != "void"])
-    doc = (ROOT / "INTEGRATION.md").read_text()
+    src = re.sub(r"//[^\n]*", "", (ROOT / "molla_b200" / "ffi" / "mpm_b200_ffi.rs").read_text())
     bound = {}
-    for name, args in re.findall(r"pub fn (mpm_\w+)\(([^)]*)\)", doc, flags=re.S):
+    for name, args in re.findall(r"pub fn (mpm_\w+)\(([^)]*)\)", src, flags=re.S):
         bound[name] = len([a for a in args.split(",") if a.strip()])
     assert set(arity) == set(declared_symbols())
     assert set(bound) == set(arity), set(bound) ^ set(arity)
