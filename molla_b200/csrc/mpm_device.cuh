@@ -200,20 +200,25 @@ __device__ __forceinline__ T det3(const T* a) {
 // most `sweeps` sweeps, stop when the largest off-diagonal is below `tol`;
 // sigma_i = |F v_i|, u_i = F v_i / sigma_i; sign fixes so det U = det V = +1.
 //
-// The FP32 form keeps the reference's rotation formulas (theta, t, c with
-// IEEE division and square root).
+// Both forms run the iteration on the shifted matrix A' = F^T F - I (the same
+// eigenvectors and the same off-diagonal entries, so the same rotations and
+// stopping test in exact arithmetic), held in FP32 and formed there as
+// E + E^T + E^T E from the exact E = F - I, so that its entries keep full
+// relative precision however small the strain.  (F^T F itself carries
+// rounding noise of half an ulp of 1 on its diagonal, which a tolerance of
+// 1e-7 on the off-diagonal then chases through extra sweeps.)  Each rotation
+// angle t = sgn(d) e / (|d| + sqrt(d^2+e^2)) (d = a'_qq - a'_pp,
+// e = 2 a'_pq; algebraically 1/(theta + sgn(theta) sqrt(1 + theta^2)), the
+// reference's formula) is computed in FP32 with the hardware reciprocal
+// square root and division.
 //
-// The FP64 form (svd3<double>) is mixed precision, built for the
-// small-strain regime where F^T F = I + O(strain): the Jacobi iteration runs
-// on the shifted matrix A' = F^T F - I (same eigenvectors), held in FP32 and
-// formed there as E + E^T + E^T E from the exact E = F - I, so that its
-// entries keep full relative precision however small the strain.  Each
-// rotation angle t = sgn(d) e / (|d| + sqrt(d^2+e^2))
-// (d = a'_qq - a'_pp, e = 2 a'_pq; algebraically 1/(theta + sgn(theta)
-// sqrt(1 + theta^2))) is computed in FP32; V accumulates the same rotations
-// in FP64 with c = (1 + t^2)^(-1/2) Newton-refined to FP64 and s = t c, so V
-// stays orthogonal to FP64 rounding.  sigma_i = |F v_i| and u_i = F v_i /
-// sigma_i are FP64.  Double division and square roots are replaced by
+// The FP32 form accumulates V in FP32; sigma_i = |F v_i| and u_i = F v_i /
+// sigma_i in FP32.
+//
+// The FP64 form (svd3<double>) is mixed precision: V accumulates the same
+// rotations in FP64 with c = (1 + t^2)^(-1/2) Newton-refined to FP64 and
+// s = t c, so V stays orthogonal to FP64 rounding.  sigma_i = |F v_i| and
+// u_i = F v_i / sigma_i are FP64.  Double division and square roots are replaced by
 // Newton-Raphson refinement of single-precision seeds (two steps each,
 // quadratic convergence from 2^-22 to below 2^-52).
 // U is held in FP32 in both forms: its consumers (the stress record and
@@ -257,18 +262,10 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
   const float aqq = a[Q][Q];
   float t, c, s;
   T cv, sv;
-  if constexpr (sizeof(T) == 4) {
-    const float theta = (aqq - app) / (2.0f * apq);
-    if (theta >= 0.0f) {
-      t = 1.0f / (theta + sqrtf(1.0f + theta * theta));
-    } else {
-      t = 1.0f / (theta - sqrtf(1.0f + theta * theta));
-    }
-    c = 1.0f / sqrtf(1.0f + t * t);
-    s = t * c;
-    cv = c;
-    sv = s;
-  } else {
+  {
+    // t = 1 / (theta + sgn(theta) sqrt(1 + theta^2)), theta = d / e, written
+    // as sgn(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq
+    // (no division by a small a_pq); c = (1 + t^2)^(-1/2), s = t c.
     float d = aqq - app;
     float e = 2.0f * apq;
     // power-of-two rescale keeps d^2 + e^2 inside the normal FP32 range
@@ -281,6 +278,11 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
     t = __fdividef(d >= 0.0f ? e : -e, fabsf(d) + hyp);
     c = rsqrtf(1.0f + t * t);
     s = t * c;
+  }
+  if constexpr (sizeof(T) == 4) {
+    cv = c;
+    sv = s;
+  } else {
     // FP64 rotation for V: exactly orthogonal to FP64 rounding for this t.
     const double td = (double)t;
     const double h = 0.5 * fma(td, td, 1.0);
@@ -324,15 +326,7 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
   // so its entries keep full FP32 relative precision however small the
   // strain, as forming F^T F - I in FP64 and rounding does.
   float a[3][3];
-  if constexpr (sizeof(T) == 4) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int r = c; r < 3; ++r) {
-        a[c][r] = f[3 * r] * f[3 * c] + f[3 * r + 1] * f[3 * c + 1] + f[3 * r + 2] * f[3 * c + 2];
-        a[r][c] = a[c][r];
-      }
-  } else {
+  {
     float e[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) e[i] = (i % 4 == 0) ? f32[i] - 1.0f : f32[i];
@@ -364,7 +358,8 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
     const T z = f[2] * v[3 * i] + f[5] * v[3 * i + 1] + f[8] * v[3 * i + 2];
     T s;
     if constexpr (sizeof(T) == 4) {
-      s = sqrtf(x * x + y * y + z * z);
+      const float q = x * x + y * y + z * z;
+      s = q > 0.0f ? q * rsqrtf(q) : 0.0f;
     } else {
       const T q = x * x + y * y + z * z;
       s = q > T(0) ? q * nr_rsqrt(q) : T(0);
@@ -372,9 +367,10 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
     o.s[i] = s;
     if (s > T(1.0e-12)) {
       if constexpr (sizeof(T) == 4) {
-        o.u[3 * i] = x / s;
-        o.u[3 * i + 1] = y / s;
-        o.u[3 * i + 2] = z / s;
+        const float inv = __frcp_rn(s);
+        o.u[3 * i] = x * inv;
+        o.u[3 * i + 1] = y * inv;
+        o.u[3 * i + 2] = z * inv;
       } else {
         const float inv = 1.0f / (float)s;
         o.u[3 * i] = (float)x * inv;
