@@ -499,6 +499,12 @@ typedef struct mpm_server_stats {
   double tick_ms_p99;
   double queue_ms_p50;
   double queue_ms_p99;
+  /* host wall time spent admitting, stepping (launch to completion) and
+   * retiring since creation, and the ticks run */
+  double admit_ms;
+  double step_ms;
+  double retire_ms;
+  uint64_t ticks;
 } mpm_server_stats;
 MPM_API int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out);
 

@@ -82,6 +82,10 @@ class mpm_server_stats(C.Structure):
         ("tick_ms_p99", C.c_double),
         ("queue_ms_p50", C.c_double),
         ("queue_ms_p99", C.c_double),
+        ("admit_ms", C.c_double),
+        ("step_ms", C.c_double),
+        ("retire_ms", C.c_double),
+        ("ticks", C.c_uint64),
     ]
 
 

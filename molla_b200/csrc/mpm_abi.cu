@@ -1126,6 +1126,8 @@ struct mpm_server {
   uint64_t next_id = 1;
   uint64_t admitted = 0, completed = 0, particle_steps = 0;
   std::vector<double> tick_ms, queue_ms;
+  double admit_ms = 0, step_ms = 0, retire_ms = 0;
+  uint64_t ticks = 0;
   std::unique_ptr<mpm::OwnedEvent> e0, e1;  // tick timing
 };
 
@@ -1197,6 +1199,7 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
     mpm::Group& g = *server->g;
     cudaStream_t st = server->eng->stream;
     for (uint32_t tick = 0; tick < ticks; ++tick) {
+      const double t_admit0 = now_ms();
       // admit in arrival order while the budget and pools allow
       while (!server->queue.empty()) {
         Ticket& t = server->tickets.at(server->queue.front());
@@ -1228,7 +1231,7 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         }
         if (!added) break;
         // the scene stops on the device after exactly its requested substeps
-        g.set_scene_budget(sid, t.steps, st);
+        g.set_scene_budget(sid, t.steps, st, /*fresh=*/true);
         t.sid = sid;
         t.state = 1;
         t.t_admit = now_ms();
@@ -1241,6 +1244,8 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
       // One tick of a fixed length through a captured graph: every resident
       // scene advances min(remaining, substeps_per_tick) substeps (a scene
       // whose budget ends inside the tick stands still for the rest of it).
+      const double t_step0 = now_ms();
+      server->admit_ms += t_step0 - t_admit0;
       const uint32_t len = substeps_per_tick;
       uint64_t parts = 0;
       for (auto& kv : server->tickets)
@@ -1257,6 +1262,9 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
       MPM_CK(cudaEventElapsedTime(&ms, *server->e0, *server->e1));
       server->tick_ms.push_back(ms / (float)len);
       server->particle_steps += parts;
+      server->ticks++;
+      const double t_ret0 = now_ms();
+      server->step_ms += t_ret0 - t_step0;
       // retire finished scenes: their slots go back at the next regrouping
       for (auto& kv : server->tickets) {
         Ticket& t = kv.second;
@@ -1271,6 +1279,7 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
           server->completed++;
         }
       }
+      server->retire_ms += now_ms() - t_ret0;
     }
   });
 }
@@ -1608,6 +1617,10 @@ int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out) {
     out->tick_ms_p99 = pct(server->tick_ms, 0.99);
     out->queue_ms_p50 = pct(server->queue_ms, 0.5);
     out->queue_ms_p99 = pct(server->queue_ms, 0.99);
+    out->admit_ms = server->admit_ms;
+    out->step_ms = server->step_ms;
+    out->retire_ms = server->retire_ms;
+    out->ticks = server->ticks;
   });
 }
 

@@ -1,6 +1,7 @@
 // mpm_kernels.cu — grid update, regrouping, work-list and data-movement
 // kernels of the B200 MLS-MPM path (the particle kernel is in
 // mpm_particles.cu).
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -400,29 +401,23 @@ __global__ void k_tile_start(const uint32_t* __restrict__ sorted_keys, uint32_t 
 }
 
 // Work items: every occupied tile, cut into chunks of at most `chunk` slots.
-// scene_of_tile is found by a search over the scene key offsets.  Items of
-// FP32-SVD scenes take slots from 0 up (count n_items[0]), items of FP64-SVD
-// scenes slots from item_top - 1 down (count n_items[1]), so that the gather
-// of each SVD form is one launch over a contiguous range.
-__global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, const uint32_t* __restrict__ key_offs,
-                        uint32_t n_scenes, const uint32_t* __restrict__ scene_ids, const SceneDev* __restrict__ scenes,
-                        uint32_t chunk, uint32_t item_top, Item* __restrict__ items, uint32_t* __restrict__ n_items,
-                        uint32_t* __restrict__ tile_item) {
+// key_scene gives the scene of every tile key (each scene holds a stable
+// range of the key space).  Items of FP32-SVD scenes take slots from 0 up
+// (count n_items[0]), items of FP64-SVD scenes slots from item_top - 1 down
+// (count n_items[1]), so that the gather of each SVD form is one launch over
+// a contiguous range.
+__global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, const uint32_t* __restrict__ key_scene,
+                        const SceneDev* __restrict__ scenes, uint32_t chunk, uint32_t item_top,
+                        Item* __restrict__ items, uint32_t* __restrict__ n_items, uint32_t* __restrict__ tile_item) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= K) return;
   const uint32_t a = tile_start[t], b = tile_start[t + 1];
   if (b <= a) return;
-  // last scene whose key offset is <= t
-  uint32_t lo = 0, hi = n_scenes;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) / 2;
-    if (key_offs[mid] <= t) lo = mid;
-    else hi = mid;
-  }
+  const uint32_t scene = key_scene[t];
+  if (scene == 0xffffffffu) return;  // no live scene holds this key (cannot carry particles)
   const uint32_t cnt = b - a;
   chunk = chunk ? chunk : cnt;
   const uint32_t pieces = (cnt + chunk - 1) / chunk;
-  const uint32_t scene = scene_ids[lo];
   const bool up = scenes[scene].svd64 == 0u;
   const uint32_t base = atomicAdd(&n_items[up ? 0 : 1], pieces);
   for (uint32_t i = 0; i < pieces; ++i) {
@@ -430,7 +425,7 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
     it.start = a + i * chunk;
     it.count = min(chunk, cnt - i * chunk);
     it.scene = scene;
-    it.tile = t - key_offs[lo];
+    it.tile = t - scenes[scene].key_off;
     const uint32_t slot = up ? base + i : item_top - 1u - (base + i);
     items[slot] = it;
     if (tile_item && i == 0) tile_item[t] = slot;
@@ -666,15 +661,26 @@ cudaError_t launch_reorder(const float* src, float* dst, uint32_t cap, const uin
 }
 
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
-                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids,
-                         const SceneDev* scenes, uint32_t chunk, uint32_t item_top, Item* items, uint32_t* n_items,
-                         uint32_t* tile_item, cudaStream_t st) {
+                         const uint32_t* key_scene, const SceneDev* scenes, uint32_t chunk, uint32_t item_top,
+                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st) {
   cudaMemsetAsync(n_items, 0, 2 * sizeof(uint32_t), st);
   if (tile_item) cudaMemsetAsync(tile_item, 0xff, (size_t)(K + 1) * sizeof(uint32_t), st);
   k_tile_start<<<(K + 1 + 255) / 256, 256, 0, st>>>(sorted_keys, n_live, K, shift, tile_start);
   if (K > 0)
-    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_offs, n_scenes, scene_ids, scenes, chunk, item_top,
-                                             items, n_items, tile_item);
+    k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_scene, scenes, chunk, item_top, items, n_items,
+                                             tile_item);
+  return cudaGetLastError();
+}
+
+__global__ void k_fill_u32(uint32_t* __restrict__ p, uint64_t n, uint32_t v) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+cudaError_t launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 4096);
+  k_fill_u32<<<(unsigned)blocks, 256, 0, st>>>(p, n, v);
   return cudaGetLastError();
 }
 

@@ -77,9 +77,10 @@ cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene,
 // Work list of the regrouped particles (see k_items): FP32-SVD items in slots
 // [0, n_items[0]), FP64-SVD items in [item_top - n_items[1], item_top).
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
-                         const uint32_t* key_offs, uint32_t n_scenes, const uint32_t* scene_ids,
-                         const SceneDev* scenes, uint32_t chunk, uint32_t item_top, Item* items, uint32_t* n_items,
-                         uint32_t* tile_item, cudaStream_t st);
+                         const uint32_t* key_scene, const SceneDev* scenes, uint32_t chunk, uint32_t item_top,
+                         Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);
+// p[0, n) = v, stream-ordered.
+cudaError_t launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st);
 cudaError_t launch_pack_positions(const PoolDev& p, const uint32_t* slot_of, uint32_t id_base, uint32_t n,
                                   float4* out, cudaStream_t st);
 cudaError_t launch_gather_xyz(const PoolDev& p, int first, const uint32_t* slot_of, uint32_t id_base, uint32_t n,

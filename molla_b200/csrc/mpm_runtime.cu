@@ -255,8 +255,6 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   touched[1].alloc(cell_cap / kCellBlock);
   scenes_d.alloc(max_scenes);
   status_d.alloc((size_t)kStatusWords * max_scenes);
-  key_offs_d.alloc(max_scenes);
-  scene_ids_d.alloc(max_scenes);
   n_items.alloc(2);
   totals_d.alloc(8);
   MPM_CK(cudaMallocHost((void**)&scenes_h, sizeof(SceneDev) * max_scenes));
@@ -275,6 +273,9 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   MPM_CK(cudaMemsetAsync(scenes_d.ptr, 0, scenes_d.bytes(), stream));
   ids.init(cap);
   cells.init(cell_cap);
+  // tile keys carry 6 cell bits below them in 32-bit sort keys, and the
+  // all-ones key marks removed particles
+  keyr.init((1ull << (32 - kCellBits)) - 2);
   grid_gather32 = gather_grid_size(false);
   grid_gather64 = gather_grid_size(true);
   grid_scatter = scatter_grid_size();
@@ -336,52 +337,37 @@ uint64_t Group::resident_bytes() const {
   return b;
 }
 
-// Recompute key offsets, item capacity and scene records after a change of
-// membership.
-void Group::rebuild_layout() {
-  std::vector<uint32_t> offs, sids;
-  uint64_t k = 0;
-  for (uint32_t i = 0; i < scenes.size(); ++i) {
-    SceneHost& s = scenes[i];
-    if (!s.live) continue;
-    s.key_off = (uint32_t)k;
-    offs.push_back((uint32_t)k);
-    sids.push_back(i);
-    k += s.tiles;
-    if ((k << kCellBits) >= 0xfffffff0ull) throw Error(MPM_ERR_INVALID, "MPM group key space exceeds 32 bits");
-  }
-  key_space = (uint32_t)k;
-  layout_scenes = (uint32_t)offs.size();
-  if (tile_start.count < (size_t)key_space + 2) tile_start.alloc((size_t)key_space + 2);
+// Geometric growth; the contents are not kept.
+template <class T> static void grow(DevBuf<T>& b, size_t need) {
+  if (b.count < need) b.alloc(std::max(need, b.count + b.count / 2));
+}
+
+// Geometric growth keeping the contents (stream-ordered copy, then the old
+// allocation is freed).
+template <class T> static void grow_keep(DevBuf<T>& b, size_t need, cudaStream_t st) {
+  if (b.count >= need) return;
+  DevBuf<T> nb(std::max(need, b.count + b.count / 2));
+  if (b.count) MPM_CK(cudaMemcpyAsync(nb.ptr, b.ptr, b.bytes(), cudaMemcpyDeviceToDevice, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  std::swap(b.ptr, nb.ptr);
+  std::swap(b.count, nb.count);
+}
+
+void Group::layout_changed() {
+  key_space = (uint32_t)keyr.high_water();
+  grow(tile_start, (size_t)key_space + 2);
   const size_t max_items = max_item_count();
-  if (items.count < max_items) items.alloc(max_items);
-  if (item_order.count < 64 * max_items) item_order.alloc(64 * max_items);
-  item_top = (uint32_t)max_items;
+  if (items.count < max_items) {
+    grow(items, max_items);
+    grow(item_order, 64 * items.count);
+  }
+  // The work list's FP64-SVD items count down from item_top: it may change
+  // only here, where a regrouping (which rebuilds the list) falls due.
+  item_top = (uint32_t)items.count;
   if (deterministic) {
-    const size_t tiles = (size_t)key_space + 2;
-    if (tile_item.count < tiles) tile_item.alloc(tiles);
-    if (det_blocks.count < max_items * kTileNodes) det_blocks.alloc(max_items * kTileNodes);
+    grow(tile_item, (size_t)key_space + 2);
+    grow(det_blocks, (size_t)item_top * kTileNodes);
   }
-  if (!offs.empty()) {
-    MPM_CK(cudaMemcpyAsync(key_offs_d.ptr, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, stream));
-    MPM_CK(cudaMemcpyAsync(scene_ids_d.ptr, sids.data(), sids.size() * 4, cudaMemcpyHostToDevice, stream));
-  }
-  for (uint32_t i = 0; i < scenes.size(); ++i) {
-    SceneHost& s = scenes[i];
-    SceneDev d = s.live ? make_scene_dev(s.cfg, s.rows, s.dt) : scenes_h[i];
-    if (s.live) {
-      d.n_rigid = s.n_rigid;
-      d.key_off = s.key_off;
-      d.status = i;
-      d.grid_off = s.grid_off;
-      d.id_base = s.id_base;
-      d.n_particles = s.n;
-    } else {
-      d.live = 0;
-    }
-    scenes_h[i] = d;
-  }
-  MPM_CK(cudaStreamSynchronize(stream));  // host staging is rewritten below on the next change
   scenes_dirty = true;
   need_regroup = true;
   invalidate_graphs();
@@ -420,6 +406,14 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
     ids.release(id0, n);
     throw Error(MPM_ERR_BUSY, "MPM group grid pool is full");
   }
+  const uint32_t w = (cfg.grid_size + 3u) / 4u;
+  const uint64_t tiles = (uint64_t)w * w * w;
+  uint64_t k0 = 0;
+  if (!keyr.alloc(tiles, 1, &k0)) {
+    ids.release(id0, n);
+    cells.release(g0, glen);
+    throw Error(MPM_ERR_BUSY, "MPM group key space is full");
+  }
   if (sid == scenes.size()) scenes.emplace_back();
   SceneHost& s = scenes[sid];
   s.live = true;
@@ -430,8 +424,8 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   s.id_base = (uint32_t)id0;
   s.grid_off = g0;
   s.grid_len = glen;
-  const uint32_t w = (cfg.grid_size + 3u) / 4u;
-  s.tiles = w * w * w;
+  s.tiles = (uint32_t)tiles;
+  s.key_off = (uint32_t)k0;
 
   // upload particles
   if (n) {
@@ -462,46 +456,29 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   MPM_CK(cudaMemsetAsync(rigid_blocks.ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   MPM_CK(cudaMemsetAsync(touched[0].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
   MPM_CK(cudaMemsetAsync(touched[1].ptr + g0 / kCellBlock, 0, glen / kCellBlock, stream));
-  {
-    std::vector<uint32_t> bs(glen / kCellBlock, sid);
-    MPM_CK(cudaMemcpyAsync(block_scene.ptr + g0 / kCellBlock, bs.data(), bs.size() * 4, cudaMemcpyHostToDevice,
-                           stream));
-    MPM_CK(cudaStreamSynchronize(stream));
-  }
+  MPM_CK(launch_fill_u32(block_scene.ptr + g0 / kCellBlock, glen / kCellBlock, sid, stream));
+  grow_keep(key_scene, (size_t)keyr.high_water(), stream);
+  MPM_CK(launch_fill_u32(key_scene.ptr + k0, tiles, sid, stream));
+  eng->launches += 2;
   MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, stream));
   n_live += n;
-  rebuild_layout();
+  SceneDev d = make_scene_dev(cfg, rows, dt);
+  d.n_rigid = 0;
+  d.key_off = s.key_off;
+  d.status = sid;
+  d.grid_off = g0;
+  d.id_base = s.id_base;
+  d.n_particles = n;
+  scenes_h[sid] = d;
+  s.n_rigid = 0;
+  layout_changed();
   return sid;
 }
 
 void Group::remove_scene(uint32_t sid) {
-  if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
-  SceneHost& s = scenes[sid];
-  const uint32_t removed = s.n;
-  s.live = false;
-  s.n_rigid = 0;
-  rebuild_layout();  // marks the scene record dead, new key offsets
-  // Compact: keys of every pooled particle (dead ones get 0xffffffff), sort,
-  // keep the live prefix (scenes retired earlier leave with it).
-  sync_scenes(stream);
-  const uint32_t n_slots = n_live;
-  MPM_CK(launch_keys(pool(), n_slots, stream));
-  eng->launches += 1;
-  n_live -= removed;
-  regroup(false, stream);
-  finish_retirements();
-  // Dead identities keep key 0xffffffff for later sorts.
-  MPM_CK(cudaMemsetAsync(keys_by_id.ptr + s.id_base, 0xff, (size_t)s.n * 4, stream));
-  {
-    std::vector<uint32_t> bs(s.grid_len / kCellBlock, 0xffffffffu);
-    MPM_CK(cudaMemcpyAsync(block_scene.ptr + s.grid_off / kCellBlock, bs.data(), bs.size() * 4,
-                           cudaMemcpyHostToDevice, stream));
-    MPM_CK(cudaStreamSynchronize(stream));
-  }
-  ids.release(s.id_base, s.n);
-  cells.release(s.grid_off, s.grid_len);
-  s.n = 0;
-  need_regroup = n_live > 0;
+  // A retirement compacted out at once: one regrouping of the pool.
+  retire_scene(sid);
+  compact(stream);
 }
 
 void Group::retire_scene(uint32_t sid) {
@@ -525,33 +502,36 @@ void Group::retire_scene(uint32_t sid) {
 void Group::finish_retirements() {
   if (!compact_issued) return;
   compact_issued = false;
-  std::vector<uint32_t> bs;
   for (uint32_t sid : retiring) {
     SceneHost& s = scenes[sid];
-    bs.assign(s.grid_len / kCellBlock, 0xffffffffu);
-    if (!bs.empty()) {
-      MPM_CK(cudaMemcpyAsync(block_scene.ptr + s.grid_off / kCellBlock, bs.data(), bs.size() * 4,
-                             cudaMemcpyHostToDevice, stream));
-      MPM_CK(cudaStreamSynchronize(stream));  // bs is reused
-    }
+    MPM_CK(launch_fill_u32(block_scene.ptr + s.grid_off / kCellBlock, s.grid_len / kCellBlock, 0xffffffffu, stream));
+    MPM_CK(launch_fill_u32(key_scene.ptr + s.key_off, s.tiles, 0xffffffffu, stream));
+    eng->launches += 2;
     ids.release(s.id_base, s.n);
     cells.release(s.grid_off, s.grid_len);
+    keyr.release(s.key_off, s.tiles);
     n_live -= s.n;
     s.n = 0;
     s.retiring = false;
   }
   retiring.clear();
   n_retiring = 0;
+  // Later regroupings sort fewer keys over a smaller key space; graphs
+  // captured with the old counts are stale.
+  key_space = (uint32_t)keyr.high_water();
+  invalidate_graphs();
 }
 
-void Group::set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st) {
+void Group::set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st, bool fresh) {
   if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
-  uint32_t done = 0;
-  MPM_CK(cudaMemcpyAsync(&done, status_d.ptr + (size_t)sid * kStatusWords + 1, 4, cudaMemcpyDeviceToHost, st));
-  MPM_CK(cudaStreamSynchronize(st));
+  uint32_t done = 0;  // a scene just added has completed none
+  if (!fresh) {
+    MPM_CK(cudaMemcpyAsync(&done, status_d.ptr + (size_t)sid * kStatusWords + 1, 4, cudaMemcpyDeviceToHost, st));
+    MPM_CK(cudaStreamSynchronize(st));
+  }
   const uint32_t budget = substeps ? done + substeps : 0u;
-  MPM_CK(cudaMemcpyAsync(status_d.ptr + (size_t)sid * kStatusWords + 2, &budget, 4, cudaMemcpyHostToDevice, st));
-  MPM_CK(cudaStreamSynchronize(st));
+  MPM_CK(launch_fill_u32(status_d.ptr + (size_t)sid * kStatusWords + 2, 1, budget, st));
+  eng->launches += 1;
 }
 
 bool Group::any_svd32() const {
@@ -728,12 +708,12 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   eng->launches += 1;
   cur ^= 1;
   if (move_records) rec_cur ^= 1;
-  if (n_retiring) compact_issued = true;
+  if (!retiring.empty()) compact_issued = true;
   // Items: whole tiles for the fixed-order scatter (one item per tile);
   // otherwise tiles cut into pieces of at most kStageMax particles, whose
   // scatter records fit the shared-memory stage.
-  MPM_CK(launch_items(skeys, kCellBits, n_keep, key_space, tile_start.ptr, key_offs_d.ptr, layout_scenes,
-                      scene_ids_d.ptr, scenes_d.ptr, deterministic ? 0u : (uint32_t)kStageMax, item_top, items.ptr,
+  MPM_CK(launch_items(skeys, kCellBits, n_keep, key_space, tile_start.ptr, key_scene.ptr, scenes_d.ptr,
+                      deterministic ? 0u : (uint32_t)kStageMax, item_top, items.ptr,
                       n_items.ptr, deterministic ? tile_item.ptr : nullptr, st));
   eng->launches += key_space ? 2 : 1;
   if (!deterministic && key_space) {
@@ -997,16 +977,22 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
 
 void Group::compact(cudaStream_t st) {
   eng->check();
-  if (!n_retiring) return;
-  sync_scenes(st);
-  regroup(true, st);
+  if (retiring.empty()) return;
+  if (n_retiring && n_live > n_retiring) {
+    sync_scenes(st);
+    regroup(true, st);
+  } else {
+    // nothing live to sort out from among them: every slot is dropped
+    compact_issued = true;
+    need_regroup = true;
+  }
   finish_retirements();
 }
 
 void Group::step(uint32_t substeps, cudaStream_t st) {
   eng->check();
   if (substeps && n_live == n_retiring) compact(st);
-  if (!substeps || n_live == 0) return;
+  if (!substeps || n_live == 0 || n_live == n_retiring) return;
   sync_scenes(st);
   run_substeps(substeps, st);
   finish_retirements();
@@ -1030,7 +1016,7 @@ Group::GraphKey Group::graph_key(uint32_t substeps) const {
 void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
   eng->check();
   if (substeps && repeat && n_live == n_retiring) compact(st);
-  if (!substeps || n_live == 0 || !repeat) return;
+  if (!substeps || n_live == 0 || n_live == n_retiring || !repeat) return;
   sync_scenes(st);
   for (uint32_t r = 0; r < repeat; ++r) {
     const GraphKey key = graph_key(substeps);
@@ -1085,7 +1071,7 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
       need_regroup = false;
       since = 0;
       ++regroups;
-      if (n_retiring) compact_issued = true;
+      if (!retiring.empty()) compact_issued = true;
     };
     if (need_regroup || deterministic) regrouped(false);
     int a = acc_zero;

@@ -194,7 +194,11 @@ class Group {
   // scenes
   DevBuf<SceneDev> scenes_d;
   DevBuf<uint32_t> status_d;
-  DevBuf<uint32_t> tile_start, key_offs_d, scene_ids_d, n_items;
+  DevBuf<uint32_t> tile_start, n_items;
+  // Scene of every tile key (0xffffffff: no live scene).  Each scene holds a
+  // stable range of the key space (allocated from `keyr` when it is added),
+  // so adding or retiring a scene re-keys no other scene.
+  DevBuf<uint32_t> key_scene;
   DevBuf<Item> items;
   DevBuf<uint8_t> item_order;  // scatter lane order, 64 cells per item
   DevBuf<uint32_t> tile_item;  // deterministic mode: item of each occupied tile
@@ -204,12 +208,9 @@ class Group {
   SceneDev* scenes_h = nullptr;
 
   std::vector<SceneHost> scenes;
-  RangeAlloc ids, cells;
+  RangeAlloc ids, cells, keyr;
   uint32_t n_live = 0;
-  uint32_t key_space = 0;
-  // Scenes listed in key_offs_d / scene_ids_d (those live at the last layout
-  // change; a scene retired since keeps its empty key range until the next).
-  uint32_t layout_scenes = 0;
+  uint32_t key_space = 0;  // one past the highest allocated tile key
   int cur = 0;       // current particle buffer
   int acc_zero = 0;  // accumulator known to be all zero
   int acc_last = 1;  // accumulator holding the last scatter
@@ -288,7 +289,7 @@ class Group {
   // particle kernels skip the scene once its completed-substep count has
   // passed the budget, so a scene advances by exactly that many substeps
   // however long the calls that step the group are.
-  void set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st);
+  void set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st, bool fresh = false);
   // Regroups now if retired scenes await compaction, and gives their
   // slots, identities and grid ranges back.
   void compact(cudaStream_t st);
@@ -337,7 +338,10 @@ class Group {
   uint32_t live_scenes() const;
 
  private:
-  void rebuild_layout();
+  // Buffers sized by the key space and the item capacity, after a scene was
+  // added: grows them (geometrically), marks a regrouping due and drops the
+  // captured graphs.
+  void layout_changed();
   void invalidate_graphs();
   // Host bookkeeping after a regrouping that dropped the retiring scenes.
   void finish_retirements();

@@ -133,6 +133,7 @@ pub struct mpm_server_stats {
     pub admitted: u64, pub completed: u64, pub resident_scenes: u64, pub resident_bytes: u64,
     pub particle_steps: u64,
     pub tick_ms_p50: f64, pub tick_ms_p99: f64, pub queue_ms_p50: f64, pub queue_ms_p99: f64,
+    pub admit_ms: f64, pub step_ms: f64, pub retire_ms: f64, pub ticks: u64,
 }
 #[repr(C)] pub struct mpm_sim64 { _p: [u8; 0] }
 
