@@ -85,24 +85,71 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons during the
+    timed region: through NVML every ~2 ms when it is available (a timed
+    region of a few tens of ms still gets many samples), else through
+    nvidia-smi every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, reason bits) from NVML
+        self.sm_max = None
+        self.nvml = None
+        self.stop = False
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        handle = None
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        return pynvml, handle
+
+    def _poll(self):
+        nv, h = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop:
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+            except Exception:
+                break
+            time.sleep(0.002)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            nv, h = self.nvml
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            self.source = "nvml"
+            time.sleep(0.01)
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            self.source = "nvidia-smi"
         except Exception:
             self.proc = None
         return self
@@ -112,6 +159,9 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self.stop = True
+        if self.nvml:
+            self.thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -120,7 +170,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons = [], self.sm_max, set()
+        for mhz, bits in self.samples:
+            sm.append(mhz)
+            for name, bit in self.REASON_BITS.items():
+                if bits & bit:
+                    reasons.add(name)
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
@@ -135,8 +190,9 @@ class ClockSampler:
                 if val.lower().startswith("active"):
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["unsampled"], "source": self.source}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "source": self.source}
 
 
 def dist_env():
@@ -345,10 +401,13 @@ def run_ours(args):
     sim.step_n(scene.dt, first)
     engine.synchronize()
     tune = None
+    shapes = None
     if args.sort_interval > 0:
         interval = args.sort_interval
     else:
-        interval, tune = sim.autotune(scene.dt, probe_substeps=32)
+        # interval, item size, fused or separate kernels, CTAs per SM
+        shapes, tune = sim.autotune_shapes(scene.dt, probe_substeps=32)
+        interval = shapes["sort_interval"]
     sim.set_sort_interval(interval)
     if start_at > first:
         sim.step_n(scene.dt, start_at - first)
@@ -484,8 +543,9 @@ def run_ours(args):
             "warmup": start_at, "ms_per_step": 1000.0 * elapsed_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 svd)" if svd_prec else "f32",
             "data": "synthetic (seeded boxes; no dataset)",
-            "config": dict(meta, active_cells=active, sort_interval=interval,
-                           autotune_ms_per_substep=tune,
+            "config": dict(meta, active_cells=active, sort_interval=interval, shapes=shapes,
+                           autotune_probes=[{"knob": k, "value": v, "ms_per_substep": round(ms, 4)}
+                                            for k, v, ms in (tune or [])],
                            timed_substeps=f"{start_at}..{start_at + args.steps} of the scene's trajectory "
                                           f"(untimed advance of {start_at} substeps, --warmup included)",
                            regroups_in_window=regroups_in_window,
@@ -657,7 +717,8 @@ def measure_batched(args, quiet=False):
     for s in ss:
         g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt)
     g.step_graph(max(3, args.batched_advance // 2), 1)
-    chosen, tune = g.autotune(probe_substeps=32)
+    shapes, tune = g.autotune_shapes(probe_substeps=32)
+    chosen = shapes["sort_interval"]
     g.step_graph(max(3, args.batched_advance - args.batched_advance // 2), 1)
     g.step_graph(steps, 1)  # captures the timed sequence's graph
     engine.synchronize()
@@ -711,7 +772,7 @@ def measure_batched(args, quiet=False):
     engine.close()
     return {
         "workload": f"batched: {len(ss)} scenes, grids 32^3..128^3, {total} particles, mixed elastic/snow, FP32, "
-                    f"CUDA-graph captured, autotuned regroup interval; {steps} substeps timed after "
+                    f"CUDA-graph captured, autotuned shapes (regroup interval, item size, fused or separate kernels, CTAs per SM); {steps} substeps timed after "
                     f"{args.batched_advance + steps} untimed",
         "value": value, "unit": UNIT, "ms_per_step": 1000.0 * t_batched / steps,
         "plain": {"value": plain, "ms_per_step": 1000.0 * t_plain / steps,
@@ -719,7 +780,8 @@ def measure_batched(args, quiet=False):
         "batched_over_plain": value / plain,
         "p50_step_ms": float(np.percentile(lat, 50)) if lat else None,
         "p99_step_ms": float(np.percentile(lat, 99)) if lat else None,
-        "scenes": len(ss), "particles": total, "regroup_interval": chosen, "autotune_ms_per_substep": tune,
+        "scenes": len(ss), "particles": total, "regroup_interval": chosen, "shapes": shapes,
+        "autotune_probes": [{"knob": k, "value": v, "ms_per_substep": round(ms, 4)} for k, v, ms in tune],
         "stages_ms_per_step": {k: v[1] / 8 for k, v in prof.items()},
         "gpu_launches": int(launches), "clocks": clocks.summary(),
     }

@@ -421,6 +421,44 @@ MPM_API int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const 
  * particles). */
 MPM_API int mpm_group_tune(mpm_group* group, uint32_t chunk, uint32_t sort_interval);
 
+/* Launch and tile shapes of the substep (no reference counterpart): the
+ * regroup interval, the particles per work item (128..640; a tile with more
+ * is cut into several items), whether the non-final substeps run the fused
+ * gather + scatter kernel, and the resident gather and scatter CTAs per SM
+ * of the persistent kernels (at most their occupancy maxima). */
+typedef struct mpm_shapes {
+  uint32_t sort_interval;
+  uint32_t item_particles;
+  uint32_t fused;
+  uint32_t gather_ctas_per_sm;
+  uint32_t scatter_ctas_per_sm;
+  uint32_t reserved[3];
+} mpm_shapes;
+/* One timing of the shapes autotuner: knob 0 interval, 1 item particles,
+ * 2 fused, 3 gather CTAs per SM, 4 scatter CTAs per SM; the value tried and
+ * the measured ms per substep. */
+typedef struct mpm_tune_probe {
+  uint32_t knob;
+  uint32_t value;
+  float ms_per_substep;
+} mpm_tune_probe;
+/* Autotuner of the shapes (no reference counterpart): tunes the knobs in the
+ * order interval {8,16,32,64}, item particles {640,512,384,256}, fused {0,1},
+ * gather CTAs per SM {max, max-1}, scatter CTAs per SM {max, max-1}, each
+ * over its candidates with the earlier knobs fixed at their best, timing
+ * max(probe_substeps, 2 x interval) substeps per candidate on a snapshot of
+ * the device state, which is restored (the scenes do not advance).  Applies
+ * and returns the shapes kept; probes (may be NULL) receive up to `cap`
+ * timings, *n_probes their count. */
+MPM_API int mpm_group_autotune_shapes(mpm_group* group, uint32_t probe_substeps, mpm_shapes* chosen,
+                                      mpm_tune_probe* probes, uint32_t cap, uint32_t* n_probes);
+/* The same for a single simulation (dt as in mpm_step_n). */
+MPM_API int mpm_autotune_shapes(mpm_sim* sim, float dt, uint32_t probe_substeps, mpm_shapes* chosen,
+                                mpm_tune_probe* probes, uint32_t cap, uint32_t* n_probes);
+/* The shapes in force; setting them marks a regrouping due. */
+MPM_API int mpm_group_get_shapes(mpm_group* group, mpm_shapes* out);
+MPM_API int mpm_group_set_shapes(mpm_group* group, const mpm_shapes* in);
+
 /* ---- soil checkpoints -------------------------------------------------------
  * The reference's lossless particle checkpoint byte format
  * (crates/molla-solvers/src/mpm_checkpoint.rs:71-92, :187-275): magic

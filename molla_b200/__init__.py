@@ -501,6 +501,11 @@ class MpmSimulation:
         return int(chosen.value), dict(zip(c.tolist(), ms.tolist()))
 
     # -- stepping -----------------------------------------------------------
+    def autotune_shapes(self, dt: float, probe_substeps: int = 32):
+        """MpmGroup.autotune_shapes for this simulation."""
+        return _tune_shapes(lambda sh, pr, cap, n: _ffi.lib().mpm_autotune_shapes(
+            self._h, dt, probe_substeps, sh, pr, cap, n))
+
     def step(self, dt: float, engine=None):
         self.step_n(dt, 1)
 
@@ -735,6 +740,23 @@ class MpmSimulation64:
         return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
 
 
+TUNE_KNOBS = ("sort_interval", "item_particles", "fused", "gather_ctas_per_sm", "scatter_ctas_per_sm")
+
+
+def _shapes_dict(sh) -> dict:
+    return {k: int(getattr(sh, k)) for k in TUNE_KNOBS}
+
+
+def _tune_shapes(call):
+    sh = _ffi.mpm_shapes()
+    cap = 64
+    probes = (_ffi.mpm_tune_probe * cap)()
+    n = C.c_uint32()
+    _check(call(C.byref(sh), probes, cap, C.byref(n)))
+    return _shapes_dict(sh), [(TUNE_KNOBS[p.knob], int(p.value), float(p.ms_per_substep))
+                              for p in probes[: min(n.value, cap)]]
+
+
 class MpmGroup:
     """Many independent scenes stepped by shared launches (no reference
     equivalent; same per-scene numerics as MpmSimulation)."""
@@ -782,6 +804,26 @@ class MpmGroup:
         chosen = C.c_uint32()
         _check(_ffi.lib().mpm_group_autotune(self._h, probe_substeps, _up(c), len(c), _fp(ms), C.byref(chosen)))
         return int(chosen.value), dict(zip(c.tolist(), ms.tolist()))
+
+    def autotune_shapes(self, probe_substeps: int = 32):
+        """Tunes the regroup interval, the item size, fused vs separate
+        kernels and the CTAs per SM of the gather and scatter on a snapshot
+        (the scenes do not advance).  Returns (shapes dict, [(knob, value,
+        ms per substep), ...])."""
+        return _tune_shapes(lambda sh, pr, cap, n: _ffi.lib().mpm_group_autotune_shapes(
+            self._h, probe_substeps, sh, pr, cap, n))
+
+    def shapes(self) -> dict:
+        sh = _ffi.mpm_shapes()
+        _check(_ffi.lib().mpm_group_get_shapes(self._h, C.byref(sh)))
+        return _shapes_dict(sh)
+
+    def set_shapes(self, **kw):
+        sh = _ffi.mpm_shapes()
+        _check(_ffi.lib().mpm_group_get_shapes(self._h, C.byref(sh)))
+        for k, v in kw.items():
+            setattr(sh, k, int(v))
+        _check(_ffi.lib().mpm_group_set_shapes(self._h, C.byref(sh)))
 
     def read_positions(self, sid: int) -> np.ndarray:
         n = self.counts[sid]

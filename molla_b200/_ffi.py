@@ -89,6 +89,21 @@ class mpm_server_stats(C.Structure):
     ]
 
 
+class mpm_shapes(C.Structure):
+    _fields_ = [
+        ("sort_interval", C.c_uint32),
+        ("item_particles", C.c_uint32),
+        ("fused", C.c_uint32),
+        ("gather_ctas_per_sm", C.c_uint32),
+        ("scatter_ctas_per_sm", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
+    ]
+
+
+class mpm_tune_probe(C.Structure):
+    _fields_ = [("knob", C.c_uint32), ("value", C.c_uint32), ("ms_per_substep", C.c_float)]
+
+
 class mpm_render_view(C.Structure):
     _fields_ = [
         ("positions", C.c_void_p),
@@ -193,6 +208,10 @@ SIGNATURES = {
     "mpm_group_autotune": (I, [P, U32, U32P, U32, F32P, U32P]),
     "mpm_autotune": (I, [P, C.c_float, U32, U32P, U32, F32P, U32P]),
     "mpm_group_tune": (I, [P, U32, U32]),
+    "mpm_group_autotune_shapes": (I, [P, U32, C.POINTER(mpm_shapes), C.POINTER(mpm_tune_probe), U32, U32P]),
+    "mpm_autotune_shapes": (I, [P, C.c_float, U32, C.POINTER(mpm_shapes), C.POINTER(mpm_tune_probe), U32, U32P]),
+    "mpm_group_get_shapes": (I, [P, C.POINTER(mpm_shapes)]),
+    "mpm_group_set_shapes": (I, [P, C.POINTER(mpm_shapes)]),
     "mpm_set_rigid_spheres": (I, [P, F32P, U32]),
     "mpm_read_rigid_wrenches": (I, [P, F32P, U32, U32P]),
     "mpm_checkpoint_save": (I, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),

@@ -1057,6 +1057,74 @@ int mpm_autotune(mpm_sim* sim, float dt, uint32_t probe_substeps, const uint32_t
   });
 }
 
+static void shapes_to_c(const mpm::Group::Shapes& sh, mpm_shapes* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->sort_interval = sh.interval;
+  out->item_particles = sh.item_particles;
+  out->fused = sh.fused;
+  out->gather_ctas_per_sm = sh.gather_per_sm;
+  out->scatter_ctas_per_sm = sh.scatter_per_sm;
+}
+
+static void tune_shapes(mpm::Group& g, uint32_t probe_substeps, mpm_shapes* chosen, mpm_tune_probe* probes,
+                        uint32_t cap, uint32_t* n_probes, cudaStream_t st) {
+  using G = mpm::Group;
+  std::vector<G::Probe> out;
+  const G::Shapes sh = g.autotune_shapes(
+      probe_substeps ? probe_substeps : 32,
+      {{G::kKnobInterval, {}}, {G::kKnobItem, {}}, {G::kKnobFused, {}}, {G::kKnobGatherCtas, {}},
+       {G::kKnobScatterCtas, {}}},
+      &out, st);
+  if (chosen) shapes_to_c(sh, chosen);
+  if (probes)
+    for (uint32_t i = 0; i < cap && i < out.size(); ++i) probes[i] = {out[i].knob, out[i].value, out[i].ms};
+  if (n_probes) *n_probes = (uint32_t)out.size();
+}
+
+int mpm_group_autotune_shapes(mpm_group* group, uint32_t probe_substeps, mpm_shapes* chosen, mpm_tune_probe* probes,
+                              uint32_t cap, uint32_t* n_probes) {
+  return guard([&] {
+    REQUIRE(group, MPM_ERR_INVALID, "null group");
+    tune_shapes(*group->g, probe_substeps, chosen, probes, cap, n_probes, group->eng->stream);
+  });
+}
+
+int mpm_autotune_shapes(mpm_sim* sim, float dt, uint32_t probe_substeps, mpm_shapes* chosen, mpm_tune_probe* probes,
+                        uint32_t cap, uint32_t* n_probes) {
+  return guard([&] {
+    REQUIRE(sim, MPM_ERR_INVALID, "null simulation");
+    sim_check_step(sim, dt);
+    REQUIRE(!sim->order_enabled, MPM_ERR_INVALID, "particle ordering fixes the interval at one substep");
+    if (sim->count == 0) {
+      if (chosen) shapes_to_c(sim->group->shapes(), chosen);
+      if (n_probes) *n_probes = 0;
+      return;
+    }
+    sim->group->set_scene_dt(sim->sid, dt);
+    tune_shapes(*sim->group, probe_substeps, chosen, probes, cap, n_probes, sim->eng->stream);
+    sim->sort_interval = sim->group->sort_interval;
+    sim->apply_group_settings();
+    sim->invalidate();
+  });
+}
+
+int mpm_group_get_shapes(mpm_group* group, mpm_shapes* out) {
+  return guard([&] {
+    REQUIRE(group && out, MPM_ERR_INVALID, "null argument");
+    shapes_to_c(group->g->shapes(), out);
+  });
+}
+
+int mpm_group_set_shapes(mpm_group* group, const mpm_shapes* in) {
+  return guard([&] {
+    REQUIRE(group && in, MPM_ERR_INVALID, "null argument");
+    REQUIRE(in->sort_interval >= 1, MPM_ERR_INVALID, "the regroup interval must be at least 1");
+    mpm::Group::Shapes sh{in->sort_interval, in->item_particles, in->fused ? 1u : 0u, in->gather_ctas_per_sm,
+                          in->scatter_ctas_per_sm};
+    group->g->apply_shapes(sh);
+  });
+}
+
 int mpm_group_set_deterministic(mpm_group* group, int enabled) {
   return guard([&] {
     REQUIRE(group, MPM_ERR_INVALID, "null group");

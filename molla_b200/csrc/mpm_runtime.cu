@@ -276,11 +276,12 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   // tile keys carry 6 cell bits below them in 32-bit sort keys, and the
   // all-ones key marks removed particles
   keyr.init((1ull << (32 - kCellBits)) - 2);
-  grid_gather32 = gather_grid_size(false);
-  grid_gather64 = gather_grid_size(true);
-  grid_scatter = scatter_grid_size();
-  grid_fused32 = fused_grid_size(false);
-  grid_fused64 = fused_grid_size(true);
+  const int nsm = std::max(eng->sms, 1);
+  occ_gather32 = std::max(1, gather_grid_size(false) / nsm);
+  occ_gather64 = std::max(1, gather_grid_size(true) / nsm);
+  occ_scatter = std::max(1, scatter_grid_size() / nsm);
+  occ_fused32 = std::max(1, fused_grid_size(false) / nsm);
+  occ_fused64 = std::max(1, fused_grid_size(true) / nsm);
   if (const char* env = std::getenv("MOLLA_MPM_FUSED")) fused_mode = std::strcmp(env, "0") != 0 ? 1 : 0;
   MPM_CK(cudaStreamSynchronize(stream));
 }
@@ -713,7 +714,7 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   // otherwise tiles cut into pieces of at most kStageMax particles, whose
   // scatter records fit the shared-memory stage.
   MPM_CK(launch_items(skeys, kCellBits, n_keep, key_space, tile_start.ptr, key_scene.ptr, scenes_d.ptr,
-                      deterministic ? 0u : (uint32_t)kStageMax, item_top, items.ptr,
+                      deterministic ? 0u : item_chunk, item_top, items.ptr,
                       n_items.ptr, deterministic ? tile_item.ptr : nullptr, st));
   eng->launches += key_space ? 2 : 1;
   if (!deterministic && key_space) {
@@ -726,6 +727,23 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   eng->prof_end(&pr, st);
 }
 
+int Group::gather_grid(bool f64) const {
+  const int mx = f64 ? occ_gather64 : occ_gather32;
+  return std::max(eng->sms, 1) * (gather_per_sm ? std::min<int>((int)gather_per_sm, mx) : mx);
+}
+
+int Group::fused_grid(bool f64) const {
+  // the fused kernel follows the gather's count, scaled to its own maximum
+  const int mx = f64 ? occ_fused64 : occ_fused32;
+  const int g = f64 ? occ_gather64 : occ_gather32;
+  const int k = gather_per_sm ? std::max(1, (int)(gather_per_sm * mx + g - 1) / g) : mx;
+  return std::max(eng->sms, 1) * std::min(k, mx);
+}
+
+int Group::scatter_grid() const {
+  return std::max(eng->sms, 1) * (scatter_per_sm ? std::min<int>((int)scatter_per_sm, occ_scatter) : occ_scatter);
+}
+
 // The gather runs once per SVD form present: over the FP32-SVD items, then
 // over the FP64-SVD items of the work list.
 void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
@@ -734,7 +752,7 @@ void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
   for (int f64 = 0; f64 < 2; ++f64) {
     if (!(f64 ? any_svd64() : any_svd32())) continue;
     MPM_CK(launch_gather(mode, keys, f64 != 0, pool(), f64 ? svd_tol64 : svd_tol32, svd_sweeps, reuse_svd ? 1 : 0,
-                         f64 ? grid_gather64 : grid_gather32, st));
+                         gather_grid(f64 != 0), st));
     eng->launches += 1;
   }
   eng->prof_end(&pr, st);
@@ -744,11 +762,11 @@ void Group::launch_scatter_pass(int acc_out, cudaStream_t st) {
   ProfRec pr;
   eng->prof_begin(kStageScatter, st, &pr);
   if (deterministic) {
-    MPM_CK(launch_scatter_det(pool(), det_blocks.ptr, acc_out, grid_scatter, st));
+    MPM_CK(launch_scatter_det(pool(), det_blocks.ptr, acc_out, scatter_grid(), st));
     MPM_CK(launch_combine_det(pool(), det_blocks.ptr, tile_item.ptr, key_space, acc_out, st));
     eng->launches += 1;
   } else {
-    MPM_CK(launch_scatter(pool(), rec_map[rec_cur], acc_out, grid_scatter, st));
+    MPM_CK(launch_scatter(pool(), rec_map[rec_cur], acc_out, scatter_grid(), st));
   }
   eng->prof_end(&pr, st);
   eng->launches += 1;
@@ -760,15 +778,57 @@ void Group::launch_fused_pass(int acc_out, bool keys, cudaStream_t st) {
   for (int f64 = 0; f64 < 2; ++f64) {
     if (!(f64 ? any_svd64() : any_svd32())) continue;
     MPM_CK(launch_fused(keys, f64 != 0, pool(), f64 ? svd_tol64 : svd_tol32, svd_sweeps, reuse_svd ? 1 : 0, acc_out,
-                        f64 ? grid_fused64 : grid_fused32, st));
+                        fused_grid(f64 != 0), st));
     eng->launches += 1;
   }
   eng->prof_end(&pr, st);
 }
 
+Group::Shapes Group::shapes() const {
+  Shapes sh;
+  sh.interval = sort_interval;
+  sh.item_particles = item_chunk;
+  sh.fused = use_fused() ? 1u : 0u;
+  sh.gather_per_sm = gather_per_sm ? gather_per_sm : (uint32_t)occ_gather32;
+  sh.scatter_per_sm = scatter_per_sm ? scatter_per_sm : (uint32_t)occ_scatter;
+  return sh;
+}
+
+void Group::apply_shapes(const Shapes& sh) {
+  if (sh.item_particles < kMinItemParticles || sh.item_particles > (uint32_t)kStageMax)
+    throw Error(MPM_ERR_INVALID, "MPM item size must be in 128..=" + std::to_string(kStageMax) + " particles");
+  if (sh.gather_per_sm < 1 || sh.scatter_per_sm < 1)
+    throw Error(MPM_ERR_INVALID, "MPM CTAs per SM must be at least 1");
+  if (sh.interval != sort_interval) {
+    sort_interval = sh.interval;
+    need_regroup = true;
+  }
+  if (sh.item_particles != item_chunk) {
+    item_chunk = sh.item_particles;
+    need_regroup = true;  // the work list is cut anew
+  }
+  fused_mode = sh.fused ? 1 : 0;
+  gather_per_sm = std::min<uint32_t>(sh.gather_per_sm, (uint32_t)std::max(occ_gather32, occ_gather64));
+  scatter_per_sm = std::min<uint32_t>(sh.scatter_per_sm, (uint32_t)occ_scatter);
+  invalidate_graphs();
+}
+
 uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_out, cudaStream_t st) {
-  eng->check();
   if (!n_live || !probe || n_cands <= 0) return sort_interval;
+  std::vector<Probe> probes;
+  const Shapes sh = autotune_shapes(probe, {{kKnobInterval, std::vector<uint32_t>(cands, cands + n_cands)}}, &probes, st);
+  for (size_t i = 0; i < probes.size() && ms_out; ++i) ms_out[i] = probes[i].ms;
+  return sh.interval;
+}
+
+Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair<uint32_t, std::vector<uint32_t>>>& knobs,
+                                     std::vector<Probe>* out, cudaStream_t st) {
+  eng->check();
+  Shapes best_sh = shapes();
+  if (!n_live || !probe) return best_sh;
+  // The probes regroup; retired scenes must not leave the pool behind the
+  // host's back.
+  if (n_retiring) throw Error(MPM_ERR_BUSY, "MPM autotune with retired scenes awaiting compaction");
   sync_scenes(st);
   // Snapshot of everything a substep reads or writes.
   const size_t pbytes = (size_t)kPlanes * cap * sizeof(float);
@@ -808,57 +868,85 @@ uint32_t Group::autotune(uint32_t probe, const uint32_t* cands, int n_cands, flo
     }
   };
   const int cur0 = cur, az0 = acc_zero, al0 = acc_last;
-  const bool nr0 = need_regroup;
   const uint64_t done0 = substeps_done, regroups0 = regroups;
-  const uint32_t interval0 = sort_interval;
-  // The probes regroup; retired scenes must not leave the pool behind the
-  // host's back.
-  if (n_retiring) throw Error(MPM_ERR_BUSY, "MPM autotune with retired scenes awaiting compaction");
   save(true);
   OwnedEvent e0, e1;
-  float best = 1e30f;
-  uint32_t best_i = interval0;
-  for (int c = 0; c < n_cands; ++c) {
+  auto rewind = [&]() {
     cur = cur0;
     acc_zero = az0;
     acc_last = al0;
-    need_regroup = true;  // every candidate starts from a fresh regrouping
-    if (c) save(false);
-    sort_interval = cands[c];
-    // at least two regroupings inside the timed window
-    const uint32_t n = std::max<uint32_t>(probe, 2u * cands[c]);
-    run_substeps(n, st);  // warm
-    cur = cur0;
-    acc_zero = az0;
-    acc_last = al0;
-    need_regroup = true;
+    need_regroup = true;  // every run starts from a fresh regrouping
     save(false);
+  };
+  auto time_current = [&]() {
+    // at least two regroupings inside the timed window
+    const uint32_t n = std::max<uint32_t>(probe, 2u * std::max<uint32_t>(sort_interval, 1u));
+    rewind();
+    run_substeps(n, st);  // warm
+    rewind();
     MPM_CK(cudaEventRecord(e0, st));
     run_substeps(n, st);
     MPM_CK(cudaEventRecord(e1, st));
     MPM_CK(cudaEventSynchronize(e1));
     float ms = 0.f;
     MPM_CK(cudaEventElapsedTime(&ms, e0, e1));
-    ms /= (float)n;
-    if (ms_out) ms_out[c] = ms;
-    if (ms < best) {
-      best = ms;
-      best_i = cands[c];
+    return ms / (float)n;
+  };
+  try {
+    for (const auto& kv : knobs) {
+      const uint32_t knob = kv.first;
+      std::vector<uint32_t> cands = kv.second;
+      if (cands.empty()) {
+        switch (knob) {
+          case kKnobInterval: cands = {8, 16, 32, 64}; break;
+          case kKnobItem: cands = {(uint32_t)kStageMax, 512, 384, 256}; break;
+          case kKnobFused: cands = {0, 1}; break;
+          case kKnobGatherCtas: cands = {best_sh.gather_per_sm, best_sh.gather_per_sm - 1}; break;
+          case kKnobScatterCtas: cands = {best_sh.scatter_per_sm, best_sh.scatter_per_sm - 1}; break;
+          default: throw Error(MPM_ERR_INVALID, "unknown MPM tuning knob");
+        }
+      }
+      if (deterministic && (knob == kKnobItem || knob == kKnobFused)) continue;  // whole tiles, never fused
+      float best = 1e30f;
+      Shapes keep = best_sh;
+      for (uint32_t v : cands) {
+        if (knob == kKnobFused ? v > 1 : v == 0) continue;
+        Shapes sh = best_sh;
+        switch (knob) {
+          case kKnobInterval: sh.interval = v; break;
+          case kKnobItem: sh.item_particles = std::min<uint32_t>(std::max<uint32_t>(v, kMinItemParticles), kStageMax); break;
+          case kKnobFused: sh.fused = v; break;
+          case kKnobGatherCtas: sh.gather_per_sm = v; break;
+          case kKnobScatterCtas: sh.scatter_per_sm = v; break;
+          default: break;
+        }
+        apply_shapes(sh);
+        const float ms = time_current();
+        if (out) out->push_back({knob, v, ms});
+        if (ms < best) {
+          best = ms;
+          keep = shapes();
+        }
+      }
+      best_sh = keep;
     }
+  } catch (...) {
+    rewind();
+    cudaStreamSynchronize(st);
+    substeps_done = done0;
+    regroups = regroups0;
+    since = 0;
+    throw;
   }
-  cur = cur0;
-  acc_zero = az0;
-  acc_last = al0;
-  save(false);
+  apply_shapes(best_sh);
+  rewind();
   MPM_CK(cudaStreamSynchronize(st));
-  (void)nr0;
   need_regroup = true;  // the work list belongs to the probes; rebuild it
   substeps_done = done0;
   regroups = regroups0;
   since = 0;
-  sort_interval = best_i;
   invalidate_graphs();
-  return best_i;
+  return best_sh;
 }
 
 // Fixed-order P2G: a regrouping after every gather (so every particle sits in

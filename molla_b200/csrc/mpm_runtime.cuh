@@ -255,7 +255,16 @@ class Group {
   bool use_fused() const {
     return !deterministic && (fused_mode > 0 || (fused_mode < 0 && n_live <= kFusedMaxParticles));
   }
-  int grid_gather32 = 0, grid_gather64 = 0, grid_scatter = 0, grid_fused32 = 0, grid_fused64 = 0;
+  // Persistent grids: SMs x resident CTAs per SM.  occ_* are the occupancy
+  // maxima of each kernel; the tuned counts (0: the maximum) may be lower.
+  int occ_gather32 = 1, occ_gather64 = 1, occ_scatter = 1, occ_fused32 = 1, occ_fused64 = 1;
+  uint32_t gather_per_sm = 0, scatter_per_sm = 0;
+  int gather_grid(bool f64) const;
+  int fused_grid(bool f64) const;
+  int scatter_grid() const;
+  // Particles per work item (a tile with more is cut into several items):
+  // at most kStageMax, the scatter's shared-memory record stage.
+  uint32_t item_chunk = kStageMax;
   uint64_t substeps_done = 0;
   uint64_t epoch = 1;  // bumps on every change that invalidates captured graphs
 
@@ -318,8 +327,10 @@ class Group {
   void grid_pass(int a, uint32_t max_jacobi, bool rigid, cudaStream_t st);
   void jacobi_pass(int a, uint32_t max_jacobi, cudaStream_t st);
   uint32_t max_jacobi_iters() const;
-  // one item per occupied tile, plus one per kStageMax particles of a tile
-  size_t max_item_count() const { return (size_t)key_space + cap / kStageMax + 2; }
+  // one item per occupied tile, plus one per kMinItemParticles particles of
+  // a tile (the smallest item size the tuner may pick)
+  static constexpr uint32_t kMinItemParticles = 128;
+  size_t max_item_count() const { return (size_t)key_space + cap / kMinItemParticles + 2; }
   void sync_scenes(cudaStream_t st);
 
   PoolDev pool() const;
@@ -359,6 +370,28 @@ class Group {
   // fastest interval.  Returns it and fills ms_per_substep (one per
   // candidate, may be null).
   uint32_t autotune(uint32_t probe, const uint32_t* cands, int n_cands, float* ms_per_substep, cudaStream_t st);
+  // The launch and tile shapes an autotuner may pick.
+  struct Shapes {
+    uint32_t interval;        // substeps between regroupings
+    uint32_t item_particles;  // particles per work item (<= kStageMax)
+    uint32_t fused;           // 1: fused gather + scatter for the non-final substeps
+    uint32_t gather_per_sm;   // resident gather CTAs per SM (<= occupancy maximum)
+    uint32_t scatter_per_sm;  // resident scatter CTAs per SM
+  };
+  enum Knob : uint32_t { kKnobInterval = 0, kKnobItem = 1, kKnobFused = 2, kKnobGatherCtas = 3, kKnobScatterCtas = 4 };
+  struct Probe {
+    uint32_t knob, value;
+    float ms;
+  };
+  Shapes shapes() const;
+  void apply_shapes(const Shapes& sh);
+  // Tunes the knobs one after the other, each over its candidates (an empty
+  // list takes the defaults), keeping the fastest value before the next
+  // knob: every candidate times max(probe, 2 x interval) substeps on a
+  // snapshot of the device state, which is restored afterwards (the scenes
+  // do not advance).  Returns the shapes kept; `out` receives every probe.
+  Shapes autotune_shapes(uint32_t probe, const std::vector<std::pair<uint32_t, std::vector<uint32_t>>>& knobs,
+                         std::vector<Probe>* out, cudaStream_t st);
  private:
   void run_substeps(uint32_t substeps, cudaStream_t st);
   GraphKey graph_key(uint32_t substeps) const;

@@ -136,6 +136,13 @@ pub struct mpm_server_stats {
     pub admit_ms: f64, pub step_ms: f64, pub retire_ms: f64, pub ticks: u64,
 }
 #[repr(C)] pub struct mpm_sim64 { _p: [u8; 0] }
+#[repr(C)] #[derive(Clone, Copy, Default)]
+pub struct mpm_shapes {
+    pub sort_interval: u32, pub item_particles: u32, pub fused: u32,
+    pub gather_ctas_per_sm: u32, pub scatter_ctas_per_sm: u32, pub reserved: [u32; 3],
+}
+#[repr(C)] #[derive(Clone, Copy, Default)]
+pub struct mpm_tune_probe { pub knob: u32, pub value: u32, pub ms_per_substep: f32 }
 
 extern "C" {
     // regroup-interval autotune and per-stage timing
@@ -164,6 +171,13 @@ extern "C" {
     pub fn mpm_group_set_deterministic(g: *mut mpm_group, enabled: c_int) -> c_int;
     pub fn mpm_group_scene_count(g: *mut mpm_group, count: *mut u32) -> c_int;
     pub fn mpm_group_tune(g: *mut mpm_group, chunk: u32, sort_interval: u32) -> c_int;
+    // launch and tile shapes: autotuned on a snapshot, or set directly
+    pub fn mpm_group_autotune_shapes(g: *mut mpm_group, probe_substeps: u32, chosen: *mut mpm_shapes,
+                                     probes: *mut mpm_tune_probe, cap: u32, n_probes: *mut u32) -> c_int;
+    pub fn mpm_autotune_shapes(s: *mut mpm_sim, dt: f32, probe_substeps: u32, chosen: *mut mpm_shapes,
+                               probes: *mut mpm_tune_probe, cap: u32, n_probes: *mut u32) -> c_int;
+    pub fn mpm_group_get_shapes(g: *mut mpm_group, out: *mut mpm_shapes) -> c_int;
+    pub fn mpm_group_set_shapes(g: *mut mpm_group, shapes: *const mpm_shapes) -> c_int;
     // admission-controlled serving over one group
     pub fn mpm_server_create(e: *mut mpm_engine, hbm_budget_bytes: u64, max_scenes: u32,
                              out: *mut *mut mpm_server) -> c_int;

@@ -291,3 +291,51 @@ def test_regroup_cadence_independent_of_call_chunking(engine):
     n_mixed, p_mixed = run([5, 3, 17, 1, 30, 8])
     assert n_one == n_many == n_mixed == 8
     assert np.abs(p_one - p_many).max() < TOL and np.abs(p_one - p_mixed).max() < TOL
+
+
+def test_autotune_shapes_keeps_state_and_picks_candidates(engine):
+    """The shapes autotuner (interval, item size, fused or separate kernels,
+    CTAs per SM) leaves the state untouched and keeps values from its
+    candidate sets."""
+    ss = small_scenes()[:3]
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 1024
+    g = m.MpmGroup(engine, 8, total, cells)
+    ids = [g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt) for s in ss]
+    g.step(5)
+    before = [g.read_positions(i) for i in ids]
+    shapes, probes = g.autotune_shapes(probe_substeps=8)
+    assert shapes["sort_interval"] in (8, 16, 32, 64)
+    assert shapes["item_particles"] in (640, 512, 384, 256)
+    assert shapes["fused"] in (0, 1)
+    assert shapes["gather_ctas_per_sm"] >= 1 and shapes["scatter_ctas_per_sm"] >= 1
+    knobs = {k for k, _, _ in probes}
+    assert knobs == {"sort_interval", "item_particles", "fused", "gather_ctas_per_sm", "scatter_ctas_per_sm"}
+    assert all(ms > 0 for _, _, ms in probes)
+    assert g.shapes() == shapes
+    for i, b in zip(ids, before):
+        assert np.array_equal(g.read_positions(i), b)
+        assert g.read_status(i).completed_substeps == 5
+    g.step(5)
+    for k, i in enumerate(ids):
+        assert np.abs(g.read_positions(i) - alone(engine, ss[k], 10)).max() < TOL
+    g.close()
+
+
+@pytest.mark.parametrize("shape", [dict(item_particles=128, fused=1, gather_ctas_per_sm=1),
+                                   dict(item_particles=256, fused=0, scatter_ctas_per_sm=2, sort_interval=3)])
+def test_shapes_do_not_change_results(engine, shape):
+    ss = small_scenes()
+    total = sum(s.n for s in ss)
+    cells = sum(s.grid_size ** 3 for s in ss) + 256 * len(ss)
+    g = m.MpmGroup(engine, 16, total, cells)
+    ids = [g.add_scene(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt) for s in ss]
+    g.set_shapes(**shape)
+    got = g.shapes()
+    for k, v in shape.items():
+        assert got[k] == v, (k, got)
+    g.step(12)
+    g.step_graph(6, 2)
+    for sid, s in zip(ids, ss):
+        assert np.abs(g.read_positions(sid) - alone(engine, s, 24)).max() < TOL
+    g.close()
