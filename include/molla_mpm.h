@@ -130,8 +130,9 @@ typedef enum mpm_preset {
 typedef struct mpm_status_info {
   uint32_t numerical_fault;   /* latched non-finite state (mpm.wgsl:217-231) */
   uint32_t completed_substeps;/* gathers run since the last fault reset (mpm.wgsl:1246) */
-  uint32_t fault_bits;        /* raw latch word */
-  uint32_t reserved;
+  uint32_t fault_bits;        /* raw latch word: 2 numerical fault, 4 a deposit left the fixed
+                                 order, 8 a bounded device wait gave up, 16 sparse tile overflow */
+  uint32_t active_tiles;      /* sparse grid storage: tiles of the current map (0 when dense) */
 } mpm_status_info;
 
 /* Opaque handles. */
@@ -172,6 +173,16 @@ MPM_API float mpm_dp_alpha(float friction_angle);
 
 /* MpmSimulation::new (mpm.rs:834-843, validation :855-900). */
 MPM_API int mpm_sim_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim** out);
+/* MpmSimulation::new_sparse (mpm.rs:846-853): grid storage for
+ * `tile_capacity` tiles of 4^3 nodes instead of grid_size^3 nodes
+ * (1 <= tile_capacity <= ceil(grid_size / 4)^3).  Every substep the tiles the
+ * particles' stencils touch get slots; more than tile_capacity of them latch
+ * the tile-overflow bit (16) in the status word, and the scene freezes as on
+ * a numerical fault (MpmActiveGridStats::overflow, mpm.rs:257-283).  Results
+ * equal the dense storage's.  Explicit time step only; rigid spheres are not
+ * coupled to sparse storage (MPM_ERR_UNSUPPORTED). */
+MPM_API int mpm_sim_create_sparse(mpm_engine* engine, const mpm_config* cfg, uint32_t tile_capacity,
+                                  mpm_sim** out);
 MPM_API int mpm_sim_destroy(mpm_sim* sim);
 
 /* set_particles / set_particles_with_velocity (mpm.rs:1451-1519):
@@ -391,6 +402,12 @@ MPM_API int mpm_group_destroy(mpm_group* group);
  * row per scene plus per-particle material ids (NULL: row 0). */
 MPM_API int mpm_group_add_scene(mpm_group* group, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
                         const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t* scene_id);
+/* mpm_group_add_scene with sparse grid storage of `tile_capacity` tiles
+ * (see mpm_sim_create_sparse); the scene's grid range holds 64 x
+ * tile_capacity nodes. */
+MPM_API int mpm_group_add_scene_sparse(mpm_group* group, const mpm_config* cfg, const mpm_rheology* rows,
+                                       uint32_t n_rows, const float* xyz, const uint32_t* ids_or_null, uint32_t n,
+                                       float dt, uint32_t tile_capacity, uint32_t* scene_id);
 MPM_API int mpm_group_remove_scene(mpm_group* group, uint32_t scene_id);
 /* Advances every scene in the group by `substeps` substeps at its own dt. */
 MPM_API int mpm_group_step(mpm_group* group, uint32_t substeps);

@@ -215,14 +215,21 @@ class MpmConfig:
 
 @dataclass
 class MpmActiveGridStats:
-    """MpmActiveGridStats (mpm.rs:257-283)."""
+    """MpmActiveGridStats (mpm.rs:257-283).  active_tiles / overflow concern
+    sparse grid storage (MpmSimulation.new_sparse)."""
 
     numerical_fault: bool
     completed_substeps: int
     fault_bits: int
+    active_tiles: int = 0
+    tile_capacity: int = 0
+
+    @property
+    def overflow(self) -> bool:
+        return bool(self.fault_bits & 16)
 
     def faulted(self) -> bool:
-        return self.numerical_fault
+        return self.numerical_fault or self.overflow
 
 
 class Engine:
@@ -392,18 +399,30 @@ class MpmParticleRenderView:
 class MpmSimulation:
     """MpmSimulation (crates/molla-solvers/src/mpm.rs:695-2957) on the B200 path."""
 
-    def __init__(self, engine: Engine, cfg: MpmConfig):
+    def __init__(self, engine: Engine, cfg: MpmConfig, tile_capacity: int | None = None):
+        """tile_capacity: None for the dense grid, else sparse storage of that
+        many 4^3-node tiles (MpmSimulation::new_sparse)."""
         self.engine = engine
         self.cfg = cfg
+        self.tile_capacity = int(tile_capacity or 0)
         h = C.c_void_p()
         c = cfg.to_c()
-        _check(_ffi.lib().mpm_sim_create(engine._h, C.byref(c), C.byref(h)))
+        if tile_capacity is not None:
+            _check(_ffi.lib().mpm_sim_create_sparse(engine._h, C.byref(c), int(tile_capacity), C.byref(h)))
+        else:
+            _check(_ffi.lib().mpm_sim_create(engine._h, C.byref(c), C.byref(h)))
         self._h = h
         self.particle_count = 0
 
     @classmethod
     def new(cls, engine: Engine, cfg: MpmConfig) -> "MpmSimulation":
         return cls(engine, cfg)
+
+    @classmethod
+    def new_sparse(cls, engine: Engine, cfg: MpmConfig, tile_capacity: int) -> "MpmSimulation":
+        """MpmSimulation::new_sparse (mpm.rs:846-853): grid storage for
+        tile_capacity tiles of 4^3 nodes."""
+        return cls(engine, cfg, tile_capacity)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -617,7 +636,8 @@ class MpmSimulation:
     def read_active_grid_status(self) -> MpmActiveGridStats:
         s = _ffi.mpm_status_info()
         _check(_ffi.lib().mpm_read_status(self._h, C.byref(s)))
-        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
+        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits),
+                                  int(s.active_tiles), getattr(self, 'tile_capacity', 0))
 
     read_active_grid_status_with = read_active_grid_status
 
@@ -737,7 +757,8 @@ class MpmSimulation64:
     def read_active_grid_status(self) -> MpmActiveGridStats:
         s = _ffi.mpm_status_info()
         _check(_ffi.lib().mpm_sim64_read_status(self._h, C.byref(s)))
-        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
+        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits),
+                                  int(s.active_tiles), getattr(self, 'tile_capacity', 0))
 
 
 TUNE_KNOBS = ("sort_interval", "item_particles", "fused", "gather_ctas_per_sm", "scatter_ctas_per_sm")
@@ -768,14 +789,19 @@ class MpmGroup:
         self._h = h
         self.counts = {}
 
-    def add_scene(self, cfg: MpmConfig, rows, positions, ids=None, dt: float = 1e-4) -> int:
+    def add_scene(self, cfg: MpmConfig, rows, positions, ids=None, dt: float = 1e-4, tile_capacity: int = 0) -> int:
+        """tile_capacity > 0: sparse grid storage of that many 4^3-node tiles."""
         c = cfg.to_c()
         r = _rows_c(rows)
         pos = _f32(positions, 3)
         idv = None if ids is None else np.ascontiguousarray(np.asarray(ids, np.uint32))
         sid = C.c_uint32()
-        _check(_ffi.lib().mpm_group_add_scene(self._h, C.byref(c), r, len(rows), _fp(pos), _up(idv), pos.shape[0],
-                                              dt, C.byref(sid)))
+        if tile_capacity:
+            _check(_ffi.lib().mpm_group_add_scene_sparse(self._h, C.byref(c), r, len(rows), _fp(pos), _up(idv),
+                                                         pos.shape[0], dt, int(tile_capacity), C.byref(sid)))
+        else:
+            _check(_ffi.lib().mpm_group_add_scene(self._h, C.byref(c), r, len(rows), _fp(pos), _up(idv),
+                                                  pos.shape[0], dt, C.byref(sid)))
         self.counts[sid.value] = pos.shape[0]
         return sid.value
 
@@ -835,7 +861,8 @@ class MpmGroup:
     def read_status(self, sid: int) -> MpmActiveGridStats:
         s = _ffi.mpm_status_info()
         _check(_ffi.lib().mpm_group_read_status(self._h, sid, C.byref(s)))
-        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
+        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits),
+                                  int(s.active_tiles), getattr(self, 'tile_capacity', 0))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -67,7 +67,7 @@ class mpm_status_info(C.Structure):
         ("numerical_fault", C.c_uint32),
         ("completed_substeps", C.c_uint32),
         ("fault_bits", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("active_tiles", C.c_uint32),
     ]
 
 
@@ -155,6 +155,7 @@ SIGNATURES = {
     "mpm_config_preset": (I, [U32, C.POINTER(mpm_config)]),
     "mpm_dp_alpha": (C.c_float, [C.c_float]),
     "mpm_sim_create": (I, [P, C.POINTER(mpm_config), PP]),
+    "mpm_sim_create_sparse": (I, [P, C.POINTER(mpm_config), U32, PP]),
     "mpm_sim_destroy": (I, [P]),
     "mpm_set_particles": (I, [P, F32P, F32P, U32]),
     "mpm_set_particle_mass_volume": (I, [P, F32P, F32P, U32]),
@@ -198,6 +199,8 @@ SIGNATURES = {
     "mpm_group_destroy": (I, [P]),
     "mpm_group_add_scene": (I, [P, C.POINTER(mpm_config), C.POINTER(mpm_rheology), U32, F32P, U32P, U32,
                                 C.c_float, U32P]),
+    "mpm_group_add_scene_sparse": (I, [P, C.POINTER(mpm_config), C.POINTER(mpm_rheology), U32, F32P, U32P, U32,
+                                       C.c_float, U32, U32P]),
     "mpm_group_remove_scene": (I, [P, U32]),
     "mpm_group_step": (I, [P, U32]),
     "mpm_group_step_graph": (I, [P, U32, U32]),

@@ -103,6 +103,7 @@ struct mpm_sim {
   uint64_t render_source = 0;  // binding identity of `render`
   uint64_t epoch = 1;
   float dt = 1.0e-4f;
+  uint32_t tile_cap = 0;  // new_sparse: grid storage of this many 4^3-node tiles (0: dense)
 
   std::vector<mpm_rheology> effective_rows() const {
     if (!rows.empty()) return rows;
@@ -378,6 +379,38 @@ int mpm_config_preset(uint32_t preset, mpm_config* out) {
 
 // ---- simulation ---------------------------------------------------------------
 
+static mpm_sim* sim_new(mpm_engine* engine, const mpm_config* cfg, uint32_t tile_cap) {
+  REQUIRE(engine && cfg, MPM_ERR_INVALID, "null argument");
+  engine->e->check();
+  validate_config(*cfg);
+  const uint64_t w = (cfg->grid_size + 3u) / 4u;
+  REQUIRE(tile_cap <= w * w * w, MPM_ERR_INVALID, "MPM tile pool capacity is invalid");
+  REQUIRE(!tile_cap || cfg->time_step != MPM_TIME_STEP_IMPLICIT, MPM_ERR_UNSUPPORTED,
+          "sparse MPM grid storage runs the explicit time step only");
+  auto* s = new mpm_sim();
+  try {
+    s->hold = engine->e;
+    s->eng = engine->e.get();
+    s->cfg = *cfg;
+    s->tile_cap = tile_cap;
+    const uint64_t cells = tile_cap ? 64ull * tile_cap : (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
+    s->group.reset(new mpm::Group(s->eng, 1, std::max<uint32_t>(cfg->max_particles, 1), cells));
+    s->apply_group_settings();
+  } catch (...) {
+    delete s;
+    throw;
+  }
+  return s;
+}
+
+int mpm_sim_create_sparse(mpm_engine* engine, const mpm_config* cfg, uint32_t tile_capacity, mpm_sim** out) {
+  return guard([&] {
+    REQUIRE(out, MPM_ERR_INVALID, "null argument");
+    REQUIRE(tile_capacity > 0, MPM_ERR_INVALID, "MPM tile pool capacity is invalid");
+    *out = sim_new(engine, cfg, tile_capacity);
+  });
+}
+
 int mpm_sim_create(mpm_engine* engine, const mpm_config* cfg, mpm_sim** out) {
   return guard([&] {
     REQUIRE(engine && cfg && out, MPM_ERR_INVALID, "null argument");
@@ -421,7 +454,7 @@ static void sim_reseed(mpm_sim* s, const float* xyz, const float* vel, uint32_t 
   }
   const float* mass = s->mass.size() == n && n ? s->mass.data() : nullptr;
   const float* vol = s->volume.size() == n && n ? s->volume.data() : nullptr;
-  s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, ids, n, s->dt);
+  s->sid = s->group->add_scene(s->cfg, s->effective_rows(), xyz, vel, mass, vol, ids, n, s->dt, s->tile_cap);
   s->count = n;
   s->apply_group_settings();
   if (!s->spheres.empty())
@@ -977,6 +1010,24 @@ int mpm_group_add_scene(mpm_group* group, const mpm_config* cfg, const mpm_rheol
   });
 }
 
+int mpm_group_add_scene_sparse(mpm_group* group, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
+                               const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt,
+                               uint32_t tile_capacity, uint32_t* scene_id) {
+  return guard([&] {
+    REQUIRE(group && cfg && scene_id, MPM_ERR_INVALID, "null argument");
+    REQUIRE(n == 0 || xyz, MPM_ERR_INVALID, "null positions");
+    REQUIRE(tile_capacity > 0, MPM_ERR_INVALID, "MPM tile pool capacity is invalid");
+    validate_config(*cfg);
+    REQUIRE(std::isfinite(dt) && dt > 0.f, MPM_ERR_INVALID, "MPM timestep must be finite and positive");
+    auto r = rows_of(*cfg, rows, n_rows);
+    REQUIRE(r.size() <= 8, MPM_ERR_INVALID, "MPM scene needs 1..=8 material rows");
+    if (ids_or_null)
+      for (uint32_t i = 0; i < n; ++i)
+        REQUIRE(ids_or_null[i] < r.size(), MPM_ERR_INVALID, "particle material id out of range");
+    *scene_id = group->g->add_scene(*cfg, r, xyz, nullptr, nullptr, nullptr, ids_or_null, n, dt, tile_capacity);
+  });
+}
+
 int mpm_group_remove_scene(mpm_group* group, uint32_t scene_id) {
   return guard([&] {
     REQUIRE(group, MPM_ERR_INVALID, "null group");
@@ -1164,9 +1215,38 @@ struct Ticket {
   uint32_t state = 0;  // 0 queued, 1 running, 2 done
   uint32_t sid = 0xffffffffu;
   uint64_t bytes = 0;
+  uint32_t tile_cap = 0;  // sparse grid storage when it saves memory (0: dense)
   std::vector<float> result;
   double t_submit = 0, t_admit = 0;
 };
+
+// Tile capacity for a served scene: the 4^3-node tiles of the particles'
+// stencil bounding box, widened by 2 tiles (8 cells) on every side for the
+// motion of the scene's lifetime and clamped to the grid; 0 (dense storage)
+// when that is more than half the grid's tiles.  A scene that spreads beyond
+// it latches the tile-overflow bit and stops.
+uint32_t served_tile_capacity(const mpm_config& cfg, const float* xyz, uint32_t n) {
+  const uint32_t w = (cfg.grid_size + 3u) / 4u;
+  const uint64_t all = (uint64_t)w * w * w;
+  if (n == 0) return 0;
+  int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+  const float inv_dx = 1.0f / cfg.cell_size;
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      const float xp = (xyz[3 * (size_t)i + a] - cfg.grid_origin[a]) * inv_dx;
+      if (!std::isfinite(xp)) return 0;
+      const int b = (int)std::floor(xp - 0.5f) - cfg.grid_window_cells[a];
+      lo[a] = std::min(lo[a], b);
+      hi[a] = std::max(hi[a], b + 2);
+    }
+  uint64_t tiles = 1;
+  for (int a = 0; a < 3; ++a) {
+    const int t0 = std::max(0, (std::max(lo[a], 0) >> 2) - 2);
+    const int t1 = std::min((int)w - 1, (std::min(hi[a], (int)cfg.grid_size - 1) >> 2) + 2);
+    tiles *= (uint64_t)std::max(t1 - t0 + 1, 1);
+  }
+  return 2 * tiles <= all ? (uint32_t)tiles : 0u;
+}
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -1250,8 +1330,14 @@ int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheol
     t.n = n;
     t.dt = dt;
     t.steps = t.remaining = steps;
-    const uint64_t n3 = (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
-    t.bytes = (uint64_t)n * kServerBytesPerParticle + (n3 + 255) / 256 * 256 * 48ull;
+    // sparse grid storage when the particles occupy a small part of the grid
+    // and the configuration allows it (explicit time step)
+    t.tile_cap = cfg->time_step == MPM_TIME_STEP_IMPLICIT ? 0u : served_tile_capacity(*cfg, xyz, n);
+    const uint64_t wt = (cfg->grid_size + 3u) / 4u;
+    const uint64_t n3 = t.tile_cap ? 64ull * t.tile_cap : (uint64_t)cfg->grid_size * cfg->grid_size * cfg->grid_size;
+    // particles, grid nodes (two accumulators and the velocity), and with
+    // sparse storage the per-tile map and marks
+    t.bytes = (uint64_t)n * kServerBytesPerParticle + (n3 + 255) / 256 * 256 * 48ull + (t.tile_cap ? wt * wt * wt * 5 : 0);
     REQUIRE(n <= server->g->cap && (n3 + 255) / 256 * 256 <= server->g->cell_cap && t.bytes <= server->budget,
             MPM_ERR_INVALID, "scene exceeds the server's HBM budget or pools");
     t.t_submit = now_ms();
@@ -1288,7 +1374,7 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         for (int attempt = 0; attempt < 2 && !added; ++attempt) {
           try {
             sid = g.add_scene(t.cfg, t.rows, t.xyz.data(), nullptr, nullptr, nullptr,
-                              t.ids.empty() ? nullptr : t.ids.data(), t.n, t.dt);
+                              t.ids.empty() ? nullptr : t.ids.data(), t.n, t.dt, t.tile_cap);
             added = true;
           } catch (const Error& e) {
             if (e.code != MPM_ERR_BUSY) throw;
@@ -1669,7 +1755,7 @@ int mpm_sim64_read_status(mpm_sim64* sim, mpm_status_info* out) {
     out->numerical_fault = (w[0] & 2u) ? 1u : 0u;
     out->completed_substeps = w[1];
     out->fault_bits = w[0];
-    out->reserved = 0;
+    out->active_tiles = 0;
   });
 }
 

@@ -37,6 +37,10 @@ constexpr uint32_t kFaultNumerical = 2u;  // mpm.wgsl:229 numerical_fault()
 // substeps: the grid update counts one past the budget and stops counting,
 // and the particle kernels skip a scene whose count is past its budget.
 constexpr uint32_t kStatusWords = 4u;
+// Status word 3 of a sparse scene counts its active tiles (the slots of the
+// current map).
+constexpr uint32_t kFaultTileOverflow = 16u;  // more active tiles than the sparse scene's capacity
+constexpr uint32_t kNoSlot = 0xffffffffu;
 constexpr int kMaxMaterials = 8;          // MAX_MPM_MATERIALS, mpm.rs:660
 
 // Work items cover the particles regrouped under one 4^3 tile of base cells
@@ -85,6 +89,14 @@ struct SceneDev {
   float youngs;           // the configuration's Young's modulus (implicit stiffness estimate)
   uint32_t n_rigid;       // rigid spheres of this scene (slots scene * kMaxRigid ...)
   uint32_t svd64;         // 1: the mixed-precision (FP64) SVD and principal-frame stress, 0: the FP32 reference form
+  // Sparse grid storage (MpmSimulation::new_sparse, mpm.rs:846-853): 0 keeps
+  // the dense n^3 grid; otherwise the scene's grid range holds tile_cap
+  // 4^3-node tiles, and the tile map (tile_slot, by tile key) gives each
+  // active tile its slot.  The map is rebuilt every substep from the tiles
+  // the particles' stencils touch; more active tiles than tile_cap latch
+  // kFaultTileOverflow.
+  uint32_t tile_cap;
+  uint32_t pad_sparse;
   MatDev mat[kMaxMaterials];
 };
 
@@ -127,6 +139,12 @@ struct PoolDev {
   const uint32_t* n_items;
   uint32_t item_top;
   const uint8_t* item_order;  // per item: its tile's 64 cells by descending count at the regrouping
+  // Sparse grid storage: slot of every tile key (kNoSlot: none), the tile
+  // (scene-local index) of every slot of the grid pool (indexed by grid pool
+  // cell / 64), and the tiles marked by this substep's gather.
+  uint32_t* tile_slot;
+  uint32_t* slot_tile;
+  uint8_t* tile_mark;
 };
 
 __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }
@@ -135,6 +153,44 @@ __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.plan
 // items first, then the FP64-SVD items.
 __device__ __forceinline__ uint32_t item_slot(const PoolDev& p, uint32_t n32, uint32_t i) {
   return i < n32 ? i : p.item_top - 1u - (i - n32);
+}
+
+// Grid pool index of node (ix, iy, iz) of a scene (scene-local lattice
+// coordinates), or -1 when the node lies outside the grid or, in a sparse
+// scene, in a tile without a slot.  Dense: row-major x-fastest n^3 block;
+// sparse: 64 nodes per tile slot, x-fastest inside the 4^3 tile.
+__device__ __forceinline__ int64_t node_index(const SceneDev& sc, const uint32_t* __restrict__ tile_slot, int ix,
+                                              int iy, int iz) {
+  const int n = (int)sc.n;
+  if ((unsigned)ix >= (unsigned)n || (unsigned)iy >= (unsigned)n || (unsigned)iz >= (unsigned)n) return -1;
+  if (!sc.tile_cap)
+    return (int64_t)(sc.grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz));
+  const uint32_t t = (uint32_t)(ix >> 2) + sc.w * ((uint32_t)(iy >> 2) + sc.w * (uint32_t)(iz >> 2));
+  const uint32_t slot = tile_slot[sc.key_off + t];
+  if (slot == kNoSlot) return -1;
+  return (int64_t)(sc.grid_off + 64ull * slot + (uint64_t)((ix & 3) + 4 * (iy & 3) + 16 * (iz & 3)));
+}
+
+// Marks the tiles of the 3^3 stencil of a particle with base node (bx, by,
+// bz) in a sparse scene (1 or 2 tiles per axis).
+__device__ __forceinline__ void mark_stencil_tiles(const SceneDev& sc, uint8_t* __restrict__ tile_mark, int bx, int by,
+                                                   int bz) {
+  const int n = (int)sc.n;
+  int lo[3], hi[3];
+  const int b[3] = {bx, by, bz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int l = max(b[a], 0), h = min(b[a] + 2, n - 1);
+    if (l > h) return;  // the stencil misses the grid on this axis
+    lo[a] = l >> 2;
+    hi[a] = h >> 2;
+  }
+  for (int tz = lo[2]; tz <= hi[2]; ++tz)
+    for (int ty = lo[1]; ty <= hi[1]; ++ty)
+      for (int tx = lo[0]; tx <= hi[0]; ++tx) {
+        uint8_t* m = tile_mark + sc.key_off + (uint32_t)tx + sc.w * ((uint32_t)ty + sc.w * (uint32_t)tz);
+        if (*m == 0) *m = 1;
+      }
 }
 
 // Whether a scene's particles stand still this substep: a latched fault, or

@@ -56,8 +56,20 @@ __device__ __forceinline__ void grid_node(const PoolDev& p, uint32_t sid, const 
                                           uint64_t g, float4 a, bool in_a, bool rb, int acc_in) {
   const uint32_t n = sc.n;
   const uint32_t local = (uint32_t)(g - sc.grid_off);  // grids hold fewer than 2^32 cells
-  const uint32_t q = local / n;
-  const int ix = (int)(local - q * n), iy = (int)(q % n), iz = (int)(q / n);
+  int ix, iy, iz;
+  if (sc.tile_cap) {
+    // sparse storage: node (local & 63) of the tile in slot local / 64
+    const uint32_t tile = p.slot_tile[g >> 6];
+    const uint32_t tx = tile % sc.w, ty = (tile / sc.w) % sc.w, tz = tile / (sc.w * sc.w);
+    ix = 4 * (int)tx + (int)(local & 3u);
+    iy = 4 * (int)ty + (int)((local >> 2) & 3u);
+    iz = 4 * (int)tz + (int)((local >> 4) & 3u);
+  } else {
+    const uint32_t q = local / n;
+    ix = (int)(local - q * n);
+    iy = (int)(q % n);
+    iz = (int)(q / n);
+  }
   bool rigid = false;
   if (rb && sc.n_rigid) {
     const float node[3] = {sc.ox + (float)(ix + sc.winx) * sc.dx, sc.oy + (float)(iy + sc.winy) * sc.dx,
@@ -149,7 +161,11 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_grid_update(PoolDev p, cons
       if (status[0] == 0u && (status[2] == 0u || status[1] <= status[2]))
         atomicAdd(const_cast<uint32_t*>(status) + 1, 1u);
     }
-    conv[b] = (in_a[b] || rb[b]) && local64 < (uint64_t)sc.n * sc.n * sc.n;
+    // dense: the n^3 block; sparse: the slots of the current tile map
+    const uint64_t extent =
+        sc.tile_cap ? 64ull * min(*((volatile uint32_t*)p.status + (size_t)sc.status * kStatusWords + 3), sc.tile_cap)
+                    : (uint64_t)sc.n * sc.n * sc.n;
+    conv[b] = (in_a[b] || rb[b]) && local64 < extent;
     if (conv[b]) acc_v[b] = p.acc[acc_in][g];
   }
   __syncthreads();  // every thread has read the marks
@@ -669,6 +685,50 @@ cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live
   if (K > 0)
     k_items<<<(K + 255) / 256, 256, 0, st>>>(tile_start, K, key_scene, scenes, chunk, item_top, items, n_items,
                                              tile_item);
+  return cudaGetLastError();
+}
+
+// Sparse tile maps (the reference marks the active tiles and builds its
+// hashed map every step, crates/molla-solvers/src/mpm_active_tiles.rs:242-302):
+// the active-tile counters of the sparse scenes start at zero ...
+__global__ void k_tiles_reset(PoolDev p, uint32_t n_scenes) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_scenes; s += gridDim.x * blockDim.x) {
+    const SceneDev& sc = p.scenes[s];
+    if (sc.live && sc.tile_cap) p.status[(size_t)sc.status * kStatusWords + 3] = 0u;
+  }
+}
+
+// ... then every tile the gather marked gets a slot (slot order is
+// immaterial: each tile owns its 64 nodes), every other tile none, and the
+// marks are cleared.  More active tiles than the capacity latch
+// kFaultTileOverflow; the excess tiles get no slot (their deposits are
+// dropped and the scene freezes from the next substep).
+__global__ void k_tiles_finalize(PoolDev p, const uint32_t* __restrict__ key_scene, uint32_t K) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= K) return;
+  const uint32_t sid = key_scene[t];
+  if (sid == 0xffffffffu) return;
+  const SceneDev& sc = p.scenes[sid];
+  if (!sc.tile_cap || !sc.live) return;
+  uint32_t slot = kNoSlot;
+  if (p.tile_mark[t]) {
+    p.tile_mark[t] = 0;
+    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
+    const uint32_t s = atomicAdd(status + 3, 1u);
+    if (s < sc.tile_cap) {
+      slot = s;
+      p.slot_tile[(sc.grid_off >> 6) + s] = t - sc.key_off;
+    } else {
+      atomicOr(status, kFaultTileOverflow);
+    }
+  }
+  p.tile_slot[t] = slot;
+}
+
+cudaError_t launch_tiles_finalize(const PoolDev& p, const uint32_t* key_scene, uint32_t K, uint32_t n_scenes,
+                                  cudaStream_t st) {
+  k_tiles_reset<<<(n_scenes + 255) / 256, 256, 0, st>>>(p, n_scenes);
+  if (K) k_tiles_finalize<<<(K + 255) / 256, 256, 0, st>>>(p, key_scene, K);
   return cudaGetLastError();
 }
 

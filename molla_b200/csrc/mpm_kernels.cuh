@@ -79,6 +79,10 @@ cudaError_t launch_vel_copy(const uint8_t* touched, const uint32_t* block_scene,
 cudaError_t launch_items(const uint32_t* sorted_keys, int shift, uint32_t n_live, uint32_t K, uint32_t* tile_start,
                          const uint32_t* key_scene, const SceneDev* scenes, uint32_t chunk, uint32_t item_top,
                          Item* items, uint32_t* n_items, uint32_t* tile_item, cudaStream_t st);
+// Rebuilds the tile maps of the sparse scenes from the tiles the last gather
+// marked (two launches).
+cudaError_t launch_tiles_finalize(const PoolDev& p, const uint32_t* key_scene, uint32_t K, uint32_t n_scenes,
+                                  cudaStream_t st);
 // p[0, n) = v, stream-ordered.
 cudaError_t launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st);
 cudaError_t launch_pack_positions(const PoolDev& p, const uint32_t* slot_of, uint32_t id_base, uint32_t n,

@@ -66,10 +66,12 @@ __device__ __forceinline__ uint32_t base_key(const SceneDev& sc, const int* base
 // unrolled shared-memory path stays small; it takes scalars and writes
 // v (3) and G = sum w gv d^T (9) to the caller's shared-memory slot, so the
 // call needs no local memory.
-__device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int n, float xp0, float xp1, float xp2,
-                                           int wx, int wy, int wz, float dx, float* out) {
+__device__ __noinline__ void gather_global(const float4* __restrict__ vel_pool, const SceneDev& sc,
+                                           const uint32_t* __restrict__ tile_slot, float xp0, float xp1, float xp2,
+                                           float* out) {
   const float xp[3] = {xp0, xp1, xp2};
-  const int win[3] = {wx, wy, wz};
+  const int win[3] = {sc.winx, sc.winy, sc.winz};
+  const float dx = sc.dx;
   float w[3][3], d[3][3];
   int base[3];
   for (int a = 0; a < 3; ++a) {
@@ -83,9 +85,9 @@ __device__ __noinline__ void gather_global(const float4* __restrict__ gvel, int 
   for (int i = 0; i < 12; ++i) acc[i] = 0.f;
   for (int q = 0; q < 27; ++q) {
     const int i = q / 9, j = (q / 3) % 3, k = q % 3;
-    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
-    if ((unsigned)ix >= (unsigned)n || (unsigned)iy >= (unsigned)n || (unsigned)iz >= (unsigned)n) continue;
-    const float4 g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+    const int64_t c = node_index(sc, tile_slot, base[0] + i, base[1] + j, base[2] + k);
+    if (c < 0) continue;
+    const float4 g = __ldg(&vel_pool[c]);
     const float wt = w[0][i] * w[1][j] * w[2][k];
     const float gv[3] = {wt * g.x, wt * g.y, wt * g.z};
     for (int r = 0; r < 3; ++r) {
@@ -243,7 +245,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         }
       } else {
         float* slot = fallback;
-        gather_global(p.vel + sc.grid_off, n, xp[0], xp[1], xp[2], win[0], win[1], win[2], sc.dx, slot);
+        gather_global(p.vel, sc, p.tile_slot, xp[0], xp[1], xp[2], slot);
 #pragma unroll
         for (int r = 0; r < 3; ++r) vs[r] = slot[r];
 #pragma unroll
@@ -408,6 +410,14 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
     rec[2] = make_float4(B[1], B[2], B[3], B[4]);
     rec[3] = make_float4(B[5], B[6], B[7], B[8]);
   }
+  if constexpr (kScatter) {
+    // sparse storage: the tiles this record's deposit will touch
+    if (sc.tile_cap && ok) {
+      const float xq[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
+      mark_stencil_tiles(sc, p.tile_mark, (int)floorf(xq[0] - 0.5f) - sc.winx, (int)floorf(xq[1] - 0.5f) - sc.winy,
+                         (int)floorf(xq[2] - 0.5f) - sc.winz);
+    }
+  }
   if constexpr (WRITE_KEYS) {
     const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
     const int win[3] = {sc.winx, sc.winy, sc.winz};
@@ -452,12 +462,10 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
     const int n = (int)scp->n;
     if constexpr (kGather) {
       // Stage the 8^3-node velocity block (out-of-grid nodes read as zero).
-      const float4* __restrict__ gvel = p.vel + scp->grid_off;
       for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-        const int ix = rx + (r & 7), iy = ry + ((r >> 3) & 7), iz = rz + (r >> 6);
+        const int64_t c = node_index(*scp, p.tile_slot, rx + (r & 7), ry + ((r >> 3) & 7), rz + (r >> 6));
         float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-        if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n)
-          g = __ldg(&gvel[(size_t)ix + (size_t)n * ((size_t)iy + (size_t)n * (size_t)iz)]);
+        if (c >= 0) g = __ldg(&p.vel[c]);
         s_gath.vel[r] = g;
       }
     }
@@ -517,9 +525,11 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol
 // up sets kFaultDeviceWait in the scene's status word and ends the CTA after
 // a second bounded wait for its copy in flight.
 __device__ __noinline__ void deposit_global(float4 r0, float4 r1, float4 r2, float4 r3, float4* __restrict__ acc,
-                                            uint8_t* __restrict__ touched, uint64_t grid_off, int n, float ox,
-                                            float oy, float oz, float inv_dx, float dx, int wx, int wy, int wz) {
-  const int win[3] = {wx, wy, wz};
+                                            uint8_t* __restrict__ touched, const SceneDev* __restrict__ scp,
+                                            const uint32_t* __restrict__ tile_slot) {
+  const SceneDev& sc = *scp;
+  const int win[3] = {sc.winx, sc.winy, sc.winz};
+  const float ox = sc.ox, oy = sc.oy, oz = sc.oz, inv_dx = sc.inv_dx, dx = sc.dx;
   const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
   const float xp[3] = {(r0.x - ox) * inv_dx, (r0.y - oy) * inv_dx, (r0.z - oz) * inv_dx};
   float wgt[3][3], fx[3];
@@ -532,14 +542,13 @@ __device__ __noinline__ void deposit_global(float4 r0, float4 r1, float4 r2, flo
   }
   for (int q = 0; q < 27; ++q) {
     const int i = q / 9, j = (q / 3) % 3, k = q % 3;
-    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
-    if ((unsigned)ix >= (unsigned)n || (unsigned)iy >= (unsigned)n || (unsigned)iz >= (unsigned)n) continue;
+    const int64_t c = node_index(sc, tile_slot, base[0] + i, base[1] + j, base[2] + k);
+    if (c < 0) continue;
     const float wt = wgt[0][i] * wgt[1][j] * wgt[2][k];
     const float d0 = ((float)i - fx[0]) * dx, d1 = ((float)j - fx[1]) * dx, d2 = ((float)k - fx[2]) * dx;
     const float4 v = make_float4(wt * r0.w, wt * (r1.x + B[0] * d0 + B[3] * d1 + B[6] * d2),
                                  wt * (r1.y + B[1] * d0 + B[4] * d1 + B[7] * d2),
                                  wt * (r1.z + B[2] * d0 + B[5] * d1 + B[8] * d2));
-    const uint64_t c = grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
     atomicAdd(&acc[c], v);
     touch(touched, c);
   }
@@ -564,10 +573,15 @@ struct ItemFrame {
   uint64_t grid_off;
   float4* acc;
   uint8_t* touched;
+  const SceneDev* sc;         // the scene record (global memory)
+  const uint32_t* tile_slot;  // sparse storage: slot of every tile key
 };
 
-__device__ __forceinline__ ItemFrame item_frame(const SceneDev& sc, const Item& item, float4* acc, uint8_t* touched) {
+__device__ __forceinline__ ItemFrame item_frame(const SceneDev& sc, const Item& item, float4* acc, uint8_t* touched,
+                                                const uint32_t* tile_slot) {
   ItemFrame f;
+  f.sc = &sc;
+  f.tile_slot = tile_slot;
   f.ox = sc.ox;
   f.oy = sc.oy;
   f.oz = sc.oz;
@@ -627,7 +641,7 @@ __device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bo
           lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
         } else {
           deposit_global(r0, stage_chunk(stage, j, 1), stage_chunk(stage, j, 2), stage_chunk(stage, j, 3), f.acc,
-                         f.touched, f.grid_off, f.n, f.ox, f.oy, f.oz, f.inv_dx, f.dx, f.wx, f.wy, f.wz);
+                         f.touched, f.sc, f.tile_slot);
         }
       }
     }
@@ -804,12 +818,10 @@ __device__ __forceinline__ void flush_item(const ItemFrame& f, ScatterShared& ss
       ss.acc[1][q] = 0.f;
       ss.acc[2][q] = 0.f;
       ss.acc[3][q] = 0.f;
-      const int ix = f.rx + lx, iy = f.ry + ly, iz = f.rz + lz;
-      if ((unsigned)ix < (unsigned)f.n && (unsigned)iy < (unsigned)f.n && (unsigned)iz < (unsigned)f.n) {
-        const uint64_t c =
-            f.grid_off + (uint64_t)ix + (uint64_t)f.n * ((uint64_t)iy + (uint64_t)f.n * (uint64_t)iz);
+      const int64_t c = node_index(*f.sc, f.tile_slot, f.rx + lx, f.ry + ly, f.rz + lz);
+      if (c >= 0) {
         atomicAdd(&f.acc[c], make_float4(m, px, py, pz));
-        touch(f.touched, c);
+        touch(f.touched, (uint64_t)c);
       }
     }
   }
@@ -864,7 +876,7 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
     // retired scene) freezes the scene; one latched by this substep's gather
     // is handled per particle (m = 0 in its record).
     const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
-    const ItemFrame f = item_frame(*scp, item, acc, touched);
+    const ItemFrame f = item_frame(*scp, item, acc, touched, p.tile_slot);
     const bool staged = item.count - 1u < (uint32_t)kStageMax;
     bool ok = staged;
     if (staged) {
@@ -929,17 +941,13 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
     const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
     const bool publish_vc = budget_ends(status);
-    const ItemFrame f = item_frame(*scp, item, acc, touched);
+    const ItemFrame f = item_frame(*scp, item, acc, touched, p.tile_slot);
     const bool fits = item.count <= (uint32_t)kStageMax;
     {
       // Stage the 8^3-node velocity block (out-of-grid nodes read as zero).
-      const float4* __restrict__ gvel = p.vel + f.grid_off;
       for (int r = threadIdx.x; r < kRegionNodes; r += kFusedThreads) {
-        const int ix = f.rx + (r & 7), iy = f.ry + ((r >> 3) & 7), iz = f.rz + (r >> 6);
-        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-        if ((unsigned)ix < (unsigned)f.n && (unsigned)iy < (unsigned)f.n && (unsigned)iz < (unsigned)f.n)
-          g = __ldg(&gvel[(size_t)ix + (size_t)f.n * ((size_t)iy + (size_t)f.n * (size_t)iz)]);
-        s_vel[r] = g;
+        const int64_t c = node_index(*scp, p.tile_slot, f.rx + (r & 7), f.ry + ((r >> 3) & 7), f.rz + (r >> 6));
+        s_vel[r] = c >= 0 ? __ldg(&p.vel[c]) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
     if (threadIdx.x == 0) {
@@ -992,10 +1000,8 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
     const Item item = p.items[slot];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
     const uint32_t w = scp->w;
-    const int n = (int)scp->n;
     const float ox = scp->ox, oy = scp->oy, oz = scp->oz, inv_dx = scp->inv_dx, dx = scp->dx;
     const int winx = scp->winx, winy = scp->winy, winz = scp->winz;
-    const uint64_t grid_off = scp->grid_off;
     uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     if (threadIdx.x == 0) s_fault = (scene_frozen(status) || !scp->live) ? 1u : 0u;
@@ -1064,12 +1070,10 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_p2g_det(PoolDev p, float
               // the last regrouping): deposited with an atomic that the
               // combine pass adds to, outside the fixed order; flagged in
               // the status word.
-              const int ix = base[0] + slab, iy = base[1] + j, iz = base[2] + kk;
-              if ((unsigned)ix < (unsigned)n && (unsigned)iy < (unsigned)n && (unsigned)iz < (unsigned)n) {
-                const uint64_t c =
-                    grid_off + (uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * (uint64_t)iz);
+              const int64_t c = node_index(*scp, p.tile_slot, base[0] + slab, base[1] + j, base[2] + kk);
+              if (c >= 0) {
                 atomicAdd(&p.acc[acc_out][c], make_float4(dm, px, py, pz));
-                touch(p.touched[acc_out], c);
+                touch(p.touched[acc_out], (uint64_t)c);
               }
             }
           }
@@ -1153,13 +1157,13 @@ __global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, cons
           sum.z += b.z;
           sum.w += b.w;
         }
-    if (mine) {
+    const int64_t c = mine ? node_index(*scp, p.tile_slot, g[0], g[1], g[2]) : -1;
+    if (c >= 0) {
       // One writer per node; the cell holds zero or out-of-order deposits.
-      const uint64_t c = scp->grid_off + (uint64_t)g[0] + (uint64_t)n * ((uint64_t)g[1] + (uint64_t)n * g[2]);
       float4& a = p.acc[acc_out][c];
       const float4 old = a;
       a = make_float4(old.x + sum.x, old.y + sum.y, old.z + sum.z, old.w + sum.w);
-      touch(p.touched[acc_out], c);
+      touch(p.touched[acc_out], (uint64_t)c);
     }
   }
 }

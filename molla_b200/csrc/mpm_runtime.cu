@@ -243,6 +243,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
     acc[i].alloc(cell_cap);
   }
   slot_of.alloc(cap);
+  slot_tile.alloc(cell_cap / 64);
   keys_by_id.alloc(cap);
   slot_key.alloc(cap);
   hist.alloc(sort_hist_words(cap));
@@ -321,6 +322,9 @@ PoolDev Group::pool() const {
   p.items = items.ptr;
   p.n_items = n_items.ptr;
   p.item_top = item_top;
+  p.tile_slot = tile_slot.ptr;
+  p.slot_tile = slot_tile.ptr;
+  p.tile_mark = tile_mark.ptr;
   p.item_order = item_order.ptr;
   return p;
 }
@@ -387,11 +391,19 @@ void Group::sync_scenes(cudaStream_t st) {
 
 uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
                           const float* velp, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
-                          float dt) {
+                          float dt, uint32_t tile_cap) {
   eng->check();
   if (rows.empty() || rows.size() > (size_t)kMaxMaterials)
     throw Error(MPM_ERR_INVALID, "MPM scene needs 1..=8 material rows");
-  const uint64_t n3 = (uint64_t)cfg.grid_size * cfg.grid_size * cfg.grid_size;
+  {
+    const uint64_t wt = (cfg.grid_size + 3u) / 4u;
+    if (tile_cap > wt * wt * wt) throw Error(MPM_ERR_INVALID, "MPM tile pool capacity is invalid");
+    if (tile_cap && cfg.time_step == MPM_TIME_STEP_IMPLICIT)
+      throw Error(MPM_ERR_UNSUPPORTED, "sparse MPM grid storage runs the explicit time step only");
+  }
+  // dense: the n^3 block; sparse: tile_cap tiles of 64 nodes
+  const uint64_t n3 = tile_cap ? 64ull * tile_cap
+                               : (uint64_t)cfg.grid_size * cfg.grid_size * cfg.grid_size;
   uint32_t sid = (uint32_t)scenes.size();
   for (uint32_t i = 0; i < scenes.size(); ++i)
     if (!scenes[i].live && !scenes[i].retiring) {
@@ -427,6 +439,7 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   s.grid_len = glen;
   s.tiles = (uint32_t)tiles;
   s.key_off = (uint32_t)k0;
+  s.tile_cap = tile_cap;
 
   // upload particles
   if (n) {
@@ -461,6 +474,17 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   grow_keep(key_scene, (size_t)keyr.high_water(), stream);
   MPM_CK(launch_fill_u32(key_scene.ptr + k0, tiles, sid, stream));
   eng->launches += 2;
+  if (tile_cap) {
+    grow_keep(tile_slot, (size_t)keyr.high_water(), stream);
+    if (tile_mark.count < (size_t)keyr.high_water()) {
+      const size_t old = tile_mark.count;
+      grow_keep(tile_mark, (size_t)keyr.high_water(), stream);
+      MPM_CK(cudaMemsetAsync(tile_mark.ptr + old, 0, tile_mark.count - old, stream));
+    }
+    MPM_CK(launch_fill_u32(tile_slot.ptr + k0, tiles, kNoSlot, stream));
+    MPM_CK(cudaMemsetAsync(tile_mark.ptr + k0, 0, tiles, stream));
+    eng->launches += 1;
+  }
   MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, stream));
   n_live += n;
   SceneDev d = make_scene_dev(cfg, rows, dt);
@@ -470,6 +494,7 @@ uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>
   d.grid_off = g0;
   d.id_base = s.id_base;
   d.n_particles = n;
+  d.tile_cap = tile_cap;
   scenes_h[sid] = d;
   s.n_rigid = 0;
   layout_changed();
@@ -535,6 +560,18 @@ void Group::set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st, b
   eng->launches += 1;
 }
 
+bool Group::any_sparse() const {
+  for (size_t i = 0; i < scenes.size(); ++i)
+    if (scenes[i].live && scenes[i].tile_cap) return true;
+  return false;
+}
+
+void Group::finalize_tiles(cudaStream_t st) {
+  if (!any_sparse()) return;
+  MPM_CK(launch_tiles_finalize(pool(), key_scene.ptr, key_space, (uint32_t)scenes.size(), st));
+  eng->launches += 2;
+}
+
 bool Group::any_svd32() const {
   for (size_t i = 0; i < scenes.size(); ++i)
     if (scenes[i].live && scenes[i].cfg.svd_precision != MPM_SVD_FP64) return true;
@@ -558,6 +595,7 @@ void Group::set_scene_dt(uint32_t sid, float dt) {
   d.grid_off = s.grid_off;
   d.id_base = s.id_base;
   d.n_particles = s.n;
+  d.tile_cap = s.tile_cap;
   scenes_h[sid] = d;
   scenes_dirty = true;
   if (d.jacobi_iters && vel2.count < cell_cap) vel2.alloc(cell_cap);
@@ -573,6 +611,8 @@ void Group::set_scene_rigid(uint32_t sid, const float* sp, uint32_t n, cudaStrea
   SceneHost& s = scenes.at(sid);
   if (!s.live) throw Error(MPM_ERR_INVALID, "scene is not live");
   if (n > (uint32_t)kMaxRigid) throw Error(MPM_ERR_INVALID, "at most 8 rigid spheres per scene");
+  if (n && s.tile_cap)
+    throw Error(MPM_ERR_UNSUPPORTED, "rigid spheres are not coupled to sparse MPM grid storage");
   std::vector<RigidDev> rd(n);
   for (uint32_t r = 0; r < n; ++r) {
     const float* q = sp + 7 * (size_t)r;
@@ -647,6 +687,8 @@ void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) 
 
 void Group::set_scene_cfg(uint32_t sid, const mpm_config& cfg) {
   SceneHost& s = scenes.at(sid);
+  if (s.tile_cap && cfg.time_step == MPM_TIME_STEP_IMPLICIT)
+    throw Error(MPM_ERR_UNSUPPORTED, "sparse MPM grid storage runs the explicit time step only");
   s.cfg = cfg;
   invalidate_graphs();
   const float dt = s.dt;
@@ -837,6 +879,7 @@ Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair
   DevBuf<uint32_t> bmeta(cap), borig(cap), bslot(cap), bkey(cap), bstatus(status_d.count);
   DevBuf<float4> bacc0(cells_hw), bacc1(cells_hw), bvel(cells_hw);
   DevBuf<uint8_t> btouch0(cells_hw / kCellBlock + 1), btouch1(cells_hw / kCellBlock + 1);
+  DevBuf<uint32_t> bslots(tile_slot.count), bslot_tile(cells_hw / 64 + 1);
   auto save = [&](bool to_backup) {
     auto cp = [&](void* dst, const void* src, size_t bytes) {
       if (bytes) MPM_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
@@ -853,6 +896,8 @@ Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair
       cp(bvel.ptr, vel.ptr, cells_hw * sizeof(float4));
       cp(btouch0.ptr, touched[0].ptr, cells_hw / kCellBlock);
       cp(btouch1.ptr, touched[1].ptr, cells_hw / kCellBlock);
+      cp(bslots.ptr, tile_slot.ptr, tile_slot.bytes());
+      cp(bslot_tile.ptr, slot_tile.ptr, (cells_hw / 64) * 4);
     } else {
       cp(planes[cur].ptr, bplanes.ptr, pbytes);
       cp(meta[cur].ptr, bmeta.ptr, cap * 4);
@@ -865,6 +910,8 @@ Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair
       cp(vel.ptr, bvel.ptr, cells_hw * sizeof(float4));
       cp(touched[0].ptr, btouch0.ptr, cells_hw / kCellBlock);
       cp(touched[1].ptr, btouch1.ptr, cells_hw / kCellBlock);
+      cp(tile_slot.ptr, bslots.ptr, tile_slot.bytes());
+      cp(slot_tile.ptr, bslot_tile.ptr, (cells_hw / 64) * 4);
     }
   };
   const int cur0 = cur, az0 = acc_zero, al0 = acc_last;
@@ -1027,6 +1074,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   const uint32_t max_jacobi = max_jacobi_iters();
   const bool rigid = any_rigid();
   launch_gather_pass(kRecord, false, st);
+  finalize_tiles(st);  // sparse scenes: the tile map of the first deposit
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
   const bool fused = use_fused();
@@ -1046,6 +1094,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
     }
     launch_gather_pass(last ? kG2P : kG2PRecord, due, st);
     if (!last) {
+      finalize_tiles(st);  // sparse scenes: the tile map of the next deposit
       if (deterministic) {
         // Fixed order: particles (and their records) regrouped into the
         // cells of their new positions before they are deposited.
@@ -1216,24 +1265,52 @@ void Group::write_rows(uint32_t sid, int first, int count, const float* in, cuda
 
 void Group::read_grid(uint32_t sid, float* mass, float* mom, cudaStream_t st) {
   const SceneHost& s = scenes.at(sid);
-  const uint64_t n3 = (uint64_t)s.cfg.grid_size * s.cfg.grid_size * s.cfg.grid_size;
-  std::vector<float4> h(n3);
-  MPM_CK(cudaMemcpyAsync(h.data(), acc[acc_last].ptr + s.grid_off, n3 * sizeof(float4), cudaMemcpyDeviceToHost, st));
-  MPM_CK(cudaStreamSynchronize(st));
-  for (uint64_t i = 0; i < n3; ++i) {
-    if (mass) mass[i] = h[i].x;
+  const uint32_t n = s.cfg.grid_size;
+  const uint64_t n3 = (uint64_t)n * n * n;
+  auto put = [&](uint64_t i, const float4& v) {
+    if (mass) mass[i] = v.x;
     if (mom) {
-      mom[3 * i] = h[i].y;
-      mom[3 * i + 1] = h[i].z;
-      mom[3 * i + 2] = h[i].w;
+      mom[3 * i] = v.y;
+      mom[3 * i + 1] = v.z;
+      mom[3 * i + 2] = v.w;
+    }
+  };
+  if (!s.tile_cap) {
+    std::vector<float4> h(n3);
+    MPM_CK(cudaMemcpyAsync(h.data(), acc[acc_last].ptr + s.grid_off, n3 * sizeof(float4), cudaMemcpyDeviceToHost,
+                           st));
+    MPM_CK(cudaStreamSynchronize(st));
+    for (uint64_t i = 0; i < n3; ++i) put(i, h[i]);
+    return;
+  }
+  // sparse: the slots and the tile map, scattered into the dense layout
+  std::vector<float4> h((size_t)s.tile_cap * 64);
+  std::vector<uint32_t> map(s.tiles);
+  MPM_CK(cudaMemcpyAsync(h.data(), acc[acc_last].ptr + s.grid_off, h.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                         st));
+  MPM_CK(cudaMemcpyAsync(map.data(), tile_slot.ptr + s.key_off, map.size() * 4, cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint64_t i = 0; i < n3; ++i) put(i, zero);
+  const uint32_t w = (n + 3u) / 4u;
+  for (uint32_t t = 0; t < s.tiles; ++t) {
+    if (map[t] == kNoSlot || map[t] >= s.tile_cap) continue;
+    const uint32_t tx = t % w, ty = (t / w) % w, tz = t / (w * w);
+    for (uint32_t l = 0; l < 64; ++l) {
+      const uint32_t ix = 4 * tx + (l & 3u), iy = 4 * ty + ((l >> 2) & 3u), iz = 4 * tz + (l >> 4);
+      if (ix >= n || iy >= n || iz >= n) continue;
+      put((uint64_t)ix + (uint64_t)n * ((uint64_t)iy + (uint64_t)n * iz), h[(size_t)map[t] * 64 + l]);
     }
   }
 }
 
 void Group::totals(uint32_t sid, double* out8, cudaStream_t st) {
   const SceneHost& s = scenes.at(sid);
-  const uint64_t n3 = (uint64_t)s.cfg.grid_size * s.cfg.grid_size * s.cfg.grid_size;
-  MPM_CK(launch_totals(pool(), acc_last, s.grid_off, n3, slot_of.ptr, s.id_base, s.n, totals_d.ptr, st));
+  // the grid range: the n^3 block, or every slot of a sparse scene (slots
+  // outside the current map hold zero)
+  const uint64_t cells = s.tile_cap ? 64ull * s.tile_cap
+                                    : (uint64_t)s.cfg.grid_size * s.cfg.grid_size * s.cfg.grid_size;
+  MPM_CK(launch_totals(pool(), acc_last, s.grid_off, cells, slot_of.ptr, s.id_base, s.n, totals_d.ptr, st));
   eng->launches += 1;
   MPM_CK(cudaMemcpyAsync(out8, totals_d.ptr, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   MPM_CK(cudaStreamSynchronize(st));
@@ -1247,7 +1324,8 @@ void Group::status(uint32_t sid, mpm_status_info* out, cudaStream_t st) {
   out->numerical_fault = (w[0] & kFaultNumerical) ? 1u : 0u;
   // a scene stopped by its substep budget counts one past it (see k_grid_update)
   out->completed_substeps = (w[2] != 0u && w[1] > w[2]) ? w[2] : w[1];
-  out->reserved = 0;
+  const SceneHost& s = scenes.at(sid);
+  out->active_tiles = s.tile_cap ? std::min(w[3], s.tile_cap) : 0u;
 }
 
 void Group::reset_status(uint32_t sid, cudaStream_t st) {

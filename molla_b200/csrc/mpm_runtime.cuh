@@ -130,6 +130,7 @@ struct SceneHost {
   uint32_t tiles = 0;      // w^3
   uint32_t n_rigid = 0;    // rigid spheres set on this scene
   bool retiring = false;   // retired, its particles not yet compacted out (the slot is not reusable)
+  uint32_t tile_cap = 0;   // sparse grid storage: tiles of 4^3 nodes held (0: dense n^3)
 };
 
 struct Range {
@@ -199,6 +200,13 @@ class Group {
   // stable range of the key space (allocated from `keyr` when it is added),
   // so adding or retiring a scene re-keys no other scene.
   DevBuf<uint32_t> key_scene;
+  // Sparse grid storage (scenes added with a tile capacity): slot of every
+  // tile key, tile of every slot (by grid pool cell / 64), and the tiles the
+  // last gather marked.
+  DevBuf<uint32_t> tile_slot, slot_tile;
+  DevBuf<uint8_t> tile_mark;
+  bool any_sparse() const;
+  void finalize_tiles(cudaStream_t st);
   DevBuf<Item> items;
   DevBuf<uint8_t> item_order;  // scatter lane order, 64 cells per item
   DevBuf<uint32_t> tile_item;  // deterministic mode: item of each occupied tile
@@ -253,7 +261,10 @@ class Group {
   int fused_mode = -1;
   static constexpr uint32_t kFusedMaxParticles = 262144;
   bool use_fused() const {
-    return !deterministic && (fused_mode > 0 || (fused_mode < 0 && n_live <= kFusedMaxParticles));
+    // the fused kernel deposits an item before the other items are gathered,
+    // so a sparse scene's tile map (built from all of them) cannot precede it
+    return !deterministic && !any_sparse() &&
+           (fused_mode > 0 || (fused_mode < 0 && n_live <= kFusedMaxParticles));
   }
   // Persistent grids: SMs x resident CTAs per SM.  occ_* are the occupancy
   // maxima of each kernel; the tuned counts (0: the maximum) may be lower.
@@ -285,9 +296,11 @@ class Group {
   };
   std::map<GraphKey, Graph> graphs;
 
+  // tile_cap > 0: sparse grid storage of that many 4^3-node tiles
+  // (MpmSimulation::new_sparse, mpm.rs:846-853) instead of the dense n^3 grid.
   uint32_t add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
                      const float* vel, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
-                     float dt);
+                     float dt, uint32_t tile_cap = 0);
   void remove_scene(uint32_t sid);
   // Retires a scene without touching the rest of the pool: its record is
   // marked dead (the kernels skip its items), its identities get the

@@ -38,7 +38,7 @@ pub struct mpm_config {              // MpmConfig (mpm.rs:400-433) + extensions
 
 #[repr(C)] #[derive(Clone, Copy, Default)]
 pub struct mpm_status_info { pub numerical_fault: u32, pub completed_substeps: u32,
-                             pub fault_bits: u32, pub reserved: u32 }
+                             pub fault_bits: u32, pub active_tiles: u32 }
 
 #[repr(C)] #[derive(Clone, Copy)]
 pub struct mpm_render_view {         // MpmParticleRenderView (mpm_render_view.rs:9-13)
@@ -68,6 +68,8 @@ extern "C" {
     pub fn mpm_config_preset(preset: u32, out: *mut mpm_config) -> c_int;
     pub fn mpm_dp_alpha(friction_angle: f32) -> f32;
     pub fn mpm_sim_create(e: *mut mpm_engine, cfg: *const mpm_config, out: *mut *mut mpm_sim) -> c_int;
+    pub fn mpm_sim_create_sparse(e: *mut mpm_engine, cfg: *const mpm_config, tile_capacity: u32,
+                                 out: *mut *mut mpm_sim) -> c_int;
     pub fn mpm_sim_destroy(s: *mut mpm_sim) -> c_int;
     pub fn mpm_set_particles(s: *mut mpm_sim, xyz: *const f32, vel_or_null: *const f32, n: u32) -> c_int;
     pub fn mpm_set_materials(s: *mut mpm_sim, rows: *const mpm_rheology, n_rows: u32,
@@ -160,6 +162,9 @@ extern "C" {
     pub fn mpm_group_add_scene(g: *mut mpm_group, cfg: *const mpm_config, rows: *const mpm_rheology,
                                n_rows: u32, xyz: *const f32, ids_or_null: *const u32, n: u32, dt: f32,
                                scene_id: *mut u32) -> c_int;
+    pub fn mpm_group_add_scene_sparse(g: *mut mpm_group, cfg: *const mpm_config, rows: *const mpm_rheology,
+                                      n_rows: u32, xyz: *const f32, ids_or_null: *const u32, n: u32, dt: f32,
+                                      tile_capacity: u32, scene_id: *mut u32) -> c_int;
     pub fn mpm_group_remove_scene(g: *mut mpm_group, scene_id: u32) -> c_int;
     pub fn mpm_group_step(g: *mut mpm_group, substeps: u32) -> c_int;
     pub fn mpm_group_step_graph(g: *mut mpm_group, substeps: u32, repeat: u32) -> c_int;
