@@ -817,6 +817,7 @@ def measure_served(args, quiet=False):
     t0 = _t.perf_counter()
     next_arrival = 0.0
     submitted = refused = 0
+    first_ticket = None
     while _t.perf_counter() - t0 < args.serve_seconds:
         now = _t.perf_counter() - t0
         while next_arrival <= now:
@@ -827,10 +828,13 @@ def measure_served(args, quiet=False):
                 refused += 1
             else:
                 steps = int(rng.integers(200, 2001))
-                srv.submit(cfgs[k], s.rows, s.positions, s.ids, s.dt, steps)
+                tk = srv.submit(cfgs[k], s.rows, s.positions, s.ids, s.dt, steps)
+                first_ticket = tk if first_ticket is None else first_ticket
                 submitted += 1
             next_arrival += rng.exponential(1.0 / args.arrival_rate)
         srv.run(1, substeps_per_tick=args.tick_substeps)
+    if first_ticket is not None:
+        srv.poll(first_ticket)  # completes the tick still running
     elapsed = _t.perf_counter() - t0
     st = srv.stats()
     srv.close()

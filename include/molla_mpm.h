@@ -536,10 +536,17 @@ MPM_API int mpm_server_destroy(mpm_server* server);
 MPM_API int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheology* rows, uint32_t n_rows,
                       const float* xyz, const uint32_t* ids_or_null, uint32_t n, float dt, uint32_t steps,
                       uint64_t* ticket);
-/* Runs `ticks` scheduling rounds (admit, step `substeps_per_tick` substeps,
- * retire finished scenes). */
+/* Runs `ticks` scheduling rounds.  A round completes the round before it
+ * (waits for its GPU work, retires the scenes that finished in it: their
+ * positions are kept for poll, their memory goes back at the next
+ * regrouping), admits queued requests in arrival order while the HBM budget
+ * allows, and launches one tick of `substeps_per_tick` substeps for every
+ * resident scene (each stops on the device after its own step count).  The
+ * last round's tick is left running: the call returns while the GPU works,
+ * so requests can be submitted meanwhile. */
 MPM_API int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tick);
-/* state: 0 queued, 1 running, 2 done.  When done, positions are copied out. */
+/* state: 0 queued, 1 running, 2 done.  When done, positions are copied out.
+ * Completes a tick still running first. */
 MPM_API int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float* positions_out, uint32_t cap,
                     uint32_t* count_out);
 /* Server statistics: admitted, completed, resident scenes, resident bytes,

@@ -1276,6 +1276,11 @@ struct mpm_server {
   std::vector<double> tick_ms, queue_ms;
   double admit_ms = 0, step_ms = 0, retire_ms = 0;
   uint64_t ticks = 0;
+  bool in_flight = false;  // a tick launched and not yet completed
+  uint32_t in_flight_len = 0;
+  ~mpm_server() {
+    if (in_flight && eng) cudaEventSynchronize(*e1);
+  }
   std::unique_ptr<mpm::OwnedEvent> e0, e1;  // tick timing
 };
 
@@ -1347,12 +1352,45 @@ int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const mpm_rheol
   });
 }
 
+// Completes the tick in flight: waits for it, records its time, and retires
+// the scenes that finished in it (their results are read, their slots go
+// back at the next regrouping).
+static void server_complete_tick(mpm_server* server) {
+  if (!server->in_flight) return;
+  mpm::Group& g = *server->g;
+  cudaStream_t st = server->eng->stream;
+  const double t0 = now_ms();
+  MPM_CK(cudaEventSynchronize(*server->e1));
+  server->in_flight = false;
+  float ms = 0.f;
+  MPM_CK(cudaEventElapsedTime(&ms, *server->e0, *server->e1));
+  const uint32_t len = server->in_flight_len;
+  server->tick_ms.push_back(ms / (float)len);
+  const double t_ret0 = now_ms();
+  server->step_ms += t_ret0 - t0;
+  for (auto& kv : server->tickets) {
+    Ticket& t = kv.second;
+    if (t.state != 1) continue;
+    t.remaining = t.remaining > len ? t.remaining - len : 0;
+    if (t.remaining == 0) {
+      t.result.resize(3 * (size_t)t.n);
+      if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), st);
+      g.retire_scene(t.sid);
+      server->resident -= t.bytes;
+      t.state = 2;
+      server->completed++;
+    }
+  }
+  server->retire_ms += now_ms() - t_ret0;
+}
+
 int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tick) {
   return guard([&] {
     REQUIRE(server && substeps_per_tick > 0, MPM_ERR_INVALID, "invalid argument");
     mpm::Group& g = *server->g;
     cudaStream_t st = server->eng->stream;
     for (uint32_t tick = 0; tick < ticks; ++tick) {
+      server_complete_tick(server);
       const double t_admit0 = now_ms();
       // admit in arrival order while the budget and pools allow
       while (!server->queue.empty()) {
@@ -1411,29 +1449,13 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
       MPM_CK(cudaEventRecord(*server->e0, st));
       g.step_graph(len, 1, st);
       MPM_CK(cudaEventRecord(*server->e1, st));
-      MPM_CK(cudaEventSynchronize(*server->e1));
-      float ms = 0.f;
-      MPM_CK(cudaEventElapsedTime(&ms, *server->e0, *server->e1));
-      server->tick_ms.push_back(ms / (float)len);
+      // The tick runs on the GPU while the caller goes on (submitting
+      // requests); the next run, poll or stats call completes it.
+      server->in_flight = true;
+      server->in_flight_len = len;
       server->particle_steps += parts;
       server->ticks++;
-      const double t_ret0 = now_ms();
-      server->step_ms += t_ret0 - t_step0;
-      // retire finished scenes: their slots go back at the next regrouping
-      for (auto& kv : server->tickets) {
-        Ticket& t = kv.second;
-        if (t.state != 1) continue;
-        t.remaining = t.remaining > len ? t.remaining - len : 0;
-        if (t.remaining == 0) {
-          t.result.resize(3 * (size_t)t.n);
-          if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), st);
-          g.retire_scene(t.sid);
-          server->resident -= t.bytes;
-          t.state = 2;
-          server->completed++;
-        }
-      }
-      server->retire_ms += now_ms() - t_ret0;
+      server->step_ms += now_ms() - t_step0;
     }
   });
 }
@@ -1442,6 +1464,7 @@ int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float*
                     uint32_t* count_out) {
   return guard([&] {
     REQUIRE(server && state, MPM_ERR_INVALID, "null argument");
+    server_complete_tick(server);
     auto it = server->tickets.find(ticket);
     REQUIRE(it != server->tickets.end(), MPM_ERR_INVALID, "unknown ticket");
     Ticket& t = it->second;
