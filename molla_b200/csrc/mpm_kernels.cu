@@ -461,15 +461,10 @@ __global__ void k_items(const uint32_t* __restrict__ tile_start, uint32_t K, con
 // a warp the cells are in the order of their particle counts (thread c
 // counts cell c in the item's slot keys, sorted by cell within a tile, by
 // binary search).  The four cells with b of 30 or 31 go to the spare lanes.
-__global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ items,
-                                                   const uint32_t* __restrict__ n_items, uint32_t item_top,
-                                                   const uint32_t* __restrict__ slot_key,
-                                                   uint8_t* __restrict__ item_order) {
-  __shared__ uint32_t s_cnt[64];
-  __shared__ uint8_t s_pair[32][2];
-  __shared__ uint32_t s_fill[32];
-  const uint32_t it = blockIdx.x;  // an item slot: [0, n_items[0]) or [item_top - n_items[1], item_top)
-  if (it >= n_items[0] && it < item_top - n_items[1]) return;
+__device__ __forceinline__ void item_order_one(const Item* __restrict__ items, uint32_t it,
+                                               const uint32_t* __restrict__ slot_key, uint8_t* __restrict__ item_order,
+                                               uint32_t (&s_cnt)[64], uint8_t (&s_pair)[32][2],
+                                               uint32_t (&s_fill)[32]) {
   const Item item = items[it];
   const uint32_t c = threadIdx.x;
   const uint32_t* keys = slot_key + item.start;
@@ -525,6 +520,24 @@ __global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ item
       sort(a, 4);
       for (uint32_t i = 0; i < 4; ++i) out[60 + i] = a[i];
     }
+  }
+}
+
+// Grid-stride over the work list's items (the FP32-SVD items, then the
+// FP64-SVD ones at the top of the slot range), so that only the items that
+// exist are visited.
+__global__ void __launch_bounds__(64) k_item_order(const Item* __restrict__ items,
+                                                   const uint32_t* __restrict__ n_items, uint32_t item_top,
+                                                   const uint32_t* __restrict__ slot_key,
+                                                   uint8_t* __restrict__ item_order) {
+  __shared__ uint32_t s_cnt[64];
+  __shared__ uint8_t s_pair[32][2];
+  __shared__ uint32_t s_fill[32];
+  const uint32_t n32 = n_items[0], total = n32 + n_items[1];
+  for (uint32_t li = blockIdx.x; li < total; li += gridDim.x) {
+    const uint32_t it = li < n32 ? li : item_top - 1u - (li - n32);
+    item_order_one(items, it, slot_key, item_order, s_cnt, s_pair, s_fill);
+    __syncthreads();  // the shared tables are reused by the next item
   }
 }
 
@@ -747,7 +760,8 @@ cudaError_t launch_fill_u32(uint32_t* p, uint64_t n, uint32_t v, cudaStream_t st
 cudaError_t launch_item_order(const Item* items, const uint32_t* n_items, uint32_t item_top, const uint32_t* slot_key,
                               uint8_t* item_order, cudaStream_t st) {
   if (!item_top) return cudaSuccess;
-  k_item_order<<<item_top, 64, 0, st>>>(items, n_items, item_top, slot_key, item_order);
+  k_item_order<<<std::min<uint32_t>(item_top, 148u * 32u), 64, 0, st>>>(items, n_items, item_top, slot_key,
+                                                                        item_order);
   return cudaGetLastError();
 }
 

@@ -433,7 +433,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 // substep of a call), kG2PRecord (gather + return mapping + B for the next
 // scatter, with the return mapping's SVD reused).
 template <int MODE, bool WRITE_KEYS, class SR>
-__global__ void __launch_bounds__(kGatherThreads, 4) k_g2p(PoolDev p, double tol, int sweeps, int reuse_svd) {
+__global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol, int sweeps, int reuse_svd) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   __shared__ __align__(16) SceneDev s_sc;
