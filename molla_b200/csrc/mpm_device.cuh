@@ -280,8 +280,8 @@ __device__ __forceinline__ T det3(const T* a) {
 // U is held in FP32 in both forms: its consumers (the stress record and
 // the rebuilt F) are FP32, while sigma and V carry the form's precision.
 template <class T> struct SvdOut {
-  float u[9];
-  T s[3], v[9];
+  float u[9], v[9];
+  T s[3];
 };
 
 // Newton-Raphson reciprocal square root of x > 0: y <- y (3 - x y^2) / 2
@@ -307,8 +307,8 @@ __device__ __forceinline__ double nr_rsqrt(double x) {
 
 // One FP32 Jacobi rotation of the (P, Q) pair of the symmetric a[3][3]
 // (reference formulas); V is updated with the same c, s in type T.
-template <class T, int P, int Q>
-__device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, float& max_off) {
+template <int P, int Q>
+__device__ __forceinline__ void jacobi_rot(float (&a)[3][3], float* v, float tol, float& max_off) {
   constexpr int K = 3 - P - Q;
   const float apq = a[P][Q];
   const float aapq = fabsf(apq);
@@ -317,7 +317,6 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
   const float app = a[P][P];
   const float aqq = a[Q][Q];
   float t, c, s;
-  T cv, sv;
   {
     // t = 1 / (theta + sgn(theta) sqrt(1 + theta^2)), theta = d / e, written
     // as sgn(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq
@@ -332,23 +331,13 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
     const float r2 = d * d + e * e;
     const float hyp = r2 * rsqrtf(r2);
     t = __fdividef(d >= 0.0f ? e : -e, fabsf(d) + hyp);
-    c = rsqrtf(1.0f + t * t);
+    // c = (1 + t^2)^(-1/2): the hardware seed and one Newton step, so that
+    // c^2 + s^2 = 1 to FP32 rounding and the accumulated V stays orthogonal
+    // (a V that drifts from orthogonality rotates F through the rebuild)
+    const float h = fmaf(t, t, 1.0f);
+    c = rsqrtf(h);
+    c = c * fmaf(-0.5f * h * c, c, 1.5f);
     s = t * c;
-  }
-  if constexpr (sizeof(T) == 4) {
-    cv = c;
-    sv = s;
-  } else {
-    // FP64 rotation for V: exactly orthogonal to FP64 rounding for this t.
-    const double td = (double)t;
-    const double h = 0.5 * fma(td, td, 1.0);
-    double y = (double)c;
-    double r = fma(-h * y, y, 0.5);
-    y = fma(y, r, y);
-    r = fma(-h * y, y, 0.5);
-    y = fma(y, r, y);
-    cv = y;
-    sv = td * y;
   }
   a[P][P] = app - t * apq;
   a[Q][Q] = aqq + t * apq;
@@ -366,10 +355,10 @@ __device__ __forceinline__ void jacobi_rot(float (&a)[3][3], T* v, float tol, fl
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const T vkp = v[3 * P + k];
-    const T vkq = v[3 * Q + k];
-    v[3 * P + k] = cv * vkp - sv * vkq;
-    v[3 * Q + k] = sv * vkp + cv * vkq;
+    const float vkp = v[3 * P + k];
+    const float vkq = v[3 * Q + k];
+    v[3 * P + k] = c * vkp - s * vkq;
+    v[3 * Q + k] = s * vkp + c * vkq;
   }
 }
 
@@ -396,47 +385,59 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
         a[r][c] = a[c][r];
       }
   }
-  T* v = o.v;
+  float* v = o.v;
 #pragma unroll
-  for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? T(1) : T(0);
+  for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? 1.0f : 0.0f;
   const float ftol = (float)tol;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     float max_off = 0.0f;
-    jacobi_rot<T, 0, 1>(a, v, ftol, max_off);
-    jacobi_rot<T, 0, 2>(a, v, ftol, max_off);
-    jacobi_rot<T, 1, 2>(a, v, ftol, max_off);
+    jacobi_rot<0, 1>(a, v, ftol, max_off);
+    jacobi_rot<0, 2>(a, v, ftol, max_off);
+    jacobi_rot<1, 2>(a, v, ftol, max_off);
     if (max_off < ftol) break;
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    const T x = f[0] * v[3 * i] + f[3] * v[3 * i + 1] + f[6] * v[3 * i + 2];
-    const T y = f[1] * v[3 * i] + f[4] * v[3 * i + 1] + f[7] * v[3 * i + 2];
-    const T z = f[2] * v[3 * i] + f[5] * v[3 * i + 1] + f[8] * v[3 * i + 2];
-    T s;
     if constexpr (sizeof(T) == 4) {
+      const float x = f[0] * v[3 * i] + f[3] * v[3 * i + 1] + f[6] * v[3 * i + 2];
+      const float y = f[1] * v[3 * i] + f[4] * v[3 * i + 1] + f[7] * v[3 * i + 2];
+      const float z = f[2] * v[3 * i] + f[5] * v[3 * i + 1] + f[8] * v[3 * i + 2];
       const float q = x * x + y * y + z * z;
-      s = q > 0.0f ? q * rsqrtf(q) : 0.0f;
-    } else {
-      const T q = x * x + y * y + z * z;
-      s = q > T(0) ? q * nr_rsqrt(q) : T(0);
-    }
-    o.s[i] = s;
-    if (s > T(1.0e-12)) {
-      if constexpr (sizeof(T) == 4) {
+      const float s = sqrtf(q);  // correctly rounded: the stress depends on s - 1
+      o.s[i] = s;
+      if (s > 1.0e-12f) {
         const float inv = __frcp_rn(s);
         o.u[3 * i] = x * inv;
         o.u[3 * i + 1] = y * inv;
         o.u[3 * i + 2] = z * inv;
       } else {
-        const float inv = 1.0f / (float)s;
-        o.u[3 * i] = (float)x * inv;
-        o.u[3 * i + 1] = (float)y * inv;
-        o.u[3 * i + 2] = (float)z * inv;
+        o.u[3 * i] = i == 0 ? 1.0f : 0.0f;
+        o.u[3 * i + 1] = i == 1 ? 1.0f : 0.0f;
+        o.u[3 * i + 2] = i == 2 ? 1.0f : 0.0f;
       }
     } else {
-      o.u[3 * i] = i == 0 ? 1.0f : 0.0f;
-      o.u[3 * i + 1] = i == 1 ? 1.0f : 0.0f;
-      o.u[3 * i + 2] = i == 2 ? 1.0f : 0.0f;
+      // sigma_i = |F v_i| / |v_i| in FP64: a Rayleigh quotient, second order
+      // in the direction error of the FP32 v_i, with the norm of v_i (1 up
+      // to a few FP32 ulps) divided out: 1/|v| = 1.5 - n2/2 to O((n2-1)^2).
+      const double v0 = v[3 * i], v1 = v[3 * i + 1], v2 = v[3 * i + 2];
+      const double x = f[0] * v0 + f[3] * v1 + f[6] * v2;
+      const double y = f[1] * v0 + f[4] * v1 + f[7] * v2;
+      const double z = f[2] * v0 + f[5] * v1 + f[8] * v2;
+      const double q = x * x + y * y + z * z;
+      const double rq = q > 0.0 ? nr_rsqrt(q) : 0.0;  // 1 / |F v_i|
+      const double rn = fma(-0.5, v0 * v0 + v1 * v1 + v2 * v2, 1.5);
+      const double s = q * rq * rn;
+      o.s[i] = s;
+      if (s > 1.0e-12) {
+        // u_i = F v_i / |F v_i|
+        o.u[3 * i] = (float)(x * rq);
+        o.u[3 * i + 1] = (float)(y * rq);
+        o.u[3 * i + 2] = (float)(z * rq);
+      } else {
+        o.u[3 * i] = i == 0 ? 1.0f : 0.0f;
+        o.u[3 * i + 1] = i == 1 ? 1.0f : 0.0f;
+        o.u[3 * i + 2] = i == 2 ? 1.0f : 0.0f;
+      }
     }
   }
   if (det3(o.u) < 0.0f) {
@@ -456,10 +457,9 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
   }
   // V is a product of plane rotations, so det V = +1 up to rounding: the
   // reference's flip (mpm.wgsl:457-466) never fires.  It is kept in the FP32
-  // reference form; the FP64 form, whose rotations are refined to FP64,
-  // skips its FP64 determinant.
+  // reference form and skipped in the FP64 form.
   if constexpr (sizeof(T) == 4) {
-    if (det3(v) < T(0)) {
+    if (det3(v) < 0.0f) {
       // flip the column of V with the smallest |sigma|
       const T a0 = o.s[0] < T(0) ? -o.s[0] : o.s[0];
       const T a1 = o.s[1] < T(0) ? -o.s[1] : o.s[1];
@@ -470,11 +470,11 @@ __device__ __forceinline__ void svd3(const T* f, const float* f32, SvdOut<T>& o,
       const int mi = m2 ? 2 : (m1 ? 1 : 0);
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const T sg = (i == mi) ? T(-1) : T(1);
+        const float sg = (i == mi) ? -1.0f : 1.0f;
         v[3 * i] *= sg;
         v[3 * i + 1] *= sg;
         v[3 * i + 2] *= sg;
-        o.s[i] *= sg;
+        o.s[i] *= (T)sg;
       }
     }
   }
@@ -607,15 +607,14 @@ __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev&
   float s[3] = {(float)svd.s[0], (float)svd.s[1], (float)svd.s[2]};
   {
     float nf = 0.0f;
-    T nfv = T(0);
 #pragma unroll
     for (int a = 0; a < 3; ++a) nf = nf_acc(nf, s[a]);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       nf = nf_acc(nf, svd.u[i]);
-      nfv = nf_acc(nfv, svd.v[i]);  // |v| <= 1: finite in T is finite in FP32
+      nf = nf_acc(nf, svd.v[i]);
     }
-    if (!nf_ok(nf) || !nf_ok(nfv)) return false;
+    if (!nf_ok(nf)) return false;
   }
   T ns[3] = {svd.s[0], svd.s[1], svd.s[2]};
   float dq = 0.0f;

@@ -306,21 +306,27 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
           svd3<SR>(Fs, F, svd, stol, sweeps);
           float jp_new = jp;
           bool changed = true;
+          const SR s_trial[3] = {svd.s[0], svd.s[1], svd.s[2]};
           if (plasticity_project<SR>(svd, md, jp_new, changed)) {
             // FP32 mode rebuilds F = U s V^T every substep (the
-            // reference); the FP64-SVD mode keeps the trial F when
-            // the return mapping left every singular value unchanged.
-            SR Fr[9];
+            // reference).  The FP64-SVD mode keeps the trial F when the
+            // return mapping left every singular value unchanged, and
+            // otherwise adds U diag(s - s_trial) V^T to it: the same F as
+            // U s V^T in exact arithmetic (F = U s_trial V^T), with the
+            // FP32 rounding of U and V scaled by the (small) change in s
+            // instead of by F.
+            float Fr[9];
             const bool rebuild = sizeof(SR) == 4 || changed;
             if (rebuild) {
-              // F = U diag(s) V^T in the form's precision (U is FP32)
+              float ds[3];
+#pragma unroll
+              for (int i = 0; i < 3; ++i) ds[i] = sizeof(SR) == 4 ? (float)svd.s[i] : (float)(svd.s[i] - s_trial[i]);
 #pragma unroll
               for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
-                  Fr[3 * c + r] = ((SR)svd.u[r] * svd.s[0]) * svd.v[c] +
-                                  ((SR)svd.u[3 + r] * svd.s[1]) * svd.v[3 + c] +
-                                  ((SR)svd.u[6 + r] * svd.s[2]) * svd.v[6 + c];
+                  Fr[3 * c + r] = (sizeof(SR) == 4 ? 0.0f : F[3 * c + r]) + (svd.u[r] * ds[0]) * svd.v[c] +
+                                  (svd.u[3 + r] * ds[1]) * svd.v[3 + c] + (svd.u[6 + r] * ds[2]) * svd.v[6 + c];
             }
             // the FP32 copy must be finite too (an FP64 value beyond FP32 range)
             float nf4 = 0.0f;
