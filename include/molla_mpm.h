@@ -545,7 +545,10 @@ MPM_API int mpm_server_submit(mpm_server* server, const mpm_config* cfg, const m
  * last round's tick is left running: the call returns while the GPU works,
  * so requests can be submitted meanwhile. */
 MPM_API int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tick);
-/* state: 0 queued, 1 running, 2 done.  When done, positions are copied out.
+/* state: 0 queued, 1 running, 2 done, 3 faulted (the scene's fault latch
+ * was set: a non-finite state or a sparse grid out of tiles; it is retired
+ * at the first tick that sees it).  When done or faulted, the positions
+ * are copied out (for a faulted scene, those frozen at the fault).
  * Completes a tick still running first. */
 MPM_API int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float* positions_out, uint32_t cap,
                     uint32_t* count_out);
@@ -567,8 +570,14 @@ typedef struct mpm_server_stats {
   double step_ms;
   double retire_ms;
   uint64_t ticks;
+  /* requests retired as faulted (their particle_steps count only the
+   * substeps completed before the fault) */
+  uint64_t faulted;
 } mpm_server_stats;
 MPM_API int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out);
+/* Device status of a finished (done or faulted) request, as it stood when it
+ * was retired: fault bits and completed substeps. */
+MPM_API int mpm_server_ticket_status(mpm_server* server, uint64_t ticket, mpm_status_info* out);
 
 /* ---- errors ------------------------------------------------------------- */
 

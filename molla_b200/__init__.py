@@ -907,7 +907,14 @@ class MpmServer:
         st = C.c_uint32()
         cnt = C.c_uint32()
         _check(_ffi.lib().mpm_server_poll(self._h, ticket, C.byref(st), _fp(out), n, C.byref(cnt)))
-        return int(st.value), (out[: cnt.value] if st.value == 2 else None)
+        return int(st.value), (out[: cnt.value] if st.value in (2, 3) else None)
+
+    def ticket_status(self, ticket: int) -> MpmActiveGridStats:
+        """Device status of a finished request (state 2 done, 3 faulted) as it
+        stood at its retirement."""
+        s = _ffi.mpm_status_info()
+        _check(_ffi.lib().mpm_server_ticket_status(self._h, ticket, C.byref(s)))
+        return MpmActiveGridStats(bool(s.numerical_fault), int(s.completed_substeps), int(s.fault_bits))
 
     def stats(self) -> dict:
         s = _ffi.mpm_server_stats()

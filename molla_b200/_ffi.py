@@ -86,6 +86,7 @@ class mpm_server_stats(C.Structure):
         ("step_ms", C.c_double),
         ("retire_ms", C.c_double),
         ("ticks", C.c_uint64),
+        ("faulted", C.c_uint64),
     ]
 
 
@@ -236,6 +237,7 @@ SIGNATURES = {
     "mpm_server_run": (I, [P, U32, U32]),
     "mpm_server_poll": (I, [P, U64, U32P, F32P, U32, U32P]),
     "mpm_server_stats_get": (I, [P, C.POINTER(mpm_server_stats)]),
+    "mpm_server_ticket_status": (I, [P, C.c_uint64, C.POINTER(mpm_status_info)]),
 }
 
 _lib = None

@@ -1212,8 +1212,10 @@ struct Ticket {
   uint32_t n = 0;
   float dt = 0.f;
   uint32_t steps = 0, remaining = 0;
-  uint32_t state = 0;  // 0 queued, 1 running, 2 done
+  uint32_t state = 0;  // 0 queued, 1 running, 2 done, 3 faulted
   uint32_t sid = 0xffffffffu;
+  uint32_t counted = 0;  // substeps launched for it (counted into particle_steps)
+  mpm_status_info status{};  // device status word at retirement
   uint64_t bytes = 0;
   uint32_t tile_cap = 0;  // sparse grid storage when it saves memory (0: dense)
   std::vector<float> result;
@@ -1272,7 +1274,8 @@ struct mpm_server {
   std::deque<uint64_t> queue;
   std::map<uint64_t, Ticket> tickets;
   uint64_t next_id = 1;
-  uint64_t admitted = 0, completed = 0, particle_steps = 0;
+  uint64_t admitted = 0, completed = 0, faulted = 0, particle_steps = 0;
+  std::vector<uint32_t> status_w;  // status words read at each tick's completion
   std::vector<double> tick_ms, queue_ms;
   double admit_ms = 0, step_ms = 0, retire_ms = 0;
   uint64_t ticks = 0;
@@ -1368,17 +1371,34 @@ static void server_complete_tick(mpm_server* server) {
   server->tick_ms.push_back(ms / (float)len);
   const double t_ret0 = now_ms();
   server->step_ms += t_ret0 - t0;
+  // One copy of every scene's status word: a scene whose fault latch is set
+  // (a non-finite state, a sparse grid out of tiles) stands frozen on the
+  // device, so it is retired now as faulted instead of running out its
+  // budget, and the substeps it did not take leave the step count.
+  g.status_words(server->status_w, st);
   for (auto& kv : server->tickets) {
     Ticket& t = kv.second;
     if (t.state != 1) continue;
-    t.remaining = t.remaining > len ? t.remaining - len : 0;
+    const uint32_t* w = server->status_w.data() + (size_t)t.sid * mpm::kStatusWords;
+    const bool fault = w[0] != 0u;
+    t.remaining = fault ? 0 : (t.remaining > len ? t.remaining - len : 0);
     if (t.remaining == 0) {
+      t.status.fault_bits = w[0];
+      t.status.numerical_fault = (w[0] & mpm::kFaultNumerical) ? 1u : 0u;
+      t.status.completed_substeps = (w[2] != 0u && w[1] > w[2]) ? w[2] : w[1];
       t.result.resize(3 * (size_t)t.n);
       if (t.n) g.read_rows(t.sid, mpm::PX, 3, t.result.data(), st);
       g.retire_scene(t.sid);
       server->resident -= t.bytes;
-      t.state = 2;
-      server->completed++;
+      if (fault) {
+        if (t.counted > t.status.completed_substeps)
+          server->particle_steps -= (uint64_t)t.n * (t.counted - t.status.completed_substeps);
+        t.state = 3;
+        server->faulted++;
+      } else {
+        t.state = 2;
+        server->completed++;
+      }
     }
   }
   server->retire_ms += now_ms() - t_ret0;
@@ -1441,7 +1461,11 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
       const uint32_t len = substeps_per_tick;
       uint64_t parts = 0;
       for (auto& kv : server->tickets)
-        if (kv.second.state == 1) parts += (uint64_t)kv.second.n * std::min(kv.second.remaining, len);
+        if (kv.second.state == 1) {
+          const uint32_t k = std::min(kv.second.remaining, len);
+          parts += (uint64_t)kv.second.n * k;
+          kv.second.counted += k;
+        }
       if (parts == 0 && g.live_scenes() == 0) {
         if (server->queue.empty()) break;
         continue;
@@ -1470,10 +1494,22 @@ int mpm_server_poll(mpm_server* server, uint64_t ticket, uint32_t* state, float*
     Ticket& t = it->second;
     *state = t.state;
     if (count_out) *count_out = t.n;
-    if (t.state == 2 && positions_out) {
+    if ((t.state == 2 || t.state == 3) && positions_out) {
       REQUIRE(cap >= t.n, MPM_ERR_INVALID, "output capacity below the particle count");
       std::memcpy(positions_out, t.result.data(), 12 * (size_t)t.n);
     }
+  });
+}
+
+int mpm_server_ticket_status(mpm_server* server, uint64_t ticket, mpm_status_info* out) {
+  return guard([&] {
+    REQUIRE(server && out, MPM_ERR_INVALID, "null argument");
+    server_complete_tick(server);
+    auto it = server->tickets.find(ticket);
+    REQUIRE(it != server->tickets.end(), MPM_ERR_INVALID, "unknown ticket");
+    const Ticket& t = it->second;
+    REQUIRE(t.state >= 2, MPM_ERR_INVALID, "the request has not finished");
+    *out = t.status;
   });
 }
 
@@ -1798,6 +1834,7 @@ int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out) {
     out->step_ms = server->step_ms;
     out->retire_ms = server->retire_ms;
     out->ticks = server->ticks;
+    out->faulted = server->faulted;
   });
 }
 

@@ -136,6 +136,17 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// Ampere-style asynchronous 4-byte global -> shared copies (cp.async), in
+// commit groups; a thread waits for its own groups.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Waits for the phase of `bar` with the given parity to complete; gives up
 // (returns false) after about one second.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
@@ -153,21 +164,46 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // and the scatter record (MODE != kG2P), returned in rec.  vblock is the
 // staged 8^3-node velocity block of the item's tile (origin node rx, ry, rz);
 // fallback is a 12-float shared-memory slot of this thread for gather_global.
+// The particle inputs the gather stages in shared memory, in order: the
+// position planes, the F planes, mass, volume and J_p (planes PX..PZ and
+// F0..JP in plane order), then the meta word.
+constexpr int kStagedInputs = 16;
+static_assert(PY == PX + 1 && PZ == PX + 2 && MASS == F0 + 9 && VOL == F0 + 10 && JP == F0 + 11,
+              "the staged planes are two runs of consecutive planes");
+
+// `in` (kStagedInputs entries kGatherThreads apart, or null) holds the
+// particle's inputs in the order of kStagedPlanes, copied to shared memory
+// ahead of time (k_g2p); null reads them from the pool.
 template <int MODE, bool WRITE_KEYS, class SR>
 __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, uint32_t* status,
                                               const float4* __restrict__ vblock, float* fallback, int rx, int ry,
                                               int rz, int n, SR stol, int sweeps, int reuse_svd, bool publish_vc,
-                                              float4 (&rec)[4]) {
+                                              float4 (&rec)[4], const float* __restrict__ in = nullptr) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
-  float x = plane(p, PX)[s], y = plane(p, PY)[s], z = plane(p, PZ)[s];
-  float F[9];
+  float x, y, z, F[9], jp, mass, vol;
+  uint32_t mat;
+  if (in) {
+    x = in[0];
+    y = in[kGatherThreads];
+    z = in[2 * kGatherThreads];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) F[i] = plane(p, F0 + i)[s];
-  float jp = plane(p, JP)[s];
-  const float mass = plane(p, MASS)[s];
-  const float vol = plane(p, VOL)[s];
-  const uint32_t mat = p.meta[s] & 7u;
+    for (int i = 0; i < 9; ++i) F[i] = in[(3 + i) * kGatherThreads];
+    mass = in[12 * kGatherThreads];
+    vol = in[13 * kGatherThreads];
+    jp = in[14 * kGatherThreads];
+    mat = __float_as_uint(in[15 * kGatherThreads]) & 7u;
+  } else {
+    x = plane(p, PX)[s];
+    y = plane(p, PY)[s];
+    z = plane(p, PZ)[s];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) F[i] = plane(p, F0 + i)[s];
+    jp = plane(p, JP)[s];
+    mass = plane(p, MASS)[s];
+    vol = plane(p, VOL)[s];
+    mat = p.meta[s] & 7u;
+  }
   float v[3], C[9];
   bool ok = true;
   SvdOut<SR> svd;
@@ -445,46 +481,85 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
   __shared__ __align__(16) SceneDev s_sc;
   __shared__ __align__(16) SharedGather s_gath;
   __shared__ uint32_t s_fault;
+  // Particle inputs of this round and the next (cp.async double buffer):
+  // [buffer][input][thread], the inputs in kStagedPlanes order.
+  __shared__ __align__(16) float s_in[2][kStagedInputs][kGatherThreads];
   // this SVD form's range of the work list: FP32-SVD items, then FP64-SVD items
   const uint32_t n32 = p.n_items[0];
   const uint32_t it_lo = sizeof(SR) == 8 ? n32 : 0u;
   const uint32_t it_hi = sizeof(SR) == 8 ? n32 + p.n_items[1] : n32;
   const SR stol = (SR)tol;
+  uint32_t s_sc_scene = 0xffffffffu;  // scene whose record s_sc holds
   for (uint32_t it = it_lo + blockIdx.x; it < it_hi; it += gridDim.x) {
     const Item item = p.items[item_slot(p, n32, it)];
-    {
+    // A thread's particles come kGatherThreads apart; the inputs of its
+    // next particle are copied to shared memory (cp.async) while it computes
+    // this one, and those of its first are requested here, so that their
+    // loads overlap the velocity block's.
+    const uint32_t tid = threadIdx.x;
+    auto fetch = [&](uint32_t k, int b) {
+      if (k < item.count) {
+        const uint32_t s = item.start + k;
+        // walk the planes with one pointer: PX..PZ, then F0..JP
+        const size_t cap = p.cap;
+        const float* src = p.planes + s;
+#pragma unroll
+        for (int q = 0; q < 3; ++q, src += cap) cp_async4(&s_in[b][q][tid], src);
+        src += (size_t)(F0 - 3) * cap;
+#pragma unroll
+        for (int q = 3; q < kStagedInputs - 1; ++q, src += cap) cp_async4(&s_in[b][q][tid], src);
+        cp_async4(&s_in[b][kStagedInputs - 1][tid], p.meta + s);
+      }
+      cp_async_commit();
+    };
+    fetch(tid, 0);
+    // The scene record goes to shared memory when the item's scene differs
+    // from the last item's (consecutive items of a CTA mostly share one):
+    // the velocity staging below reads the geometry from there, so a new
+    // record is published by a barrier first.
+    if (item.scene != s_sc_scene) {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(p.scenes + item.scene);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_sc);
-      for (int k = threadIdx.x; k < (int)(sizeof(SceneDev) / 4); k += blockDim.x) dst[k] = src[k];
+      for (int k = threadIdx.x; k < (int)(sizeof(SceneDev) / 4); k += kGatherThreads) dst[k] = src[k];
+      s_sc_scene = item.scene;
+      __syncthreads();
     }
-    const SceneDev* __restrict__ scp = p.scenes + item.scene;
-    uint32_t* status = p.status + (size_t)scp->status * kStatusWords;
+    const SceneDev& sc = s_sc;
+    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
     // a latched fault, a spent substep budget or a retired scene: stand still
-    const uint32_t fault0 = (scene_frozen(status) || !scp->live) ? 1u : 0u;
+    const uint32_t fault0 = (scene_frozen(status) || !sc.live) ? 1u : 0u;
     const bool publish_vc = budget_ends(status);
-    const uint32_t w = scp->w;
+    const uint32_t w = sc.w;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
-    const int n = (int)scp->n;
+    const int n = (int)sc.n;
     if constexpr (kGather) {
-      // Stage the 8^3-node velocity block (out-of-grid nodes read as zero).
-      for (int r = threadIdx.x; r < kRegionNodes; r += blockDim.x) {
-        const int64_t c = node_index(*scp, p.tile_slot, rx + (r & 7), ry + ((r >> 3) & 7), rz + (r >> 6));
-        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c >= 0) g = __ldg(&p.vel[c]);
-        s_gath.vel[r] = g;
+      // Stage the 8^3-node velocity block (out-of-grid nodes read as zero),
+      // the four loads of a thread in flight together.
+      constexpr int kPer = kRegionNodes / kGatherThreads;
+      static_assert(kPer * kGatherThreads == kRegionNodes, "the block splits evenly over the CTA");
+      float4 g[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        const int r = (int)threadIdx.x + q * kGatherThreads;
+        const int64_t c = node_index(sc, p.tile_slot, rx + (r & 7), ry + ((r >> 3) & 7), rz + (r >> 6));
+        g[q] = c >= 0 ? __ldg(&p.vel[c]) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) s_gath.vel[(int)threadIdx.x + q * kGatherThreads] = g[q];
     }
     if (threadIdx.x == 0) s_fault = fault0;
     __syncthreads();
-    const SceneDev& sc = s_sc;
     const bool faulted = s_fault != 0;
     if (!faulted) {
-      for (uint32_t k = threadIdx.x; k < item.count; k += blockDim.x) {
+      int b = 0;
+      for (uint32_t k = tid; k < item.count; k += kGatherThreads, b ^= 1) {
+        fetch(k + kGatherThreads, b ^ 1);
+        cp_async_wait<1>();
         const uint32_t s = item.start + k;
         float4 rec[4];
         particle_step<MODE, WRITE_KEYS, SR>(p, sc, s, status, s_gath.vel, s_gath.fallback[threadIdx.x], rx, ry, rz, n,
-                                            stol, sweeps, reuse_svd, publish_vc, rec);
+                                            stol, sweeps, reuse_svd, publish_vc, rec, &s_in[b][0][tid]);
         if constexpr (kScatter) {
           float4* r4 = reinterpret_cast<float4*>(p.rec) + 4 * (size_t)s;
           r4[0] = rec[0];
@@ -494,6 +569,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
         }
       }
     }
+    cp_async_wait<0>();
     __syncthreads();
   }
 }
@@ -625,10 +701,17 @@ __device__ __forceinline__ bool core_cell_index(int lc) {
 // Scatter step 2 (bin) for a CTA of T threads: every staged record is binned
 // by its current base cell among the 6^3 local cells (counting sort with
 // warp-aggregated counters); one whose stencil leaves the block deposits
-// straight to HBM.  Ends with a barrier after which cell[] holds exclusive
-// starts and idx[] the sorted record indices.
+// straight to HBM.  A binned record is rewritten in place in its deposit
+// form (deposit_item): with fx = x/dx - base and Bd = B dx (columns Bdx,
+// Bdy, Bdz for the x, y, z node offsets), the momentum the node of offset
+// (i, j, k) receives per unit weight is q000 + i Bdx + j Bdy + k Bdz, where
+// q000 = m v - fx0 Bdx - fx1 Bdy - fx2 Bdz (the reference's m v + B d with
+// d = ((i, j, k) - fx) dx regrouped):
+//   (m, q000), (Bdx, Bdy.x), (Bdy.y, Bdy.z, Bdz.x, Bdz.y), (Bdz.z, fx).
+// Ends with a barrier after which cell[] holds exclusive starts and idx[]
+// the sorted record indices.
 template <int T>
-__device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bool live, const ItemFrame& f,
+__device__ __forceinline__ void bin_item(float4* stage, uint32_t count, bool live, const ItemFrame& f,
                                          ScatterShared& ss) {
   constexpr int kRounds = (kStageMax + T - 1) / T;
   const uint32_t lane = threadIdx.x & 31u;
@@ -640,11 +723,25 @@ __device__ __forceinline__ void bin_item(const float4* stage, uint32_t count, bo
     if (live && j < count) {
       const float4 r0 = stage_chunk(stage, j, 0);
       if (r0.w != 0.f) {
-        const int lx = (int)floorf((r0.x - f.ox) * f.inv_dx - 0.5f) - f.wx - f.rx;
-        const int ly = (int)floorf((r0.y - f.oy) * f.inv_dx - 0.5f) - f.wy - f.ry;
-        const int lz = (int)floorf((r0.z - f.oz) * f.inv_dx - 0.5f) - f.wz - f.rz;
+        const float xp[3] = {(r0.x - f.ox) * f.inv_dx, (r0.y - f.oy) * f.inv_dx, (r0.z - f.oz) * f.inv_dx};
+        const float bx = floorf(xp[0] - 0.5f), by = floorf(xp[1] - 0.5f), bz = floorf(xp[2] - 0.5f);
+        const int lx = (int)bx - f.wx - f.rx;
+        const int ly = (int)by - f.wy - f.ry;
+        const int lz = (int)bz - f.wz - f.rz;
         if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
           lc = (uint32_t)(lx + 6 * (ly + 6 * lz));
+          const float4 r1 = stage_chunk(stage, j, 1), r2 = stage_chunk(stage, j, 2), r3 = stage_chunk(stage, j, 3);
+          const float fx0 = xp[0] - bx, fx1 = xp[1] - by, fx2 = xp[2] - bz;
+          const float dx = f.dx;
+          const float bdx[3] = {r1.w * dx, r2.x * dx, r2.y * dx};
+          const float bdy[3] = {r2.z * dx, r2.w * dx, r3.x * dx};
+          const float bdz[3] = {r3.y * dx, r3.z * dx, r3.w * dx};
+          const float q[3] = {r1.x - fx0 * bdx[0] - fx1 * bdy[0] - fx2 * bdz[0],
+                              r1.y - fx0 * bdx[1] - fx1 * bdy[1] - fx2 * bdz[1],
+                              r1.z - fx0 * bdx[2] - fx1 * bdy[2] - fx2 * bdz[2]};
+          const float4 t[4] = {make_float4(r0.w, q[0], q[1], q[2]), make_float4(bdx[0], bdx[1], bdx[2], bdy[0]),
+                               make_float4(bdy[1], bdy[2], bdz[0], bdz[1]), make_float4(bdz[2], fx0, fx1, fx2)};
+          stage_store(stage, j, t);
         } else {
           deposit_global(r0, stage_chunk(stage, j, 1), stage_chunk(stage, j, 2), stage_chunk(stage, j, 3), f.acc,
                          f.touched, f.sc, f.tile_slot);
@@ -723,47 +820,51 @@ __device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t*
   const uint32_t total = ss.total;
   // per node of the slab: (p.x, p.y) and (p.z, m), accumulated in pairs
   float2 axy[9], azm[9];
-  // Accumulates slab `slab` of the particles of local cell lc in registers;
-  // returns whether it had any.
+  // Accumulates slab `slab` of the particles of local cell lc in registers
+  // from their deposit-form records (bin_item); returns whether it had any.
+  // Node (slab, j, k) gets w_slab(fx0) w_j(fx1) w_k(fx2) (m, q000 + slab Bdx +
+  // j Bdy + k Bdz), the sums over j and k taken as running increments.
   auto accumulate = [&](int lc, int slab) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) axy[q] = azm[q] = make_float2(0.f, 0.f);
+    // the slab's B-spline weight of t = fx0 - shift: 0.5 (1.5 - fx)^2,
+    // 0.75 - (fx - 1)^2, 0.5 (fx - 0.5)^2
+    const float shift = 1.5f - 0.5f * (float)slab;
+    const bool mid = slab == 1;
+    const float fslab = (float)slab;
     const uint32_t first = ss.cell[lc], end = lc == kLocalCells - 1 ? total : ss.cell[lc + 1];
     for (uint32_t t = first; t < end; ++t) {
       const uint32_t j = ss.idx[t];
-      const float4 r0 = stage_chunk(stage, j, 0), r1 = stage_chunk(stage, j, 1), r2 = stage_chunk(stage, j, 2),
-                   r3 = stage_chunk(stage, j, 3);
-      const float mass = r0.w;
-      const float B[9] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
-      const float xp[3] = {(r0.x - f.ox) * f.inv_dx, (r0.y - f.oy) * f.inv_dx, (r0.z - f.oz) * f.inv_dx};
-      float wgt[3][3], fx[3];
+      const float4 c0 = stage_chunk(stage, j, 0), c1 = stage_chunk(stage, j, 1), c2 = stage_chunk(stage, j, 2),
+                   c3 = stage_chunk(stage, j, 3);
+      const float ts = c3.y - shift;
+      const float wi = mid ? fmaf(-ts, ts, 0.75f) : 0.5f * ts * ts;
+      float wy[3], wz[3];
+      quad_weights(c3.z, wy);
+      quad_weights(c3.w, wz);
+      // momentum at node (slab, 0, 0), paired with the mass: (q.x, q.y), (q.z, m)
+      float2 qxy = make_float2(fmaf(fslab, c1.x, c0.y), fmaf(fslab, c1.y, c0.z));
+      float2 qzm = make_float2(fmaf(fslab, c1.z, c0.w), c0.x);
+      const float2 dyxy = make_float2(c1.w, c2.x), dzxy = make_float2(c2.z, c2.w);
+      const float dyz = c2.y, dzz = c3.x;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float bf = floorf(xp[a] - 0.5f);
-        fx[a] = xp[a] - bf;
-        quad_weights(fx[a], wgt[a]);
-      }
-      // slab i of the stencil: x offset i, all (j, k)
-      const float wi = slab == 0 ? wgt[0][0] : (slab == 1 ? wgt[0][1] : wgt[0][2]);
-      const float di = ((float)slab - fx[0]) * f.dx;
-      const float qx[3] = {r1.x + B[0] * di, r1.y + B[1] * di, r1.z + B[2] * di};
-      const float dks[3] = {-fx[2] * f.dx, (1.0f - fx[2]) * f.dx, (2.0f - fx[2]) * f.dx};
-      const float2 b67 = make_float2(B[6], B[7]);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const float wij = wi * wgt[1][j];
-        const float dj = ((float)j - fx[1]) * f.dx;
-        const float2 qy01 = make_float2(qx[0] + B[3] * dj, qx[1] + B[4] * dj);
-        const float qy2 = qx[2] + B[5] * dj;
+      for (int jj = 0; jj < 3; ++jj) {
+        if (jj) {
+          qxy = add2(qxy, dyxy);
+          qzm.x += dyz;
+        }
+        const float wij = wi * wy[jj];
+        float2 cxy = qxy, czm = qzm;
 #pragma unroll
         for (int kk = 0; kk < 3; ++kk) {
-          const float wt = wij * wgt[2][kk];
-          const float dk = dks[kk];
+          if (kk) {
+            cxy = add2(cxy, dzxy);
+            czm.x += dzz;
+          }
+          const float wt = wij * wz[kk];
           const float2 w2 = make_float2(wt, wt);
-          const float2 q01 = fma2(b67, make_float2(dk, dk), qy01);
-          const float2 q2m = make_float2(qy2 + B[8] * dk, mass);
-          axy[3 * j + kk] = fma2(w2, q01, axy[3 * j + kk]);
-          azm[3 * j + kk] = fma2(w2, q2m, azm[3 * j + kk]);
+          axy[3 * jj + kk] = fma2(w2, cxy, axy[3 * jj + kk]);
+          azm[3 * jj + kk] = fma2(w2, czm, azm[3 * jj + kk]);
         }
       }
     }

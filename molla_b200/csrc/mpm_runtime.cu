@@ -1328,6 +1328,12 @@ void Group::status(uint32_t sid, mpm_status_info* out, cudaStream_t st) {
   out->active_tiles = s.tile_cap ? std::min(w[3], s.tile_cap) : 0u;
 }
 
+void Group::status_words(std::vector<uint32_t>& out, cudaStream_t st) {
+  out.resize((size_t)max_scenes * kStatusWords);
+  MPM_CK(cudaMemcpyAsync(out.data(), status_d.ptr, out.size() * 4, cudaMemcpyDeviceToHost, st));
+  MPM_CK(cudaStreamSynchronize(st));
+}
+
 void Group::reset_status(uint32_t sid, cudaStream_t st) {
   MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, st));
   MPM_CK(cudaStreamSynchronize(st));

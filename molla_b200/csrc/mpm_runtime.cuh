@@ -355,6 +355,8 @@ class Group {
   void read_grid(uint32_t sid, float* mass, float* mom, cudaStream_t st);
   void totals(uint32_t sid, double* out8, cudaStream_t st);
   void status(uint32_t sid, mpm_status_info* out, cudaStream_t st);
+  // Status words of every scene slot (kStatusWords each) in one copy.
+  void status_words(std::vector<uint32_t>& out, cudaStream_t st);
   void reset_status(uint32_t sid, cudaStream_t st);
   // (key, identity) order of one scene's particles (reference permutation).
   void sort_permutation(uint32_t sid, uint32_t* keys, uint32_t* ids, uint32_t capacity, cudaStream_t st);

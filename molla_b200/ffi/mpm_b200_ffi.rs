@@ -135,7 +135,7 @@ pub struct mpm_server_stats {
     pub admitted: u64, pub completed: u64, pub resident_scenes: u64, pub resident_bytes: u64,
     pub particle_steps: u64,
     pub tick_ms_p50: f64, pub tick_ms_p99: f64, pub queue_ms_p50: f64, pub queue_ms_p99: f64,
-    pub admit_ms: f64, pub step_ms: f64, pub retire_ms: f64, pub ticks: u64,
+    pub admit_ms: f64, pub step_ms: f64, pub retire_ms: f64, pub ticks: u64, pub faulted: u64,
 }
 #[repr(C)] pub struct mpm_sim64 { _p: [u8; 0] }
 #[repr(C)] #[derive(Clone, Copy, Default)]
@@ -194,6 +194,7 @@ extern "C" {
     pub fn mpm_server_poll(s: *mut mpm_server, ticket: u64, state: *mut u32, positions_out: *mut f32,
                            cap: u32, count: *mut u32) -> c_int;
     pub fn mpm_server_stats_get(s: *mut mpm_server, out: *mut mpm_server_stats) -> c_int;
+    pub fn mpm_server_ticket_status(s: *mut mpm_server, ticket: u64, out: *mut mpm_status_info) -> c_int;
     // all-FP64 state and grid (precision studies)
     pub fn mpm_sim64_create(e: *mut mpm_engine, cfg: *const mpm_config, out: *mut *mut mpm_sim64) -> c_int;
     pub fn mpm_sim64_destroy(s: *mut mpm_sim64) -> c_int;

@@ -242,6 +242,42 @@ def test_server_mixed_precision_exact_budgets(engine):
         assert np.abs(pos - alone_prec(engine, s, n, p)).max() < TOL, (n, p)
 
 
+def test_server_retires_faulted_request(engine):
+    """A served request whose state is not finite (one NaN position) latches
+    the numerical fault on its first substep and stands frozen on the
+    device; the server retires it at the next tick as faulted (state 3) with
+    its frozen positions and fault bits, counts only the substeps it
+    completed, and the requests served beside it finish normally
+    (mpm.wgsl:217-231 latch; MpmActiveGridStats, mpm.rs:257-283)."""
+    ss = small_scenes()
+    bad = ss[0]
+    pos_bad = bad.positions.copy()
+    pos_bad[7, 1] = np.nan
+    srv = m.MpmServer(engine, hbm_budget_bytes=64 << 20, max_scenes=8)
+    tb = srv.submit(m.config_for_scene(bad), bad.rows, pos_bad, bad.ids, bad.dt, 200)
+    good = [srv.submit(m.config_for_scene(s), s.rows, s.positions, s.ids, s.dt, 40) for s in ss[1:3]]
+    srv.run(1, substeps_per_tick=16)
+    # retired at the first tick that sees the latch, not after its 200 substeps
+    state, pos = srv.poll(tb)
+    st = srv.ticket_status(tb)
+    assert state == 3 and st.numerical_fault and st.faulted(), (state, st)
+    assert st.completed_substeps <= 1, st.completed_substeps
+    # frozen where the latch caught it (at most one substep of free fall)
+    assert np.isnan(pos[7, 1]) and np.allclose(pos, pos_bad, rtol=0, atol=1e-5, equal_nan=True)
+    for _ in range(10):
+        srv.run(1, substeps_per_tick=16)
+        if all(srv.poll(t)[0] == 2 for t in good):
+            break
+    for t, s in zip(good, ss[1:3]):
+        state_g, pos_g = srv.poll(t)
+        assert state_g == 2 and srv.ticket_status(t).completed_substeps == 40
+        assert np.abs(pos_g - alone(engine, s, 40)).max() < TOL
+    stats = srv.stats()
+    assert stats["faulted"] == 1 and stats["completed"] == 2
+    assert stats["particle_steps"] == bad.n * st.completed_substeps + 40 * sum(s.n for s in ss[1:3])
+    srv.close()
+
+
 def test_retired_scenes_leave_at_the_next_regroup(engine):
     """Retirement through the server does not regroup the pool: the
     remaining scenes keep stepping (and match their alone runs) while the
