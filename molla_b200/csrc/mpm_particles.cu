@@ -171,14 +171,24 @@ constexpr int kStagedInputs = 16;
 static_assert(PY == PX + 1 && PZ == PX + 2 && MASS == F0 + 9 && VOL == F0 + 10 && JP == F0 + 11,
               "the staged planes are two runs of consecutive planes");
 
+// The CTA-uniform values of the item a gather CTA is on, kept in shared
+// memory so that they hold no registers through the particle computation:
+// the scene's status word, the 8^3 velocity block origin, whether this
+// substep publishes v and C, and the item's slot range.
+struct GatherCtx {
+  uint32_t* status;
+  int rx, ry, rz;
+  uint32_t publish_vc;
+  uint32_t start, count;
+};
+
 // `in` (kStagedInputs entries kGatherThreads apart, or null) holds the
 // particle's inputs in the order of kStagedPlanes, copied to shared memory
 // ahead of time (k_g2p); null reads them from the pool.
 template <int MODE, bool WRITE_KEYS, class SR>
-__device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, uint32_t* status,
-                                              const float4* __restrict__ vblock, float* fallback, int rx, int ry,
-                                              int rz, int n, SR stol, int sweeps, int reuse_svd, bool publish_vc,
-                                              float4 (&rec)[4], const float* __restrict__ in = nullptr) {
+__device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, const GatherCtx& ctx,
+                                              const float4* __restrict__ vblock, float* fallback, SR stol, int sweeps,
+                                              int reuse_svd, float4 (&rec)[4], const float* __restrict__ in = nullptr) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   float x, y, z, F[9], jp, mass, vol;
@@ -216,7 +226,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 #pragma unroll
     for (int a = 0; a < 3; ++a) nf = nf_acc(nf, xp[a]);
     if (!nf_ok(nf)) {
-      atomicOr(status, kFaultNumerical);
+      atomicOr(ctx.status, kFaultNumerical);
       ok = false;
     }
     if (ok) {
@@ -232,7 +242,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 #pragma unroll
         for (int i = 0; i < 3; ++i) d[a][i] = ((float)i - fx) * sc.dx;
       }
-      const int lx0 = base[0] - rx, ly0 = base[1] - ry, lz0 = base[2] - rz;
+      const int lx0 = base[0] - ctx.rx, ly0 = base[1] - ctx.ry, lz0 = base[2] - ctx.rz;
       const bool inside = (unsigned)lx0 <= (unsigned)(kRegion - 3) && (unsigned)ly0 <= (unsigned)(kRegion - 3) &&
                           (unsigned)lz0 <= (unsigned)(kRegion - 3);
       // Separable accumulation: v = sum w gv; G = sum (w gv) d^T.
@@ -308,7 +318,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 #pragma unroll
       for (int i = 0; i < 9; ++i) nf2 = nf_acc(nf2, C[i]);
       if (!nf_ok(nf2)) {
-        atomicOr(status, kFaultNumerical);
+        atomicOr(ctx.status, kFaultNumerical);
         ok = false;
       }
       if (ok) {
@@ -327,7 +337,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 #pragma unroll
         for (int i = 0; i < 9; ++i) nf3 = nf_acc(nf3, Fn[i]);
         if (!nf_ok(nf3)) {
-          atomicOr(status, kFaultNumerical);
+          atomicOr(ctx.status, kFaultNumerical);
           ok = false;
         } else {
           x = np[0];
@@ -377,11 +387,11 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
               }
               jp = jp_new;
             } else {
-              atomicOr(status, kFaultNumerical);
+              atomicOr(ctx.status, kFaultNumerical);
               ok = false;
             }
           } else {
-            atomicOr(status, kFaultNumerical);
+            atomicOr(ctx.status, kFaultNumerical);
             ok = false;
           }
           // G2P results are published even when the return mapping
@@ -395,7 +405,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
           plane(p, PX)[s] = x;
           plane(p, PY)[s] = y;
           plane(p, PZ)[s] = z;
-          if (!kScatter || !ok || publish_vc) {
+          if (!kScatter || !ok || ctx.publish_vc) {
             plane(p, VX)[s] = v[0];
             plane(p, VY)[s] = v[1];
             plane(p, VZ)[s] = v[2];
@@ -424,7 +434,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 #pragma unroll
     for (int i = 0; i < 9; ++i) fin = fin && finitef(F[i]) && finitef(C[i]);
     if (!fin) {
-      atomicOr(status, kFaultNumerical);
+      atomicOr(ctx.status, kFaultNumerical);
       ok = false;
     }
   }
@@ -481,6 +491,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
   __shared__ __align__(16) SceneDev s_sc;
   __shared__ __align__(16) SharedGather s_gath;
   __shared__ uint32_t s_fault;
+  __shared__ GatherCtx s_ctx;
   // Particle inputs of this round and the next (cp.async double buffer):
   // [buffer][input][thread], the inputs in kStagedPlanes order.
   __shared__ __align__(16) float s_in[2][kStagedInputs][kGatherThreads];
@@ -497,9 +508,9 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
     // this one, and those of its first are requested here, so that their
     // loads overlap the velocity block's.
     const uint32_t tid = threadIdx.x;
-    auto fetch = [&](uint32_t k, int b) {
-      if (k < item.count) {
-        const uint32_t s = item.start + k;
+    auto fetch = [&](uint32_t k, int b, uint32_t start, uint32_t count) {
+      if (k < count) {
+        const uint32_t s = start + k;
         // walk the planes with one pointer: PX..PZ, then F0..JP
         const size_t cap = p.cap;
         const float* src = p.planes + s;
@@ -512,7 +523,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
       }
       cp_async_commit();
     };
-    fetch(tid, 0);
+    fetch(tid, 0, item.start, item.count);
     // The scene record goes to shared memory when the item's scene differs
     // from the last item's (consecutive items of a CTA mostly share one):
     // the velocity staging below reads the geometry from there, so a new
@@ -525,14 +536,15 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
       __syncthreads();
     }
     const SceneDev& sc = s_sc;
-    uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
-    // a latched fault, a spent substep budget or a retired scene: stand still
-    const uint32_t fault0 = (scene_frozen(status) || !sc.live) ? 1u : 0u;
-    const bool publish_vc = budget_ends(status);
     const uint32_t w = sc.w;
     const uint32_t tx = item.tile % w, ty = (item.tile / w) % w, tz = item.tile / (w * w);
     const int rx = 4 * (int)tx - 1, ry = 4 * (int)ty - 1, rz = 4 * (int)tz - 1;
-    const int n = (int)sc.n;
+    if (threadIdx.x == 0) {
+      uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
+      // a latched fault, a spent substep budget or a retired scene: stand still
+      s_fault = (scene_frozen(status) || !sc.live) ? 1u : 0u;
+      s_ctx = GatherCtx{status, rx, ry, rz, budget_ends(status) ? 1u : 0u, item.start, item.count};
+    }
     if constexpr (kGather) {
       // Stage the 8^3-node velocity block (out-of-grid nodes read as zero),
       // the four loads of a thread in flight together.
@@ -548,18 +560,17 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
 #pragma unroll
       for (int q = 0; q < kPer; ++q) s_gath.vel[(int)threadIdx.x + q * kGatherThreads] = g[q];
     }
-    if (threadIdx.x == 0) s_fault = fault0;
     __syncthreads();
     const bool faulted = s_fault != 0;
     if (!faulted) {
       int b = 0;
-      for (uint32_t k = tid; k < item.count; k += kGatherThreads, b ^= 1) {
-        fetch(k + kGatherThreads, b ^ 1);
+      for (uint32_t k = tid; k < s_ctx.count; k += kGatherThreads, b ^= 1) {
+        fetch(k + kGatherThreads, b ^ 1, s_ctx.start, s_ctx.count);
         cp_async_wait<1>();
-        const uint32_t s = item.start + k;
+        const uint32_t s = s_ctx.start + k;
         float4 rec[4];
-        particle_step<MODE, WRITE_KEYS, SR>(p, sc, s, status, s_gath.vel, s_gath.fallback[threadIdx.x], rx, ry, rz, n,
-                                            stol, sweeps, reuse_svd, publish_vc, rec, &s_in[b][0][tid]);
+        particle_step<MODE, WRITE_KEYS, SR>(p, sc, s, s_ctx, s_gath.vel, s_gath.fallback[threadIdx.x], stol, sweeps,
+                                            reuse_svd, rec, &s_in[b][0][tid]);
         if constexpr (kScatter) {
           float4* r4 = reinterpret_cast<float4*>(p.rec) + 4 * (size_t)s;
           r4[0] = rec[0];
@@ -1028,6 +1039,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
   __shared__ __align__(16) float4 s_vel[kRegionNodes];
   __shared__ ScatterShared ss;
   __shared__ uint32_t s_fault;
+  __shared__ GatherCtx s_ctx;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
   // this SVD form's range of the work list: FP32-SVD items, then FP64-SVD items
@@ -1059,6 +1071,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
     }
     if (threadIdx.x == 0) {
       s_fault = fault0;
+      s_ctx = GatherCtx{status, f.rx, f.ry, f.rz, publish_vc ? 1u : 0u, item.start, item.count};
       if (!fits) atomicOr(status, kFaultDeviceWait);
     }
     __syncthreads();
@@ -1067,9 +1080,9 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
       for (uint32_t k = threadIdx.x; k < item.count; k += kFusedThreads) {
         float4 rec[4];
         // the record's own stage slot is the scratch of gather_global
-        particle_step<kG2PRecord, WRITE_KEYS, SR>(p, s_sc, item.start + k, status, s_vel,
-                                                  reinterpret_cast<float*>(s_stage + 4 * (size_t)k), f.rx, f.ry,
-                                                  f.rz, f.n, stol, sweeps, reuse_svd, publish_vc, rec);
+        particle_step<kG2PRecord, WRITE_KEYS, SR>(p, s_sc, item.start + k, s_ctx, s_vel,
+                                                  reinterpret_cast<float*>(s_stage + 4 * (size_t)k), stol, sweeps,
+                                                  reuse_svd, rec);
         stage_store(s_stage, k, rec);
       }
     }
