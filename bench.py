@@ -60,8 +60,8 @@ KERNEL_BYTES = {
 # substep on the medium workload (128^3 grid, 2M particles, substep ~250),
 # scaled by particle count.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "GridToParticle": 156.6,
-    "ParticleToGrid": 69.1,
+    "GridToParticle": 156.4,
+    "ParticleToGrid": 70.9,
 }
 # The fused gather + scatter (k_g2p2g, groups of at most 256k particles)
 # keeps the 64-byte record in shared memory: 180 - 64 B per particle, and per
