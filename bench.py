@@ -849,7 +849,9 @@ def measure_served(args, quiet=False):
         "queue_ms_p50": st["queue_ms_p50"], "queue_ms_p99": st["queue_ms_p99"],
         "submitted": submitted, "refused": refused, "admitted": st["admitted"], "completed": st["completed"],
         "resident_scenes": st["resident_scenes"], "resident_bytes": st["resident_bytes"],
-        "ticks": st["ticks"], "host_ms": {"admit": st["admit_ms"], "step": st["step_ms"], "retire": st["retire_ms"]},
+        "ticks": st["ticks"], "host_ms": {"admit": st["admit_ms"], "step": st["step_ms"], "retire": st["retire_ms"],
+                                          "graph_build": st["graph_build_ms"]},
+        "graph_builds": st["graph_builds"], "faulted": st["faulted"],
     }
 
 

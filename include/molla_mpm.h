@@ -573,6 +573,12 @@ typedef struct mpm_server_stats {
   /* requests retired as faulted (their particle_steps count only the
    * substeps completed before the fault) */
   uint64_t faulted;
+  /* tick graphs captured (a new tick shape, or a layout change since the
+   * graph was made) and the host milliseconds spent capturing and
+   * instantiating or updating them; the tick latencies above time the
+   * graph launches alone */
+  uint64_t graph_builds;
+  double graph_build_ms;
 } mpm_server_stats;
 MPM_API int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out);
 /* Device status of a finished (done or faulted) request, as it stood when it

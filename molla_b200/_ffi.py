@@ -87,6 +87,8 @@ class mpm_server_stats(C.Structure):
         ("retire_ms", C.c_double),
         ("ticks", C.c_uint64),
         ("faulted", C.c_uint64),
+        ("graph_builds", C.c_uint64),
+        ("graph_build_ms", C.c_double),
     ]
 
 

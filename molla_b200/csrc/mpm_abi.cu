@@ -1470,9 +1470,9 @@ int mpm_server_run(mpm_server* server, uint32_t ticks, uint32_t substeps_per_tic
         if (server->queue.empty()) break;
         continue;
       }
-      MPM_CK(cudaEventRecord(*server->e0, st));
-      g.step_graph(len, 1, st);
-      MPM_CK(cudaEventRecord(*server->e1, st));
+      // the tick's events bracket its graph launch alone: a capture or
+      // update of the graph before it is host time (graph_build_ms)
+      g.step_graph(len, 1, st, *server->e0, *server->e1);
       // The tick runs on the GPU while the caller goes on (submitting
       // requests); the next run, poll or stats call completes it.
       server->in_flight = true;
@@ -1835,6 +1835,8 @@ int mpm_server_stats_get(mpm_server* server, mpm_server_stats* out) {
     out->retire_ms = server->retire_ms;
     out->ticks = server->ticks;
     out->faulted = server->faulted;
+    out->graph_builds = server->g->graph_builds;
+    out->graph_build_ms = server->g->graph_build_ms;
   });
 }
 

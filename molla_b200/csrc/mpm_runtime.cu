@@ -1,6 +1,8 @@
 // mpm_runtime.cu — host runtime of the B200 MPM path.
 #include "mpm_runtime.cuh"
 
+#include <chrono>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -1150,7 +1152,8 @@ Group::GraphKey Group::graph_key(uint32_t substeps) const {
   return k;
 }
 
-void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
+void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st, cudaEvent_t ev_begin,
+                       cudaEvent_t ev_end) {
   eng->check();
   if (substeps && repeat && n_live == n_retiring) compact(st);
   if (!substeps || n_live == 0 || n_live == n_retiring || !repeat) return;
@@ -1164,6 +1167,7 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
     auto it = graphs.find(key);
     Graph g;
     if (it == graphs.end() || it->second.epoch != epoch) {
+      const auto t_build0 = std::chrono::steady_clock::now();
       const uint64_t saved = eng->launches;
       cudaGraph_t graph = nullptr;
       MPM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -1180,7 +1184,29 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
       MPM_CK(cudaStreamEndCapture(st, &graph));
       g.kernels = eng->launches - saved;
       eng->launches = saved;
-      MPM_CK(cudaGraphInstantiate(&g.exec, graph, 0));
+      // A layout change (a scene added or retired, a regrouping moved)
+      // mostly changes launch parameters, not the sequence: update the
+      // existing executable graph in place when the topology allows, which
+      // costs far less host time than instantiating a new one.
+      bool updated = false;
+      if (it != graphs.end() && it->second.exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(it->second.exec, graph, &info) == cudaSuccess) {
+          g.exec = it->second.exec;
+          updated = true;
+        } else {
+          (void)cudaGetLastError();  // the failed update is not a sticky error
+          cudaGraphExecDestroy(it->second.exec);
+          it->second.exec = nullptr;
+        }
+      }
+      if (!updated) {
+        const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        if (ie != cudaSuccess) {
+          cudaGraphDestroy(graph);
+          MPM_CK(ie);
+        }
+      }
       cudaGraphDestroy(graph);
       g.epoch = epoch;
       // run_substeps advanced the host bookkeeping; rewind it, the launch
@@ -1193,12 +1219,16 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st) {
       regroups = regroups0;
       compact_issued = false;
       substeps_done -= substeps;
-      if (it != graphs.end() && it->second.exec) cudaGraphExecDestroy(it->second.exec);
       graphs[key] = g;
+      ++graph_builds;
+      graph_build_ms +=
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_build0).count();
     } else {
       g = it->second;
     }
+    if (ev_begin && r == 0) MPM_CK(cudaEventRecord(ev_begin, st));
     MPM_CK(cudaGraphLaunch(g.exec, st));
+    if (ev_end && r + 1 == repeat) MPM_CK(cudaEventRecord(ev_end, st));
     eng->launches += g.kernels;
     // Replay the host-side state transition of the captured sequence (the
     // same decisions run_substeps made while it was captured).

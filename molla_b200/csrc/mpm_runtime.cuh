@@ -333,7 +333,15 @@ class Group {
   // Enqueue `substeps` substeps of every live scene on `st`.
   void step(uint32_t substeps, cudaStream_t st);
   // Same through a cached CUDA graph.
-  void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st);
+  // ev_begin / ev_end (optional) are recorded right before the first graph
+  // launch and after the last, so that they time the device work alone
+  // (not a capture that precedes it).
+  void step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st, cudaEvent_t ev_begin = nullptr,
+                  cudaEvent_t ev_end = nullptr);
+  // graphs captured (and host milliseconds spent capturing and instantiating
+  // or updating them) since creation
+  uint64_t graph_builds = 0;
+  double graph_build_ms = 0.0;
   void regroup(bool compute_keys, cudaStream_t st, bool move_records = false);
   // Grid update of accumulator a, then the semi-implicit Jacobi sweeps of
   // the scenes that ask for them.

@@ -136,6 +136,7 @@ pub struct mpm_server_stats {
     pub particle_steps: u64,
     pub tick_ms_p50: f64, pub tick_ms_p99: f64, pub queue_ms_p50: f64, pub queue_ms_p99: f64,
     pub admit_ms: f64, pub step_ms: f64, pub retire_ms: f64, pub ticks: u64, pub faulted: u64,
+    pub graph_builds: u64, pub graph_build_ms: f64,
 }
 #[repr(C)] pub struct mpm_sim64 { _p: [u8; 0] }
 #[repr(C)] #[derive(Clone, Copy, Default)]
