@@ -496,17 +496,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
   return o;
 }
 
-// Two independent FP32 products / sums in one instruction (sm_100
-// mul.rn.f32x2, add.rn.f32x2), each rounded once as __fmul_rn / __fadd_rn.
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-  uint64_t ua, ub, r;
-  memcpy(&ua, &a, 8);
-  memcpy(&ub, &b, 8);
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(ua), "l"(ub));
-  float2 o;
-  memcpy(&o, &r, 8);
-  return o;
-}
+// Two independent FP32 sums in one instruction (sm_100 add.rn.f32x2), each
+// rounded once as __fadd_rn.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) {
   uint64_t ua, ub, r;
   memcpy(&ua, &a, 8);
