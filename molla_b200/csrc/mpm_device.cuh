@@ -145,6 +145,11 @@ struct PoolDev {
   uint32_t* tile_slot;
   uint32_t* slot_tile;
   uint8_t* tile_mark;
+  // Item counters of the persistent particle kernels (0: gather, 1:
+  // scatter), zeroed before each launch: a CTA takes its first item by its
+  // index and every later one from the counter, so the items spread over
+  // the CTAs by finishing order rather than by a fixed stride.
+  uint32_t* work;
 };
 
 __device__ __forceinline__ float* plane(const PoolDev& p, int k) { return p.planes + (size_t)k * p.cap; }

@@ -492,6 +492,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
   __shared__ __align__(16) SharedGather s_gath;
   __shared__ uint32_t s_fault;
   __shared__ GatherCtx s_ctx;
+  __shared__ uint32_t s_it_next;
   // Particle inputs of this round and the next (cp.async double buffer):
   // [buffer][input][thread], the inputs in kStagedPlanes order.
   __shared__ __align__(16) float s_in[2][kStagedInputs][kGatherThreads];
@@ -501,8 +502,10 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
   const uint32_t it_hi = sizeof(SR) == 8 ? n32 + p.n_items[1] : n32;
   const SR stol = (SR)tol;
   uint32_t s_sc_scene = 0xffffffffu;  // scene whose record s_sc holds
-  for (uint32_t it = it_lo + blockIdx.x; it < it_hi; it += gridDim.x) {
+  for (uint32_t it = it_lo + blockIdx.x; it < it_hi;) {
     const Item item = p.items[item_slot(p, n32, it)];
+    // this CTA's next item, taken now and read by all after the item's work
+    if (threadIdx.x == 0) s_it_next = it_lo + gridDim.x + atomicAdd(p.work, 1u);
     // A thread's particles come kGatherThreads apart; the inputs of its
     // next particle are copied to shared memory (cp.async) while it computes
     // this one, and those of its first are requested here, so that their
@@ -581,7 +584,11 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
       }
     }
     cp_async_wait<0>();
+    // s_it_next was published by the barrier after the staging; thread 0
+    // overwrites it only after the barrier below
+    const uint32_t next = s_it_next;
     __syncthreads();
+    it = next;
   }
 }
 
@@ -959,6 +966,7 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
       reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~static_cast<uintptr_t>(1023u));
   __shared__ ScatterShared ss;
   __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_it_next;
   float4* __restrict__ acc = p.acc[acc_out];
   uint8_t* __restrict__ touched = p.touched[acc_out];
   const uint32_t n32 = p.n_items[0];
@@ -985,7 +993,10 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
   };
   if (threadIdx.x == 0 && blockIdx.x < n_items) stage(blockIdx.x);
   uint32_t parity = 0;
-  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+  for (uint32_t it = blockIdx.x; it < n_items;) {
+    // this CTA's next item, taken now; its records are staged after this
+    // item's deposit
+    if (threadIdx.x == 0) s_it_next = gridDim.x + atomicAdd(p.work + 1, 1u);
     const uint32_t slot = item_slot(p, n32, it);
     const Item item = p.items[slot];
     const SceneDev* __restrict__ scp = p.scenes + item.scene;
@@ -1012,9 +1023,13 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
       return;
     }
     // Every thread is done with the stage: the next item's copy goes now.
-    if (threadIdx.x == 0 && it + gridDim.x < n_items) stage(it + gridDim.x);
+    // (s_it_next was published by the bin's barriers; thread 0 overwrites
+    // it only after the barrier below.)
+    const uint32_t next = s_it_next;
+    if (threadIdx.x == 0 && next < n_items) stage(next);
     flush_item<kScatterThreads>(f, ss);
     __syncthreads();
+    it = next;
   }
 }
 
@@ -1292,6 +1307,8 @@ __global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, cons
 
 template <int MODE, bool KEYS, class SR>
 static cudaError_t launch_gather_t(const PoolDev& p, double tol, int sweeps, int reuse, int grid, cudaStream_t st) {
+  const cudaError_t e = cudaMemsetAsync(p.work, 0, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
   k_g2p<MODE, KEYS, SR><<<grid, kGatherThreads, 0, st>>>(p, tol, sweeps, reuse);
   return cudaGetLastError();
 }
@@ -1394,6 +1411,8 @@ cudaError_t launch_selftest_wait(uint32_t* status, unsigned long long* waited_ns
 }
 
 cudaError_t launch_scatter(const PoolDev& p, const CUtensorMap& rec_map, int acc_out, int grid, cudaStream_t st) {
+  const cudaError_t e = cudaMemsetAsync(p.work + 1, 0, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
   k_p2g<<<grid, kScatterThreads, kStageBytes, st>>>(p, rec_map, acc_out);
   return cudaGetLastError();
 }

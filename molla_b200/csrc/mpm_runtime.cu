@@ -258,6 +258,7 @@ Group::Group(Engine* e, uint32_t max_scenes_, uint64_t particle_cap, uint64_t ce
   touched[1].alloc(cell_cap / kCellBlock);
   scenes_d.alloc(max_scenes);
   status_d.alloc((size_t)kStatusWords * max_scenes);
+  work_d.alloc(2);
   n_items.alloc(2);
   totals_d.alloc(8);
   MPM_CK(cudaMallocHost((void**)&scenes_h, sizeof(SceneDev) * max_scenes));
@@ -327,6 +328,7 @@ PoolDev Group::pool() const {
   p.tile_slot = tile_slot.ptr;
   p.slot_tile = slot_tile.ptr;
   p.tile_mark = tile_mark.ptr;
+  p.work = work_d.ptr;
   p.item_order = item_order.ptr;
   return p;
 }

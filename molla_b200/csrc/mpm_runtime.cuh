@@ -205,6 +205,7 @@ class Group {
   // last gather marked.
   DevBuf<uint32_t> tile_slot, slot_tile;
   DevBuf<uint8_t> tile_mark;
+  DevBuf<uint32_t> work_d;  // item counters of the gather and the scatter (PoolDev::work)
   bool any_sparse() const;
   void finalize_tiles(cudaStream_t st);
   DevBuf<Item> items;
