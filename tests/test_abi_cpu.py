@@ -49,6 +49,41 @@ def test_rust_binding_covers_every_declared_symbol():
     assert {k: v for k, v in bound.items() if arity[k] != v} == {}
 
 
+def header_structs():
+    """Field names, in order, of every `typedef struct X { ... } X;` of the
+    header (array fields by name)."""
+    hdr = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "molla_mpm.h").read_text(), flags=re.S)
+    out = {}
+    for name, body in re.findall(r"typedef struct (mpm_\w+)\s*\{(.*?)\}\s*\1\s*;", hdr, flags=re.S):
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            # "T a, b[3]" declares a and b: the last identifier of each part
+            for part in decl.split(","):
+                fields.append(re.findall(r"(\w+)\s*(?:\[[^\]]*\])?\s*$", part.strip())[0])
+        out[name] = fields
+    return out
+
+
+def test_struct_fields_match_across_header_ctypes_and_rust():
+    """Every struct of the header has the same fields in the same order in
+    the ctypes mirror (molla_b200/_ffi.py) and in the Rust #[repr(C)]
+    mirror (molla_b200/ffi/mpm_b200_ffi.rs), so that a field added to the
+    header cannot be left out of a binding."""
+    hdr = header_structs()
+    assert {"mpm_config", "mpm_rheology", "mpm_status_info", "mpm_server_stats", "mpm_shapes"} <= set(hdr)
+    src = re.sub(r"//[^\n]*", "", (ROOT / "molla_b200" / "ffi" / "mpm_b200_ffi.rs").read_text())
+    rust = {name: re.findall(r"pub (\w+)\s*:", body)
+            for name, body in re.findall(r"pub struct (mpm_\w+)\s*\{(.*?)\}", src, flags=re.S)}
+    for name, fields in hdr.items():
+        cls = getattr(_ffi, name, None)
+        if cls is not None:
+            assert [f[0] for f in cls._fields_] == fields, name
+        assert rust.get(name) == fields, (name, rust.get(name), fields)
+
+
 def test_abi_version_and_error_channel():
     L = _ffi.lib()
     assert L.mpm_abi_version() == 1
