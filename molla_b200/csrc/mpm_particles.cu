@@ -160,10 +160,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 }  // namespace
 
-// One particle of an item: G2P + F update + return mapping (MODE != kRecord)
-// and the scatter record (MODE != kG2P), returned in rec.  vblock is the
-// staged 8^3-node velocity block of the item's tile (origin node rx, ry, rz);
-// fallback is a 12-float shared-memory slot of this thread for gather_global.
 // The particle inputs the gather stages in shared memory, in order: the
 // position planes, the F planes, mass, volume and J_p (planes PX..PZ and
 // F0..JP in plane order), then the meta word.
@@ -182,9 +178,14 @@ struct GatherCtx {
   uint32_t start, count;
 };
 
-// `in` (kStagedInputs entries kGatherThreads apart, or null) holds the
-// particle's inputs in the order of kStagedPlanes, copied to shared memory
-// ahead of time (k_g2p); null reads them from the pool.
+// One particle of an item: G2P + F update + return mapping (MODE != kRecord)
+// and the scatter record (MODE != kG2P), returned in rec.  ctx holds the
+// item's uniform values; vblock is the staged 8^3-node velocity block of the
+// item's tile (origin node ctx.rx, ctx.ry, ctx.rz); fallback is a 12-float
+// shared-memory slot of this thread for gather_global.  `in` (kStagedInputs
+// words kGatherThreads apart, or null) holds the particle's inputs in the
+// staged order above, copied to shared memory ahead of time (k_g2p); null
+// reads them from the pool.
 template <int MODE, bool WRITE_KEYS, class SR>
 __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& sc, uint32_t s, const GatherCtx& ctx,
                                               const float4* __restrict__ vblock, float* fallback, SR stol, int sweeps,
@@ -494,7 +495,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
   __shared__ GatherCtx s_ctx;
   __shared__ uint32_t s_it_next;
   // Particle inputs of this round and the next (cp.async double buffer):
-  // [buffer][input][thread], the inputs in kStagedPlanes order.
+  // [buffer][input][thread], the inputs in the staged order.
   __shared__ __align__(16) float s_in[2][kStagedInputs][kGatherThreads];
   // this SVD form's range of the work list: FP32-SVD items, then FP64-SVD items
   const uint32_t n32 = p.n_items[0];
