@@ -833,7 +833,7 @@ __device__ __forceinline__ void bin_item(float4* stage, uint32_t count, bool liv
 // particles in registers and issues 9 x 4 shared-memory atomics for the whole
 // cell; no two lanes of a warp add to the same node.
 template <int T>
-__device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t* __restrict__ order, const ItemFrame& f,
+__device__ __forceinline__ void deposit_item(const float4* stage, const uint8_t* __restrict__ order,
                                              ScatterShared& ss) {
   static_assert(T >= 192, "the core cells take 6 warps of 10 cells x 3 slabs");
   const uint32_t total = ss.total;
@@ -1015,7 +1015,7 @@ __global__ void __launch_bounds__(kScatterThreads, 4) k_p2g(PoolDev p, const __g
     }
     const bool live = ok && fault0 == 0;
     bin_item<kScatterThreads>(s_stage, item.count, live, f, ss);
-    if (live) deposit_item<kScatterThreads>(s_stage, p.item_order + (size_t)slot * 64, f, ss);
+    if (live) deposit_item<kScatterThreads>(s_stage, p.item_order + (size_t)slot * 64, ss);
     if (__syncthreads_or(!ok)) {
       // The stage did not arrive (or the item exceeds the stage): report it,
       // wait once more (bounded) for the copy in flight and stop this CTA.
@@ -1104,7 +1104,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_g2p2g(PoolDev p, double to
     }
     __syncthreads();
     bin_item<kFusedThreads>(s_stage, item.count, live, f, ss);
-    if (live) deposit_item<kFusedThreads>(s_stage, p.item_order + (size_t)slot * 64, f, ss);
+    if (live) deposit_item<kFusedThreads>(s_stage, p.item_order + (size_t)slot * 64, ss);
     __syncthreads();
     flush_item<kFusedThreads>(f, ss);
     __syncthreads();
