@@ -230,6 +230,16 @@ __device__ __forceinline__ float nf_acc(float acc, float v) { return fmaf(0.0f, 
 __device__ __forceinline__ double nf_acc(double acc, double v) { return fma(0.0, v, acc); }
 __device__ __forceinline__ bool nf_ok(float acc) { return acc == 0.0f; }
 __device__ __forceinline__ bool nf_ok(double acc) { return acc == 0.0; }
+// The same test over N values folded into four independent accumulators, so
+// that the chain the final compare waits on is N/4 fused multiply-adds long
+// rather than N (the sum of the four is NaN exactly when one of them is).
+template <int N>
+__device__ __forceinline__ bool all_finite(const float (&v)[N]) {
+  float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int i = 0; i < N; ++i) a[i & 3] = nf_acc(a[i & 3], v[i]);
+  return nf_ok((a[0] + a[1]) + (a[2] + a[3]));
+}
 
 // ---------------------------------------------------------------------------
 // 3x3 helpers on register arrays, column-major a[3*col+row].
@@ -623,15 +633,15 @@ template <class T>
 __device__ __forceinline__ bool plasticity_project(SvdOut<T>& svd, const MatDev& md, float& jp, bool& changed) {
   float s[3] = {(float)svd.s[0], (float)svd.s[1], (float)svd.s[2]};
   {
-    float nf = 0.0f;
+    float chk[21];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) nf = nf_acc(nf, s[a]);
+    for (int a = 0; a < 3; ++a) chk[a] = s[a];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      nf = nf_acc(nf, svd.u[i]);
-      nf = nf_acc(nf, svd.v[i]);
+      chk[3 + 2 * i] = svd.u[i];
+      chk[4 + 2 * i] = svd.v[i];
     }
-    if (!nf_ok(nf)) return false;
+    if (!all_finite(chk)) return false;
   }
   T ns[3] = {svd.s[0], svd.s[1], svd.s[2]};
   float dq = 0.0f;

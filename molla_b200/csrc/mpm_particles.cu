@@ -221,12 +221,8 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
   if constexpr (kGather) {
     // ---- g2p (mpm.wgsl:1242-1353) ----
     const float xp[3] = {(x - sc.ox) * sc.inv_dx, (y - sc.oy) * sc.inv_dx, (z - sc.oz) * sc.inv_dx};
-    float nf = nf_acc(nf_acc(nf_acc(nf_acc(0.0f, x), y), z), jp);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) nf = nf_acc(nf, F[i]);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) nf = nf_acc(nf, xp[a]);
-    if (!nf_ok(nf)) {
+    const float chk[16] = {x, y, z, jp, F[0], F[1], F[2], F[3], F[4], F[5], F[6], F[7], F[8], xp[0], xp[1], xp[2]};
+    if (!all_finite(chk)) {
       atomicOr(ctx.status, kFaultNumerical);
       ok = false;
     }
@@ -313,12 +309,9 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         for (int i = 0; i < 9; ++i) C[i] *= md.afac;
       }
       float np[3] = {x + sc.dt * v[0], y + sc.dt * v[1], z + sc.dt * v[2]};
-      float nf2 = 0.0f;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) nf2 = nf_acc(nf_acc(nf2, np[a]), v[a]);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) nf2 = nf_acc(nf2, C[i]);
-      if (!nf_ok(nf2)) {
+      const float chk2[15] = {np[0], v[0], np[1], v[1], np[2], v[2], C[0], C[1], C[2],
+                              C[3],  C[4], C[5],  C[6], C[7],  C[8]};
+      if (!all_finite(chk2)) {
         atomicOr(ctx.status, kFaultNumerical);
         ok = false;
       }
@@ -334,10 +327,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
         for (int i = 0; i < 9; ++i) A[i] = sc.dt * C[i] + ((i % 4 == 0) ? 1.f : 0.f);
         float Fn[9];
         matmul(A, F, Fn);
-        float nf3 = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) nf3 = nf_acc(nf3, Fn[i]);
-        if (!nf_ok(nf3)) {
+        if (!all_finite(Fn)) {
           atomicOr(ctx.status, kFaultNumerical);
           ok = false;
         } else {
@@ -376,12 +366,7 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
                                   (svd.u[3 + r] * ds[1]) * svd.v[3 + c] + (svd.u[6 + r] * ds[2]) * svd.v[6 + c];
             }
             // the FP32 copy must be finite too (an FP64 value beyond FP32 range)
-            float nf4 = 0.0f;
-            if (rebuild) {
-#pragma unroll
-              for (int i = 0; i < 9; ++i) nf4 = nf_acc(nf4, (float)Fr[i]);
-            }
-            if (nf_ok(nf4)) {
+            if (!rebuild || all_finite(Fr)) {
               if (rebuild) {
 #pragma unroll
                 for (int i = 0; i < 9; ++i) F[i] = (float)Fr[i];
