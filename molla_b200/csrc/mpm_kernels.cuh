@@ -18,8 +18,10 @@ constexpr uint32_t kCellBlock = 256;  // grid pool granularity: one scene per 25
 
 enum GatherMode : int { kRecord = 0, kG2P = 1, kG2PRecord = 2 };
 
+// publish_all: the gather writes v and C for every particle (a call's last
+// substep), not only for scenes whose substep budget ends.
 cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
-                          int reuse, int grid, cudaStream_t st);
+                          int reuse, int grid, cudaStream_t st, bool publish_all = false);
 // The scatter stages its records with TMA through `rec_map`, a 2-D tensor
 // map of the record buffer (16 floats x cap, 64-byte swizzle) built by
 // make_record_map.

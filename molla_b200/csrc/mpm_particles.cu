@@ -471,7 +471,8 @@ __device__ __forceinline__ void particle_step(const PoolDev& p, const SceneDev& 
 // substep of a call), kG2PRecord (gather + return mapping + B for the next
 // scatter, with the return mapping's SVD reused).
 template <int MODE, bool WRITE_KEYS, class SR>
-__global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol, int sweeps, int reuse_svd) {
+__global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol, int sweeps, int reuse_svd,
+                                                            int publish_all) {
   constexpr bool kGather = MODE != kRecord;
   constexpr bool kScatter = MODE != kG2P;
   __shared__ __align__(16) SceneDev s_sc;
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(kGatherThreads, 5) k_g2p(PoolDev p, double tol
       uint32_t* status = p.status + (size_t)sc.status * kStatusWords;
       // a latched fault, a spent substep budget or a retired scene: stand still
       s_fault = (scene_frozen(status) || !sc.live) ? 1u : 0u;
-      s_ctx = GatherCtx{status, rx, ry, rz, budget_ends(status) ? 1u : 0u, item.start, item.count};
+      s_ctx = GatherCtx{status, rx, ry, rz, (publish_all || budget_ends(status)) ? 1u : 0u, item.start, item.count};
     }
     if constexpr (kGather) {
       // Stage the 8^3-node velocity block (out-of-grid nodes read as zero),
@@ -1292,23 +1293,24 @@ __global__ void k_combine_det(PoolDev p, const float4* __restrict__ blocks, cons
 // ---------------------------------------------------------------------------
 
 template <int MODE, bool KEYS, class SR>
-static cudaError_t launch_gather_t(const PoolDev& p, double tol, int sweeps, int reuse, int grid, cudaStream_t st) {
+static cudaError_t launch_gather_t(const PoolDev& p, double tol, int sweeps, int reuse, int grid, cudaStream_t st,
+                                   bool publish_all) {
   const cudaError_t e = cudaMemsetAsync(p.work, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  k_g2p<MODE, KEYS, SR><<<grid, kGatherThreads, 0, st>>>(p, tol, sweeps, reuse);
+  k_g2p<MODE, KEYS, SR><<<grid, kGatherThreads, 0, st>>>(p, tol, sweeps, reuse, publish_all ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_gather(int mode, bool write_keys, bool svd_fp64, const PoolDev& p, double tol, int sweeps,
-                          int reuse, int grid, cudaStream_t st) {
-#define MPM_DISPATCH(M)                                                                        \
-  if (mode == M) {                                                                             \
-    if (svd_fp64) {                                                                            \
-      return write_keys ? launch_gather_t<M, true, double>(p, tol, sweeps, reuse, grid, st)    \
-                        : launch_gather_t<M, false, double>(p, tol, sweeps, reuse, grid, st);  \
-    }                                                                                          \
-    return write_keys ? launch_gather_t<M, true, float>(p, tol, sweeps, reuse, grid, st)       \
-                      : launch_gather_t<M, false, float>(p, tol, sweeps, reuse, grid, st);     \
+                          int reuse, int grid, cudaStream_t st, bool publish_all) {
+#define MPM_DISPATCH(M)                                                                          \
+  if (mode == M) {                                                                               \
+    if (svd_fp64) {                                                                              \
+      return write_keys ? launch_gather_t<M, true, double>(p, tol, sweeps, reuse, grid, st, publish_all) \
+                        : launch_gather_t<M, false, double>(p, tol, sweeps, reuse, grid, st, publish_all); \
+    }                                                                                            \
+    return write_keys ? launch_gather_t<M, true, float>(p, tol, sweeps, reuse, grid, st, publish_all) \
+                      : launch_gather_t<M, false, float>(p, tol, sweeps, reuse, grid, st, publish_all); \
   }
   MPM_DISPATCH(kRecord)
   MPM_DISPATCH(kG2P)

@@ -396,6 +396,7 @@ void Group::sync_scenes(cudaStream_t st) {
 uint32_t Group::add_scene(const mpm_config& cfg, const std::vector<mpm_rheology>& rows, const float* xyz,
                           const float* velp, const float* mass, const float* vol, const uint32_t* mat_ids, uint32_t n,
                           float dt, uint32_t tile_cap) {
+  records_valid = false;  // the state (or what its records depend on) changes
   eng->check();
   if (rows.empty() || rows.size() > (size_t)kMaxMaterials)
     throw Error(MPM_ERR_INVALID, "MPM scene needs 1..=8 material rows");
@@ -553,6 +554,7 @@ void Group::finish_retirements() {
 }
 
 void Group::set_scene_budget(uint32_t sid, uint32_t substeps, cudaStream_t st, bool fresh) {
+  records_valid = false;  // the state (or what its records depend on) changes
   if (sid >= scenes.size() || !scenes[sid].live) throw Error(MPM_ERR_INVALID, "unknown MPM scene");
   uint32_t done = 0;  // a scene just added has completed none
   if (!fresh) {
@@ -591,6 +593,7 @@ bool Group::any_svd64() const {
 void Group::set_scene_dt(uint32_t sid, float dt) {
   SceneHost& s = scenes.at(sid);
   if (s.dt == dt) return;
+  records_valid = false;  // the records hold dt (the stress term)
   s.dt = dt;
   SceneDev d = make_scene_dev(s.cfg, s.rows, dt);
   d.n_rigid = s.n_rigid;
@@ -682,6 +685,7 @@ void Group::read_scene_wrench(uint32_t sid, float* out6, uint32_t n, cudaStream_
 }
 
 void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) {
+  records_valid = false;  // the state (or what its records depend on) changes
   SceneHost& s = scenes.at(sid);
   s.rows = rows;
   const float dt = s.dt;
@@ -690,6 +694,7 @@ void Group::set_scene_rows(uint32_t sid, const std::vector<mpm_rheology>& rows) 
 }
 
 void Group::set_scene_cfg(uint32_t sid, const mpm_config& cfg) {
+  records_valid = false;  // the state (or what its records depend on) changes
   SceneHost& s = scenes.at(sid);
   if (s.tile_cap && cfg.time_step == MPM_TIME_STEP_IMPLICIT)
     throw Error(MPM_ERR_UNSUPPORTED, "sparse MPM grid storage runs the explicit time step only");
@@ -709,6 +714,7 @@ unsigned char* Group::staging_bytes(size_t bytes) {
 }
 
 void Group::set_material_ids(uint32_t sid, const uint32_t* host_ids, uint32_t n) {
+  records_valid = false;  // the state (or what its records depend on) changes
   SceneHost& s = scenes.at(sid);
   if (n != s.n) throw Error(MPM_ERR_INVALID, "material id count does not match the particle count");
   if (!n) return;
@@ -734,6 +740,7 @@ static int bits_for(uint64_t values) {
 // every slot is kept for the scatter, and the work list is rebuilt from the
 // tile boundaries.
 void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
+  if (!move_records) records_valid = false;  // the records stay in the old order
   ProfRec pr;
   eng->prof_begin(kStageOrdering, st, &pr);
   if (compute_keys) {
@@ -745,6 +752,9 @@ void Group::regroup(bool compute_keys, cudaStream_t st, bool move_records) {
   uint32_t* sids = nullptr;
   MPM_CK(radix_sort_pairs(st, keys_by_id.ptr, nullptr, ks[0].ptr, ks[1].ptr, vs[0].ptr, vs[1].ptr, hist.ptr, n_sort,
                           bits_for((uint64_t)key_space << kCellBits), &skeys, &sids, &eng->launches));
+  // both record buffers exist only in deterministic mode (set_deterministic)
+  if (move_records && (rec[0].count < (size_t)16 * cap || rec[1].count < (size_t)16 * cap))
+    throw Error(MPM_ERR_INVALID, "MPM regroup: records can move only between two allocated record buffers");
   const float4* rsrc = move_records ? reinterpret_cast<const float4*>(rec[rec_cur].ptr) : nullptr;
   float4* rdst = move_records ? reinterpret_cast<float4*>(rec[rec_cur ^ 1].ptr) : nullptr;
   // Particles of retired scenes sorted behind the live ones: only the live
@@ -792,13 +802,13 @@ int Group::scatter_grid() const {
 
 // The gather runs once per SVD form present: over the FP32-SVD items, then
 // over the FP64-SVD items of the work list.
-void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st) {
+void Group::launch_gather_pass(int mode, bool keys, cudaStream_t st, bool publish_all) {
   ProfRec pr;
   eng->prof_begin(mode == kRecord ? kStageRecord : kStageGather, st, &pr);
   for (int f64 = 0; f64 < 2; ++f64) {
     if (!(f64 ? any_svd64() : any_svd32())) continue;
     MPM_CK(launch_gather(mode, keys, f64 != 0, pool(), f64 ? svd_tol64 : svd_tol32, svd_sweeps, reuse_svd ? 1 : 0,
-                         gather_grid(f64 != 0), st));
+                         gather_grid(f64 != 0), st, publish_all));
     eng->launches += 1;
   }
   eng->prof_end(&pr, st);
@@ -927,6 +937,7 @@ Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair
     acc_zero = az0;
     acc_last = al0;
     need_regroup = true;  // every run starts from a fresh regrouping
+    records_valid = false;  // the records are not part of the snapshot
     save(false);
   };
   auto time_current = [&]() {
@@ -1003,6 +1014,7 @@ Group::Shapes Group::autotune_shapes(uint32_t probe, const std::vector<std::pair
 // Fixed-order P2G: a regrouping after every gather (so every particle sits in
 // its base cell when it is deposited) and the two-pass deterministic scatter.
 void Group::set_deterministic(bool on) {
+  records_valid = false;  // the state (or what its records depend on) changes
   if (on == deterministic) return;
   deterministic = on;
   if (on) {
@@ -1074,10 +1086,15 @@ bool Group::regroup_due(uint32_t s, uint32_t substeps) {
 }
 
 void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
+  // With the records of the last call still valid and no regrouping to open
+  // this call, the record-only gather is skipped.  (A regrouping moves the
+  // particles but not the records, whose second buffer exists only in
+  // deterministic mode, so after one the records are recomputed.)
+  const bool reuse_records = records_valid && !deterministic && !need_regroup;
   if (need_regroup || deterministic) regroup(true, st);
   const uint32_t max_jacobi = max_jacobi_iters();
   const bool rigid = any_rigid();
-  launch_gather_pass(kRecord, false, st);
+  if (!reuse_records) launch_gather_pass(kRecord, false, st);
   finalize_tiles(st);  // sparse scenes: the tile map of the first deposit
   launch_scatter_pass(acc_zero, st);
   int a = acc_zero;
@@ -1096,7 +1113,9 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
       a ^= 1;
       continue;
     }
-    launch_gather_pass(last ? kG2P : kG2PRecord, due, st);
+    // The last gather of a call publishes v and C; outside deterministic
+    // mode it also writes the records, for the next call's first scatter.
+    launch_gather_pass(last && deterministic ? kG2P : kG2PRecord, due, st, last);
     if (!last) {
       finalize_tiles(st);  // sparse scenes: the tile map of the next deposit
       if (deterministic) {
@@ -1114,6 +1133,7 @@ void Group::run_substeps(uint32_t substeps, cudaStream_t st) {
   acc_last = a;
   acc_zero = a ^ 1;
   substeps_done += substeps;
+  records_valid = !deterministic;
 }
 
 void Group::compact(cudaStream_t st) {
@@ -1149,7 +1169,9 @@ Group::GraphKey Group::graph_key(uint32_t substeps) const {
   k.substeps = substeps;
   k.since = deterministic ? 0u : since;
   k.interval = sort_interval;
-  k.flags = ((uint32_t)rec_cur << 5) | ((uint32_t)cur << 4) | ((uint32_t)acc_zero << 3) |
+  k.flags = ((uint32_t)(records_valid && !deterministic && !need_regroup) << 6) | ((uint32_t)rec_cur << 5) |
+            ((uint32_t)cur << 4) |
+            ((uint32_t)acc_zero << 3) |
             ((uint32_t)any_svd64() << 2) | ((uint32_t)any_svd32() << 1) | (need_regroup ? 1u : 0u);
   return k;
 }
@@ -1164,6 +1186,7 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st, cuda
     const GraphKey key = graph_key(substeps);
     const int cur0 = cur, az0 = acc_zero, rc0 = rec_cur;
     const bool nr0 = need_regroup;
+    const bool rv0 = records_valid;
     const uint32_t since0 = since;
     const uint64_t regroups0 = regroups;
     auto it = graphs.find(key);
@@ -1217,6 +1240,7 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st, cuda
       acc_zero = az0;
       rec_cur = rc0;
       need_regroup = nr0;
+      records_valid = rv0;
       since = since0;
       regroups = regroups0;
       compact_issued = false;
@@ -1254,6 +1278,7 @@ void Group::step_graph(uint32_t substeps, uint32_t repeat, cudaStream_t st, cuda
     acc_last = a;
     acc_zero = a ^ 1;
     substeps_done += substeps;
+    records_valid = !deterministic;
     finish_retirements();
   }
   cudaError_t e = cudaGetLastError();
@@ -1285,6 +1310,7 @@ void Group::pack_positions(uint32_t sid, float4* out, cudaStream_t st) {
 }
 
 void Group::write_rows(uint32_t sid, int first, int count, const float* in, cudaStream_t st) {
+  records_valid = false;  // the state (or what its records depend on) changes
   const SceneHost& s = scenes.at(sid);
   if (!s.n) return;
   const size_t bytes = (size_t)count * s.n * sizeof(float);
@@ -1367,6 +1393,7 @@ void Group::status_words(std::vector<uint32_t>& out, cudaStream_t st) {
 }
 
 void Group::reset_status(uint32_t sid, cudaStream_t st) {
+  records_valid = false;  // the state (or what its records depend on) changes
   MPM_CK(cudaMemsetAsync(status_d.ptr + (size_t)sid * kStatusWords, 0, kStatusWords * 4, st));
   MPM_CK(cudaStreamSynchronize(st));
 }

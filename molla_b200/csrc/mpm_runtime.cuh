@@ -224,6 +224,13 @@ class Group {
   int acc_zero = 0;  // accumulator known to be all zero
   int acc_last = 1;  // accumulator holding the last scatter
   bool need_regroup = true;
+  // The scatter records in rec[rec_cur] belong to the current state: the
+  // last call ended with a gather that wrote them, and nothing on the host
+  // has changed the particles, their materials or their scenes since.  The
+  // next call then starts with its scatter instead of a record-only gather
+  // (which recomputes every particle's SVD and stress).  Cleared by every
+  // host-side change of state and never set in deterministic mode.
+  bool records_valid = false;
   bool scenes_dirty = true;
   bool keys_dirty = true;  // scene key offsets changed
   uint32_t sort_interval = 32;
@@ -384,7 +391,7 @@ class Group {
   // substeps; advances `since`.  Sets need_regroup when one falls due on
   // the last substep (it opens the next call instead).
   bool regroup_due(uint32_t s, uint32_t substeps);
-  void launch_gather_pass(int mode, bool keys, cudaStream_t st);
+  void launch_gather_pass(int mode, bool keys, cudaStream_t st, bool publish_all = false);
   void launch_scatter_pass(int acc_out, cudaStream_t st);
   void launch_fused_pass(int acc_out, bool keys, cudaStream_t st);
  public:

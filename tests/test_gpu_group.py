@@ -298,6 +298,77 @@ def test_retired_scenes_leave_at_the_next_regroup(engine):
         assert np.abs(srv.poll(t)[1] - alone(engine, s, 24)).max() < TOL
 
 
+def test_records_carried_across_calls(engine):
+    """A call whose state is unchanged since the last call's final gather,
+    and which no regrouping opens, starts with its scatter on that gather's
+    records: 24 calls of step_n(1) between regroupings run one record-only
+    gather (the first call's), like one step_n(24), and end in the same
+    state; with regroupings every 8 substeps, a record-only gather follows
+    each regrouping that opens a call.  Every host change the records depend
+    on (particle state, mass and volume, materials, dt) makes the next call
+    recompute them: its state then equals a fresh simulation set up with the
+    same particles."""
+    s = small_scenes()[1]
+    cfg = m.config_for_scene(s)
+
+    def make(interval):
+        sim = m.MpmSimulation.new(engine, cfg)
+        sim.set_particles(s.positions)
+        sim.set_materials(s.rows, s.ids)
+        sim.set_sort_interval(interval)
+        return sim
+
+    def stages(fn):
+        engine.synchronize()
+        engine.reset_profile()
+        engine.profile(True)
+        fn()
+        engine.synchronize()
+        engine.profile(False)
+        prof = engine.read_profile()
+        return prof["StressRecord"][0], prof["ParticleOrdering"][0]
+
+    a = make(64)
+    assert stages(lambda: [a.step_n(s.dt, 1) for _ in range(24)])[0] == 1
+    b = make(64)
+    assert stages(lambda: b.step_n(s.dt, 24))[0] == 1
+    assert np.abs(a.read_positions() - b.read_positions()).max() < TOL
+    b.close()
+    d = make(8)
+    rec, order = stages(lambda: [d.step_n(s.dt, 1) for _ in range(24)])
+    assert rec == order == 3, (rec, order)  # the calls that regrouping opens: 1, 9 and 17
+    d.close()
+    a.set_sort_interval(64)
+    # host changes between calls: each forces one record pass
+    _, F, jp = a.read_particle_state()
+    assert stages(lambda: a.step_n(s.dt, 3))[0] <= 1  # a regrouping may open it (new cadence)
+    assert stages(lambda: a.step_n(s.dt, 3))[0] == 0
+    for change in (lambda: a.write_particle_state(F=F * np.float32(1.02)),
+                   lambda: a.set_particle_mass_volume(mass=np.full(s.n, 1.5 * cfg.particle_mass, np.float32)),
+                   lambda: a.set_materials(s.rows, s.ids),
+                   lambda: a.step_n(0.5 * s.dt, 1)):
+        change()
+        assert stages(lambda: a.step_n(s.dt, 2))[0] == 1
+        assert stages(lambda: a.step_n(s.dt, 2))[0] == 0
+    # the state after a change matches a fresh simulation given that state
+    pos, vel = a.read_positions(), a.read_velocities()
+    C, F, jp = a.read_particle_state()
+    F2 = (F * np.float32(1.03)).astype(np.float32)
+    a.write_particle_state(F=F2)
+    a.step_n(s.dt, 6)
+    c = m.MpmSimulation.new(engine, cfg)
+    c.set_particles(pos, vel)
+    c.set_materials(s.rows, s.ids)
+    c.set_particle_mass_volume(mass=np.full(s.n, 1.5 * cfg.particle_mass, np.float32))
+    c.write_particle_state(C, F2, jp)
+    c.set_sort_interval(8)
+    c.step_n(s.dt, 6)
+    assert np.abs(a.read_positions() - c.read_positions()).max() < TOL
+    assert np.abs(a.read_velocities() - c.read_velocities()).max() < 1e-4 * max(1.0, np.abs(vel).max())
+    a.close()
+    c.close()
+
+
 def test_regroup_cadence_independent_of_call_chunking(engine):
     """The regrouping cadence is carried across calls: 64 calls of
     step_n(1) regroup as often as one step_n(64) (the reference regroups on

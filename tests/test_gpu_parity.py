@@ -745,11 +745,13 @@ def test_stage_profile_counts_launches(engine):
     engine.profile(False)
     prof = engine.read_profile()
     assert set(prof) == set(m.Engine.STAGES)
-    assert prof["GridUpdate"][0] == 10 and prof["StressRecord"][0] == 1
+    # no record-only gather: the previous call's last gather left the records
+    # and no regrouping opens this call
+    assert prof["GridUpdate"][0] == 10 and prof["StressRecord"][0] == 0
     # gathers: every substep; scatters: once per call when fused, else every substep but the last
     assert prof["GridToParticle"][0] == 10
     assert prof["ParticleToGrid"][0] in (1, 10)
-    assert prof["ParticleOrdering"][0] >= 2  # the call's first regroup + one every 4 substeps
+    assert prof["ParticleOrdering"][0] >= 2  # one every 4 substeps of the cadence
     assert all(ms > 0.0 for cnt, ms in prof.values() if cnt)
     sim.step_n(1.0 / 480, 3)
     engine.synchronize()
