@@ -409,18 +409,26 @@ def run_ours(args):
         # interval, item size, fused or separate kernels, CTAs per SM
         shapes, tune = sim.autotune_shapes(scene.dt, probe_substeps=32)
         interval = shapes["sort_interval"]
+    # The regroup cadence restarts `pad` substeps before the window, so that
+    # the window's regroupings fall at cadence points around its middle (one
+    # at its middle when K < interval, where it is more than its share): the
+    # window holds its share of them rounded, and at least one.  The timed
+    # call is a stepping loop's next call: it starts on the records the
+    # previous call's last gather left, unless a regrouping opens it (pad 0).
+    pad = (interval - (args.steps // 2) % interval) % interval
     sim.set_sort_interval(interval)
-    if start_at > first:
-        sim.step_n(scene.dt, start_at - first)
+    if start_at - pad > first:
+        sim.step_n(scene.dt, start_at - pad - first)
     engine.synchronize()
     gm, _ = sim.read_grid_mass_momentum()
     active = int((gm > 0).sum())
     del gm
-    # The regroup cadence starts afresh so that the timed call opens with a
-    # regrouping: the window holds 1 + floor((K - 1) / interval) of them,
-    # at least its share at the regular cadence.
-    sim.set_sort_interval(interval)
-    regroups_in_window = 1 + (args.steps - 1) // interval
+    sim.set_sort_interval(interval)  # the cadence starts afresh: the next call opens with a regrouping
+    if pad:
+        sim.step_n(scene.dt, pad)
+    start_at = max(start_at, first + pad)
+    # a regrouping due after the window's last substep opens the next call
+    regroups_in_window = (pad + args.steps - 1) // interval if pad else 1 + (args.steps - 1) // interval
 
     # timed region: K substeps in one step_n call, bracketed by a barrier
     # and synchronisation on both sides; device time from CUDA events
