@@ -325,6 +325,18 @@ def run_reference(args):
 RUN_SUBSTEPS = 500
 
 
+def window_plan(steps: int, interval: int):
+    """(pad, regroupings) of a timed window of `steps` substeps under a
+    regroup cadence of `interval`: the cadence restarts `pad` substeps before
+    the window, which puts its regroupings at cadence points around the
+    window's middle, and the window then holds `regroupings` of them (a
+    regrouping due after its last substep opens the next call instead; with
+    pad 0 one opens the window's own call)."""
+    pad = (interval - (steps // 2) % interval) % interval
+    regroups = (pad + steps - 1) // interval if pad else 1 + (steps - 1) // interval
+    return pad, regroups
+
+
 def measure_accuracy(n_sample: int, substeps: int, threads: int):
     """Errors of the GPU's FP32 + FP64-SVD step against the FP64 oracle (FP64
     state, FP64 Jacobi SVD to 1e-14) on a sample of the large scene's
@@ -415,7 +427,7 @@ def run_ours(args):
     # window holds its share of them rounded, and at least one.  The timed
     # call is a stepping loop's next call: it starts on the records the
     # previous call's last gather left, unless a regrouping opens it (pad 0).
-    pad = (interval - (args.steps // 2) % interval) % interval
+    pad, regroups_in_window = window_plan(args.steps, interval)
     sim.set_sort_interval(interval)
     if start_at - pad > first:
         sim.step_n(scene.dt, start_at - pad - first)
@@ -427,8 +439,6 @@ def run_ours(args):
     if pad:
         sim.step_n(scene.dt, pad)
     start_at = max(start_at, first + pad)
-    # a regrouping due after the window's last substep opens the next call
-    regroups_in_window = (pad + args.steps - 1) // interval if pad else 1 + (args.steps - 1) // interval
 
     # timed region: K substeps in one step_n call, bracketed by a barrier
     # and synchronisation on both sides; device time from CUDA events
